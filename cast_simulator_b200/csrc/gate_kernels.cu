@@ -1,0 +1,330 @@
+// Gate-application kernels for sm_100a: apply a fused k-qubit complex gate
+// (2^k x 2^k, row-major) in place to an interleaved re/im statevector of 2^n
+// amplitudes, in FP32 or FP64.
+//
+// This is the hot path the reference generates per gate with LLVM NVPTX
+// (src/cpp/cuda/cuda_gen.cpp:174-342: combo -> base offset by bit insertion,
+// 2^k loads, straight-line matvec, 2^k stores, persistent grid-stride loop).
+// Here the kernels are precompiled templates on (scalar type, k) and the
+// matrix is data:
+//
+//  * k <= 5 ("register" kernels): one thread owns one gather group of 2^k
+//    amplitudes in registers.  The matrix travels in the kernel parameter
+//    block, so every matrix scalar is a constant-bank operand of the FMA that
+//    uses it (no load instruction, uniform across the warp) - the data-side
+//    equivalent of the reference's baked-in immediates.  Consecutive threads
+//    take consecutive groups, i.e. they walk the lowest non-target qubits, so
+//    each of the 2^k 128-bit (f64) / 64-bit (f32) loads of a warp is one
+//    contiguous run whenever the lowest target is >= 5 and stays within the
+//    same cache lines across the 2^k loads otherwise.
+//  * k = 6, 7 ("staged" kernels): a CTA stages 32 groups (32 x 2^k amplitudes)
+//    in shared memory with coalesced loads, then computes the 2^k x 2^k by
+//    2^k x 32 complex product with each thread holding 2^k/8 accumulators and
+//    stores straight back to HBM.
+//
+// Zero / +-1 matrix scalars (classified on the host with the reference's
+// tolerances) are exact, so dense evaluation reproduces the reference's
+// skipped / sign-flipped products bit for bit up to summation order.
+#include "internal.hpp"
+
+#include <algorithm>
+#include <mutex>
+
+namespace cb2 {
+
+namespace {
+
+template <typename T> struct Vec2;
+template <> struct Vec2<float> { using type = float2; };
+template <> struct Vec2<double> { using type = double2; };
+
+// Target qubits (ascending) with their low-bit masks, passed by value.
+struct Targets {
+  uint64_t lo_mask[kMaxGateQubits];  // (1 << q_b) - 1
+  uint64_t stride[kMaxGateQubits];   // 1 << q_b (amplitude units)
+};
+
+template <typename T, int K> struct MatParam {
+  T m[2 * (1 << K) * (1 << K)];
+};
+
+// Group index -> amplitude index of the group's first member: insert a zero
+// bit at every target position, lowest first (the PDEP of cuda_gen.cpp:174-211).
+template <int K>
+__device__ __forceinline__ uint64_t group_base(uint64_t g, const Targets &t) {
+#pragma unroll
+  for (int b = 0; b < K; ++b) g = ((g & ~t.lo_mask[b]) << 1) | (g & t.lo_mask[b]);
+  return g;
+}
+
+template <int K>
+__device__ __forceinline__ uint64_t member_offset(int a, const Targets &t) {
+  uint64_t off = 0;
+#pragma unroll
+  for (int b = 0; b < K; ++b)
+    if ((a >> b) & 1) off += t.stride[b];
+  return off;
+}
+
+// Register kernel: thread -> U gather groups (U = 2 for k <= 2 so that each
+// thread keeps >= 64 bytes in flight), no grid-stride loop: a loop would let
+// the compiler hoist the matrix out of the constant bank into registers.
+constexpr int kRegThreads = 128;
+
+template <int K> struct RegUnroll { static constexpr int U = K <= 2 ? 2 : 1; };
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kRegThreads) k_gate_reg(T *__restrict__ sv, uint64_t n_groups,
+                                                          Targets t, MatParam<T, K> M) {
+  using V = typename Vec2<T>::type;
+  constexpr int D = 1 << K;
+  constexpr int U = RegUnroll<K>::U;
+  V *psi = reinterpret_cast<V *>(sv);
+  const uint64_t g0 = (uint64_t)blockIdx.x * (kRegThreads * U) + threadIdx.x;
+  uint64_t base[U];
+  V x[U][D];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const uint64_t g = g0 + (uint64_t)u * kRegThreads;
+    base[u] = group_base<K>(g < n_groups ? g : 0, t);
+    if (g < n_groups) {
+#pragma unroll
+      for (int a = 0; a < D; ++a) x[u][a] = psi[base[u] + member_offset<K>(a, t)];
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    if (g0 + (uint64_t)u * kRegThreads >= n_groups) break;
+#pragma unroll
+    for (int r = 0; r < D; ++r) {
+      T re = T(0), im = T(0);
+#pragma unroll
+      for (int c = 0; c < D; ++c) {
+        const T mr = M.m[2 * (r * D + c)];
+        const T mi = M.m[2 * (r * D + c) + 1];
+        re = fma(mr, x[u][c].x, re);
+        re = fma(-mi, x[u][c].y, re);
+        im = fma(mr, x[u][c].y, im);
+        im = fma(mi, x[u][c].x, im);
+      }
+      V o;
+      o.x = re;
+      o.y = im;
+      psi[base[u] + member_offset<K>(r, t)] = o;
+    }
+  }
+}
+
+// Staged kernel for k = 6, 7: tiles of G groups in shared memory.
+constexpr int kStagedThreads = 256;
+constexpr int kStagedGroups = 32;
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kStagedThreads) k_gate_staged(
+    T *__restrict__ sv, uint64_t n_groups, Targets t, const typename Vec2<T>::type *__restrict__ mat) {
+  using V = typename Vec2<T>::type;
+  constexpr int D = 1 << K;
+  constexpr int G = kStagedGroups;
+  constexpr int SLOTS = kStagedThreads / G;  // row slots
+  constexpr int RPT = D / SLOTS;             // rows per thread
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V *s = reinterpret_cast<V *>(smem_raw);    // [D][G]
+  V *psi = reinterpret_cast<V *>(sv);
+  const int g_lane = threadIdx.x % G;
+  const int slot = threadIdx.x / G;
+  const uint64_t n_tiles = (n_groups + G - 1) / G;
+  for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const uint64_t g0 = tile * G;
+    // stage: thread i loads member a = i / G of group g0 + i % G
+    for (int i = threadIdx.x; i < D * G; i += kStagedThreads) {
+      const int gg = i % G, a = i / G;
+      const uint64_t g = g0 + gg;
+      if (g < n_groups) s[a * G + gg] = psi[group_base<K>(g, t) + member_offset<K>(a, t)];
+    }
+    __syncthreads();
+    const uint64_t g = g0 + g_lane;
+    if (g < n_groups) {
+      T acc_re[RPT], acc_im[RPT];
+#pragma unroll
+      for (int j = 0; j < RPT; ++j) acc_re[j] = acc_im[j] = T(0);
+#pragma unroll 4
+      for (int c = 0; c < D; ++c) {
+        const V xc = s[c * G + g_lane];
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+          const V m = __ldg(&mat[(slot + j * SLOTS) * D + c]);
+          acc_re[j] = fma(m.x, xc.x, acc_re[j]);
+          acc_re[j] = fma(-m.y, xc.y, acc_re[j]);
+          acc_im[j] = fma(m.x, xc.y, acc_im[j]);
+          acc_im[j] = fma(m.y, xc.x, acc_im[j]);
+        }
+      }
+      const uint64_t base = group_base<K>(g, t);
+#pragma unroll
+      for (int j = 0; j < RPT; ++j) {
+        V o;
+        o.x = acc_re[j];
+        o.y = acc_im[j];
+        psi[base + member_offset<K>(slot + j * SLOTS, t)] = o;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+int g_sm_count = 0;
+std::once_flag g_sm_once;
+
+template <typename F> int max_blocks_per_sm(F kernel, int threads, size_t smem) {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, smem) != cudaSuccess ||
+      b < 1)
+    b = 1;
+  return b;
+}
+
+template <typename T, int K>
+bool launch_reg(const GateData &g, void *sv, uint32_t n, const Targets &t, cudaStream_t s,
+                std::string &err) {
+  constexpr int U = RegUnroll<K>::U;
+  const uint64_t n_groups = 1ull << (n - K);
+  const uint64_t blocks = (n_groups + kRegThreads * U - 1) / (kRegThreads * U);
+  if (blocks > 0x7fffffffull) {
+    err = "statevector too large for the gate kernel grid";
+    return false;
+  }
+  const MatParam<T, K> *mp;
+  if constexpr (sizeof(T) == 8) mp = reinterpret_cast<const MatParam<T, K> *>(g.m64.data());
+  else mp = reinterpret_cast<const MatParam<T, K> *>(g.m32.data());
+  T *p = static_cast<T *>(sv);
+  void *args[] = {&p, const_cast<uint64_t *>(&n_groups), const_cast<Targets *>(&t),
+                  const_cast<MatParam<T, K> *>(mp)};
+  return cuda_ok(cudaLaunchKernel((const void *)k_gate_reg<T, K>, dim3((unsigned)blocks),
+                                  dim3(kRegThreads), args, 0, s),
+                 "gate kernel launch", err);
+}
+
+template <typename T, int K>
+bool launch_staged(const GateData &g, void *sv, uint32_t n, const Targets &t, cudaStream_t s,
+                   std::string &err) {
+  using V = typename Vec2<T>::type;
+  constexpr size_t smem = sizeof(V) * (1 << K) * kStagedGroups;
+  static int blocks_per_sm = 0;
+  static std::once_flag once;
+  static cudaError_t attr_rc = cudaSuccess;
+  std::call_once(once, [] {
+    attr_rc = cudaFuncSetAttribute(k_gate_staged<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem);
+    blocks_per_sm = max_blocks_per_sm(k_gate_staged<T, K>, kStagedThreads, smem);
+  });
+  if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(staged gate kernel)", err)) return false;
+  if (!g.d_mat) {
+    err = "staged gate kernel needs a device matrix";
+    return false;
+  }
+  const uint64_t n_groups = 1ull << (n - K);
+  const uint64_t n_tiles = (n_groups + kStagedGroups - 1) / kStagedGroups;
+  const uint64_t cap = (uint64_t)blocks_per_sm * sm_count();
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min(n_tiles, cap));
+  k_gate_staged<T, K><<<grid, kStagedThreads, smem, s>>>(static_cast<T *>(sv), n_groups, t,
+                                                          static_cast<const V *>(g.d_mat));
+  return cuda_ok(cudaGetLastError(), "staged gate kernel launch", err);
+}
+
+template <typename T>
+bool launch_t(const GateData &g, void *sv, uint32_t n, const Targets &t, cudaStream_t s,
+              std::string &err) {
+  switch (g.k) {
+  case 1: return launch_reg<T, 1>(g, sv, n, t, s, err);
+  case 2: return launch_reg<T, 2>(g, sv, n, t, s, err);
+  case 3: return launch_reg<T, 3>(g, sv, n, t, s, err);
+  case 4: return launch_reg<T, 4>(g, sv, n, t, s, err);
+  case 5: return launch_reg<T, 5>(g, sv, n, t, s, err);
+  case 6: return launch_staged<T, 6>(g, sv, n, t, s, err);
+  case 7: return launch_staged<T, 7>(g, sv, n, t, s, err);
+  default: err = "unsupported gate size"; return false;
+  }
+}
+
+}  // namespace
+
+int sm_count() {
+  std::call_once(g_sm_once, [] {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        g_sm_count < 1)
+      g_sm_count = 1;
+  });
+  return g_sm_count;
+}
+
+bool check_gate(const GateData &g, uint32_t n, std::string &err) {
+  if (g.k == 0 || g.k > kMaxGateQubits) {
+    err = "gate must act on 1.." + std::to_string(kMaxGateQubits) + " qubits, got " +
+          std::to_string(g.k);
+    return false;
+  }
+  if (n < g.k) {
+    err = "statevector has fewer qubits than the gate kernel requires";
+    return false;
+  }
+  if (n > kMaxSvQubits) {
+    err = "statevector qubit count " + std::to_string(n) + " exceeds the supported maximum";
+    return false;
+  }
+  for (uint32_t b = 0; b < g.k; ++b) {
+    if (g.qubits[b] >= n) {
+      err = "gate acts on qubit " + std::to_string(g.qubits[b]) + " outside the " +
+            std::to_string(n) + "-qubit statevector";
+      return false;
+    }
+    if (b && g.qubits[b - 1] >= g.qubits[b]) {
+      err = "gate qubits must be distinct and ascending";
+      return false;
+    }
+  }
+  const size_t want = 2ull << (2 * g.k);
+  if ((g.precision == 1 && g.m64.size() != want) || (g.precision == 0 && g.m32.size() != want)) {
+    err = "gate matrix has the wrong size";
+    return false;
+  }
+  return true;
+}
+
+bool launch_gate(const GateData &g, void *sv, uint32_t n, cudaStream_t stream, std::string &err) {
+  if (!check_gate(g, n, err)) return false;
+  if (!sv) {
+    err = "statevector pointer must not be null";
+    return false;
+  }
+  Targets t;
+  for (uint32_t b = 0; b < kMaxGateQubits; ++b) {
+    const uint32_t q = b < g.k ? g.qubits[b] : 0;
+    t.lo_mask[b] = (1ull << q) - 1;
+    t.stride[b] = 1ull << q;
+  }
+  return g.precision == 1 ? launch_t<double>(g, sv, n, t, stream, err)
+                          : launch_t<float>(g, sv, n, t, stream, err);
+}
+
+void snap_matrix(GateData &g, const double *m, double ztol, double otol) {
+  const size_t dim = 1ull << g.k;
+  const double K = (double)dim;
+  const double zt = ztol / K, ot = otol / K;
+  const size_t ns = 2 * dim * dim;
+  g.m64.resize(ns);
+  g.m32.resize(ns);
+  for (size_t i = 0; i < ns; ++i) {
+    const double v = m[i];
+    double s;
+    if (ztol > 0.0 && std::fabs(v) < zt) s = 0.0;
+    else if (otol > 0.0 && std::fabs(v - 1.0) < ot) s = 1.0;
+    else if (otol > 0.0 && std::fabs(v + 1.0) < ot) s = -1.0;
+    else s = v;
+    g.m64[i] = s;
+    g.m32[i] = (float)s;
+  }
+}
+
+}  // namespace cb2

@@ -1,0 +1,58 @@
+// Internal (non-exported) declarations shared by the CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace cb2 {
+
+constexpr uint32_t kMaxGateQubits = 7;   // largest fused gate the kernels handle
+constexpr uint32_t kMaxSvQubits = 40;    // index math is 64-bit; HBM bounds the rest
+
+// A gate ready for the device: canonical (ascending) qubits and the
+// sparsity-snapped matrix in FP64 and FP32 (row-major, interleaved re/im).
+struct GateData {
+  uint32_t k = 0;
+  uint8_t precision = 1;  // 0 = F32, 1 = F64
+  uint32_t qubits[kMaxGateQubits] = {0};
+  std::vector<double> m64;
+  std::vector<float> m32;
+  void *d_mat = nullptr;  // device copy in the gate's precision (owned by the holder)
+};
+
+// Error helper: fills `err` and returns false on a CUDA failure.
+inline bool cuda_ok(cudaError_t rc, const char *what, std::string &err) {
+  if (rc == cudaSuccess) return true;
+  err = std::string(what) + " failed: " + cudaGetErrorName(rc) + " - " + cudaGetErrorString(rc);
+  return false;
+}
+
+inline void write_err(char *buf, size_t len, const std::string &msg) {
+  if (!buf || len == 0) return;
+  const size_t n = msg.size() < len - 1 ? msg.size() : len - 1;
+  std::memcpy(buf, msg.data(), n);
+  buf[n] = '\0';
+}
+
+inline void clear_err(char *buf, size_t len) {
+  if (buf && len) buf[0] = '\0';
+}
+
+// Validates the gate against an n-qubit statevector.
+bool check_gate(const GateData &g, uint32_t n, std::string &err);
+
+// Enqueues one gate application on `stream` (in place on `sv`).
+bool launch_gate(const GateData &g, void *sv, uint32_t n, cudaStream_t stream, std::string &err);
+
+// Classifies matrix scalars as 0 / +-1 / immediate with tolerances scaled by
+// 1/2^k and fills g.m64 / g.m32 (src/cpp/cuda/cuda_gen.cpp:84-103).
+void snap_matrix(GateData &g, const double *interleaved, double ztol, double otol);
+
+// Device helpers shared with the reduction TU.
+int sm_count();
+
+}  // namespace cb2

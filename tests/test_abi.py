@@ -1,0 +1,91 @@
+"""The C-ABI library: loads, exports every declared symbol, and the
+GPU-free parts of the gate pipeline (descriptor + blob) behave like the
+reference's (error convention of src/cpp/internal/err_buf.hpp:12-23)."""
+import ctypes as C
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        names |= set(re.findall(r"\b(cast_\w+)\s*\(", text))
+    return sorted(names)
+
+
+def test_exports_every_declared_symbol(cblib):
+    names = declared_symbols()
+    assert len(names) >= 26
+    missing = [n for n in names if not hasattr(cblib, n)]
+    assert not missing, missing
+
+
+def _compile(cblib, mat, qubits, prec=1, ztol=1e-12, otol=1e-12):
+    from cast_simulator_b200 import _lib as L
+
+    spec = L.KernelGenSpec(prec, ztol, otol, 10, 0, 128)
+    m = np.ascontiguousarray(mat, dtype=np.complex128)
+    q = np.ascontiguousarray(qubits, dtype=np.uint32)
+    ptx, fn = C.c_void_p(), C.c_void_p()
+    kq, pr = C.c_uint32(), C.c_uint8()
+    eb = L.errbuf()
+    rc = cblib.cast_cuda_compile_gate_ptx(
+        C.byref(spec), m.view(np.float64).ctypes.data_as(C.POINTER(L.Complex64)), m.size,
+        q.ctypes.data_as(L.c_u32p), q.size, C.byref(ptx), C.byref(fn), C.byref(kq), C.byref(pr),
+        eb, L.ERR_LEN)
+    return rc, eb.value.decode(), ptx, fn, kq.value, pr.value
+
+
+def test_compile_descriptor_roundtrip(cblib):
+    rng = np.random.default_rng(1)
+    m = rng.standard_normal((8, 8)) + 1j * rng.standard_normal((8, 8))
+    m[0, 0] = 1 + 1e-14  # snapped to exactly 1 (otol / K)
+    rc, err, ptx, fn, k, pr = _compile(cblib, m, [1, 4, 9])
+    assert rc == 0 and err == "" and k == 3 and pr == 1
+    text = C.string_at(ptx.value).decode()
+    assert C.string_at(fn.value) == b"k_gate"
+    assert ".qubits 1 4 9" in text and ".precision f64" in text
+    from cast_simulator_b200 import _lib as L
+
+    blob, ln = C.c_void_p(), C.c_size_t()
+    eb = L.errbuf()
+    assert cblib.cast_cuda_ptx_to_cubin(text.encode(), C.byref(blob), C.byref(ln), eb, L.ERR_LEN) == 0
+    raw = C.string_at(blob.value, ln.value)
+    vals = np.frombuffer(raw[-64 * 16:], dtype=np.complex128).reshape(8, 8)
+    assert vals[0, 0] == 1.0 and np.array_equal(vals[1:], m[1:])
+    cblib.cast_cuda_cubin_free(blob)
+    cblib.cast_cuda_str_free(ptx)
+    cblib.cast_cuda_str_free(fn)
+
+
+def test_compile_errors(cblib):
+    rc, err, *_ = _compile(cblib, np.eye(4), [0])
+    assert rc == 1 and "matrixLen" in err
+    rc, err, *_ = _compile(cblib, np.eye(4), [3, 1])
+    assert rc == 1 and "ascending" in err
+    rc, err, *_ = _compile(cblib, np.eye(256), list(range(8)))
+    assert rc == 1 and "not supported" in err
+    rc, err, *_ = _compile(cblib, np.eye(2), [0], prec=5)
+    assert rc == 1 and "precision" in err
+
+
+def test_bad_descriptor_rejected(cblib):
+    from cast_simulator_b200 import _lib as L
+
+    blob, ln = C.c_void_p(), C.c_size_t()
+    eb = L.errbuf()
+    assert cblib.cast_cuda_ptx_to_cubin(b".version 8.0\n", C.byref(blob), C.byref(ln), eb, L.ERR_LEN) == 1
+    assert b"descriptor" in eb.value
+    assert cblib.cast_cuda_cubin_load(b"garbage-garbage-garbage-garbage-" * 4, 128, eb, L.ERR_LEN) is None
+    assert b"not a cast_b200 gate module" in eb.value
+    assert cblib.cast_cuda_kernel_launch(None, None, 0, 1, 4, eb, L.ERR_LEN) == 1
+    assert b"must not be null" in eb.value

@@ -1,0 +1,139 @@
+"""GPU parity of the gate path through the drop-in C ABI vs the CPU oracle.
+
+Tolerances are the reference's (tests/cpu_cuda_compare.rs:27, 397): 1e-10 per
+amplitude for FP64, 1e-5 for FP32; 1e-9 for sequential circuits
+(tests/circuit_execution_order.rs:34)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL = {1: 1e-10, 0: 1e-5}
+
+
+@pytest.fixture(scope="module")
+def cu(cblib):
+    from cast_simulator_b200 import cuda
+
+    return cuda
+
+
+def run_gates(cu, n, gates, init, prec):
+    spec = cu.CudaKernelGenSpec.f64() if prec == 1 else cu.CudaKernelGenSpec.f32()
+    mgr = cu.CudaKernelManager(spec)
+    sv = cu.CudaStatevector(n, cu.CudaPrecision(prec))
+    sv.upload(init)
+    for g in gates:
+        mgr.apply(mgr.generate(g), sv)
+    mgr.sync()
+    return sv.download()
+
+
+class _G:
+    def __init__(self, m, q):
+        self._m, self._q = np.ascontiguousarray(m), tuple(q)
+
+    def matrix(self):
+        return self._m
+
+    def qubits(self):
+        return self._q
+
+
+def haar(rng, d):
+    z = rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))
+    q, r = np.linalg.qr(z)
+    return q * (np.diag(r) / np.abs(np.diag(r)))
+
+
+@pytest.mark.parametrize("prec", [1, 0])
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5, 6, 7])
+def test_single_gate_all_placements(cu, oracle, prec, k):
+    rng = np.random.default_rng(100 + k)
+    for n in sorted({k, min(k + 2, 20), 12, 17}):
+        if n < k:
+            continue
+        placements = [tuple(range(k)), tuple(range(n - k, n))]
+        for _ in range(3):
+            placements.append(tuple(sorted(rng.choice(n, size=k, replace=False).tolist())))
+        for q in placements:
+            m = haar(rng, 1 << k)
+            init = oracle.random_state(n, 5 + k)
+            ref = init.copy()
+            oracle.apply_gate(ref, m, q)
+            got = run_gates(cu, n, [_G(m, q)], init, prec)
+            err = np.max(np.abs(got - ref))
+            assert err < TOL[prec], (n, q, err)
+
+
+@pytest.mark.parametrize("prec", [1, 0])
+def test_random_circuit_sequence(cu, oracle, prec):
+    """Random 1q/2q/3q Haar circuits, 14 qubits, 80 gates (circuit_execution_order.rs)."""
+    rng = np.random.default_rng(7)
+    n = 14
+    gates = []
+    for _ in range(80):
+        k = int(rng.integers(1, 4))
+        q = tuple(sorted(rng.choice(n, size=k, replace=False).tolist()))
+        gates.append((haar(rng, 1 << k), q))
+    init = oracle.random_state(n, 3)
+    ref = oracle.simulate(n, gates, init)
+    got = run_gates(cu, n, [_G(m, q) for m, q in gates], init, prec)
+    assert np.max(np.abs(got - ref)) < (1e-9 if prec == 1 else 1e-4)
+    rep = oracle.fidelity_report(ref, got)
+    assert rep["one_minus_abs_overlap"] < (1e-12 if prec == 1 else 1e-5)
+
+
+def test_qft14_golden_on_gpu(cu, oracle):
+    golden = np.load(os.path.join(GOLDEN, "qft14_seeded.npy"))
+    got = run_gates(cu, 14, [_G(m, q) for m, q in oracle.qft_cx(14)], oracle.seeded_state(14), 1)
+    assert np.max(np.abs(got - golden)) < 1e-10
+
+
+def test_sparse_entries_snapped(cu, oracle):
+    """Scalars within ztol/K of 0 and otol/K of +-1 behave as exact 0 / +-1
+    (cuda_gen.cpp:84-103): the GPU matches the oracle run on the snapped matrix."""
+    m = np.array([[1 + 1e-14, 2e-14j], [3e-14, -1 - 1e-14j]], dtype=complex)
+    init = oracle.random_state(10, 1)
+    ref = init.copy()
+    oracle.apply_gate(ref, oracle.snap(m, 1e-12, 1e-12), [4])
+    got = run_gates(cu, 10, [_G(m, [4])], init, 1)
+    assert np.max(np.abs(got - ref)) < 1e-15
+
+
+@pytest.mark.parametrize("prec", [1, 0])
+def test_statevector_memory_and_reductions(cu, oracle, prec):
+    n = 15
+    sv = cu.CudaStatevector(n, cu.CudaPrecision(prec))
+    sv.zero()
+    z = sv.download()
+    assert z[0] == 1 and np.count_nonzero(z) == 1
+    init = oracle.random_state(n, 9) * 3.0
+    sv.upload(init)
+    back = sv.download()
+    assert np.max(np.abs(back - init)) < (1e-15 if prec else 1e-6)
+    assert abs(sv.norm_squared() - 9.0) < (1e-12 if prec else 1e-5)
+    sv.normalize()
+    assert abs(sv.norm_squared() - 1.0) < (1e-12 if prec else 1e-5)
+    c = sv.clone_device()
+    assert np.array_equal(c.download(), sv.download())
+
+
+def test_tiny_statevectors(cu, oracle):
+    """n = k edge cases and the scalar tail of the reductions (n = 0, 1)."""
+    for n in (1, 2):
+        sv = cu.CudaStatevector(n, cu.CudaPrecision.F32)
+        sv.upload(oracle.random_state(n, 2))
+        assert abs(sv.norm_squared() - 1) < 1e-6
+
+
+def test_launch_errors(cu):
+    mgr = cu.CudaKernelManager(cu.CudaKernelGenSpec.f64())
+    kid = mgr.generate(_G(np.eye(4), (2, 5)))
+    sv = cu.CudaStatevector(4, cu.CudaPrecision.F64)
+    with pytest.raises(ValueError, match="outside"):
+        mgr.apply(kid, sv)
