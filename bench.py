@@ -1,0 +1,360 @@
+"""Benchmark: fused-gate statevector simulation on B200 (one JSON line).
+
+Workload (the 30-qubit configuration of the reference comparison): a random
+brickwork circuit on 30 qubits, depth 20 (U3 on every qubit per layer, then
+CZ on alternating neighbour pairs), started from |0...0>, fused with the
+reference's size-only fusion at width k (default 4), complex128 statevector
+(16 GiB, larger than L2).  One step = reset to |0...0> + every fused gate once.
+
+  value  : algorithmic HBM bytes / s over the K timed steps, measured through
+           the drop-in C ABI (compile_gate_ptx -> cubin_load -> kernel_launch)
+           on a device-resident statevector.  Bytes per fused-gate pass are
+           2 * 2^n * 16 (read + write, the reference's accounting,
+           src/profile.rs:427-436).
+  e2e    : same metric through the public Simulator API per step: gate
+           matrices uploaded from host, run, <Z_q> for every qubit read back.
+  roofline / cpu_baseline / clocks: see the JSON keys.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+       [--precision f64|f32] [--k 4] [--n 30] [--depth 20]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks/throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def build_fused(n: int, depth: int, k: int, seed: int = 2024):
+    from cast_simulator_b200.fusion import CircuitGraph, FusionConfig, optimize
+    from cast_simulator_b200.types import QuantumCircuit
+
+    circ = QuantumCircuit.brickwork(n, depth, seed)
+    g = CircuitGraph.from_circuit(circ)
+    optimize(g, FusionConfig.size_only(k))
+    return circ, g.gates_in_row_order()
+
+
+def cpu_baseline_run(n: int, gates, precision: str, budget_s: float, threads: int):
+    """Time the threaded SIMD CPU restatement (oracle/cpu_baseline.cpp) on the
+    host cores: as many fused-gate passes as fit in the budget.  Returns
+    (GB/s, passes, seconds)."""
+    import ctypes as C
+
+    from oracle import oracle as O
+
+    O.build()
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "build", "libcpu_baseline.so"))
+    lib.cb_alloc.restype = C.c_void_p
+    lib.cb_alloc.argtypes = [C.c_uint32, C.c_int]
+    lib.cb_free.argtypes = [C.c_void_p]
+    lib.cb_zero.argtypes = [C.c_void_p]
+    lib.cb_apply.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint32), C.c_uint32,
+                             C.c_int]
+    f32 = precision == "f32"
+    sv = lib.cb_alloc(n, int(f32))
+    if not sv:
+        raise MemoryError("cpu baseline allocation failed")
+    lib.cb_zero(sv)
+    amp_bytes = 8 if f32 else 16
+    mats = [(np.ascontiguousarray(g.matrix()).view(np.float64), np.asarray(g.qubits(), dtype=np.uint32))
+            for g in gates]
+    # one untimed warm-up pass (page faults)
+    m, q = mats[0]
+    lib.cb_apply(sv, m.ctypes.data_as(C.POINTER(C.c_double)), q.ctypes.data_as(C.POINTER(C.c_uint32)),
+                 q.size, threads)
+    passes, t0 = 0, time.perf_counter()
+    while True:
+        m, q = mats[passes % len(mats)]
+        lib.cb_apply(sv, m.ctypes.data_as(C.POINTER(C.c_double)),
+                     q.ctypes.data_as(C.POINTER(C.c_uint32)), q.size, threads)
+        passes += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s and passes >= 2:
+            break
+    lib.cb_free(sv)
+    return passes * 2 * (1 << n) * amp_bytes / el / 1e9, passes, el
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path (threaded C++ restatement of
+    CAST's CPU SIMD kernels; CAST itself cannot be built here) on the host cores."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    n_cpu = min(args.n, args.cpu_n)
+    _, gates = build_fused(n_cpu, args.depth, args.k)
+    samples = []
+    for _ in range(args.warmup):
+        cpu_baseline_run(n_cpu, gates, args.precision, args.cpu_budget / 4, threads)
+    passes_tot = 0
+    for _ in range(args.steps):
+        gbs, passes, el = cpu_baseline_run(n_cpu, gates, args.precision, args.cpu_budget, threads)
+        samples.append(gbs)
+        passes_tot += passes
+    v = float(np.mean(samples))
+    sample = (f"{n_cpu}-qubit brickwork depth {args.depth} fused k={args.k}, "
+              f"{passes_tot} fused-gate passes over {args.steps} steps of ~{args.cpu_budget:.0f} s")
+    line = {
+        "impl": "reference", "metric": "HBM GB/s (fused-gate statevector passes)", "value": v,
+        "unit": "GB/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "dtype": args.precision, "data": "synthetic",
+        "config": {"workload": f"brickwork-{args.n}q-d{args.depth}-{'c128' if args.precision == 'f64' else 'c64'}"
+                   f"-k{args.k}", "cpu_sample_qubits": n_cpu},
+        "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "vs_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def traffic_from_profile(n: int, precision: str, k: int):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (captured on a smaller statevector and scaled by amplitudes)."""
+    p = os.path.join(ROOT, "profiles", "gate_kernel_traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        e = d[f"{precision}_k{k}"]
+        return e["dram_bytes_per_launch"] * (1 << n) / (1 << e["n_qubits"])
+    except Exception:
+        return None
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--k", type=int, default=4)
+    ap.add_argument("--n", type=int, default=30)
+    ap.add_argument("--depth", type=int, default=20)
+    ap.add_argument("--cpu-n", type=int, default=28)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    ws, rank, local = dist_env()
+    pg = None
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        pg = dist
+
+    from cast_simulator_b200 import _lib as L
+    from cast_simulator_b200 import cuda as cu
+    from cast_simulator_b200.simulator import Event, Simulator
+
+    eb = L.errbuf()
+    L.check(L.lib().cast_b200_set_device(local, eb, L.ERR_LEN), eb, "set_device")
+    prec = cu.CudaPrecision.F64 if args.precision == "f64" else cu.CudaPrecision.F32
+    spec = cu.CudaKernelGenSpec.f64() if prec == cu.CudaPrecision.F64 else cu.CudaKernelGenSpec.f32()
+    amp_bytes = 16 if prec == cu.CudaPrecision.F64 else 8
+    n = args.n
+    circ, gates = build_fused(n, args.depth, args.k)
+    bytes_per_pass = 2 * (1 << n) * amp_bytes
+
+    # ---- value: drop-in C ABI path, device-resident statevector ----
+    mgr = cu.CudaKernelManager(spec, timing=True)
+    kids = [mgr.generate(g) for g in gates]
+    sv = cu.CudaStatevector(n, prec)
+
+    def step():
+        sv.zero()
+        for kid in kids:
+            mgr.apply(kid, sv)
+        return mgr.sync()
+
+    for _ in range(args.warmup):
+        step()
+    stream = mgr.stream  # the launching stream: events bracket the kernels themselves
+    if pg:
+        pg.barrier()
+    e_start, e_end = Event(), Event()
+    per_kernel = {}
+    with ClockSampler(local) as clk:
+        e_start.record(stream)
+        wall0 = time.perf_counter()
+        for _ in range(args.steps):
+            st = step()
+            for kt in st.kernels:
+                per_kernel.setdefault(kt.n_gate_qubits, []).append(kt.gpu_time)
+        e_end.record(stream)
+        e_end.sync()
+        wall = time.perf_counter() - wall0
+    t_dev = e_end.elapsed_s(e_start)
+    t = max(t_dev, 1e-12)
+    if pg:
+        import torch
+
+        tt = torch.tensor([t], device=f"cuda:{local}", dtype=torch.float64)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t = float(tt.item())
+    total_bytes = ws * args.steps * len(gates) * bytes_per_pass
+    value = total_bytes / t / 1e9
+    n_launch = args.steps * len(gates)
+
+    # dominant kernel = the gate size with the largest summed device time
+    dom_k = max(per_kernel, key=lambda kk: sum(per_kernel[kk]))
+    dom_avg = float(np.mean(per_kernel[dom_k]))
+    achieved = bytes_per_pass / dom_avg / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    traffic = traffic_from_profile(n, args.precision, dom_k)
+    kernel_share = sum(per_kernel[dom_k]) / sum(sum(v) for v in per_kernel.values())
+
+    # ---- e2e: public Simulator API, gates from host, <Z> read back ----
+    from cast_simulator_b200.fusion import CircuitGraph
+
+    sim = Simulator(spec)
+    fused_graph = CircuitGraph.from_gates(n, gates)
+    h2d = sum(16 * g.matrix().size for g in gates)
+    d2h = 8 * (n + 1)
+    del sv  # free the device-resident state before the e2e state is allocated
+    for _ in range(1):
+        sim.simulate(fused_graph).expectation_z()
+    e0 = time.perf_counter()
+    zs = None
+    for _ in range(args.steps):
+        state = sim.simulate(fused_graph)
+        zs = state.expectation_z()
+        del state
+    e2e_t = time.perf_counter() - e0
+    e2e_value = ws * args.steps * len(gates) * bytes_per_pass / e2e_t / 1e9
+
+    line = {
+        "metric": "HBM GB/s (fused-gate statevector passes)",
+        "value": value,
+        "unit": "GB/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": args.precision,
+        "data": "synthetic",
+        "config": {
+            "workload": f"brickwork-{n}q-d{args.depth}-{'c128' if args.precision == 'f64' else 'c64'}-k{args.k}",
+            "n_qubits": n, "depth": args.depth, "fusion_k": args.k,
+            "unfused_gates": len(circ), "fused_gates": len(gates),
+            "statevector_bytes": (1 << n) * amp_bytes,
+            "l2": "no flush: the statevector is larger than L2",
+            "parallelism": f"replicas{ws}",
+        },
+        "gates_amps_per_s": ws * args.steps * len(gates) * (1 << n) / t,
+        "roofline": {
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "kernel": f"k_gate k={dom_k}",
+            "kernel_time_share": kernel_share, "peak_kind": peak_kind,
+        },
+        "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": n_launch,
+        "clocks": clk.summary(),
+        "wall_s_timed": wall,
+        "z_expectation_sample": [float(x) for x in zs[:4]] if zs is not None else None,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        n_cpu = min(n, args.cpu_n)
+        _, cgates = build_fused(n_cpu, args.depth, args.k)
+        gbs, passes, el = cpu_baseline_run(n_cpu, cgates, args.precision, args.cpu_budget, threads)
+        line["cpu_baseline"] = {
+            "value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"{passes} fused-gate passes of the {n_cpu}-qubit brickwork (k={args.k}) in {el:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

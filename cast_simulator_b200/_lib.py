@@ -85,8 +85,31 @@ FFI_CUDA = [
      [C.c_uint64, C.c_size_t, C.c_uint8, C.c_double, C.c_char_p, C.c_size_t]),
 ]
 
-# Extension entry points (include/cast_b200.h), bound when present.
-CAST_B200: list = []
+# Extension entry points (include/cast_b200.h).
+CAST_B200 = [
+    ("cast_b200_set_device", C.c_int, [C.c_int, C.c_char_p, C.c_size_t]),
+    ("cast_b200_set_gate_path", C.c_int, [C.c_int]),
+    ("cast_b200_apply_gate", C.c_int,
+     [C.c_uint64, C.c_uint32, C.c_uint8, C.POINTER(Complex64), c_u32p, C.c_uint32, C.c_double,
+      C.c_double, C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("cast_b200_program_create", C.c_void_p,
+     [C.c_uint8, C.c_uint32, C.c_double, C.c_double, C.c_char_p, C.c_size_t]),
+    ("cast_b200_program_add_gate", C.c_int,
+     [C.c_void_p, C.POINTER(Complex64), c_u32p, C.c_uint32, C.c_char_p, C.c_size_t]),
+    ("cast_b200_program_num_gates", C.c_uint32, [C.c_void_p]),
+    ("cast_b200_program_run", C.c_int,
+     [C.c_void_p, C.c_uint64, C.c_void_p, C.c_int, C.c_char_p, C.c_size_t]),
+    ("cast_b200_program_destroy", None, [C.c_void_p]),
+    ("cast_b200_inner_product", C.c_int,
+     [C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint8, c_dp, c_dp, C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("cast_b200_qubit_populations", C.c_int,
+     [C.c_uint64, C.c_uint32, C.c_uint8, c_dp, c_dp, C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("cast_b200_marginal_probabilities", C.c_int,
+     [C.c_uint64, C.c_uint32, C.c_uint8, c_u32p, C.c_uint32, c_dp, C.c_void_p, C.c_char_p,
+      C.c_size_t]),
+    ("cast_b200_dm_populations", C.c_int,
+     [C.c_uint64, C.c_uint32, C.c_uint8, c_dp, C.c_void_p, C.c_char_p, C.c_size_t]),
+]
 
 
 def lib():

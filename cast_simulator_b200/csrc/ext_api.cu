@@ -1,0 +1,310 @@
+// Extension C ABI (include/cast_b200.h): one-call gate application, gate
+// programs replayed through CUDA graphs, and FP64 reductions.
+#include "../../include/cast_b200.h"
+#include "internal.hpp"
+
+#include <exception>
+#include <map>
+#include <mutex>
+#include <utility>
+
+using cb2::clear_err;
+using cb2::cuda_ok;
+using cb2::GateData;
+using cb2::write_err;
+
+namespace {
+
+constexpr uint32_t kProgramMagic = 0xCB2009A1u;
+
+bool make_gate(uint8_t precision, const cast_complex64_t *matrix, const uint32_t *qubits,
+               uint32_t k, double ztol, double otol, GateData &g, std::string &err) {
+  if (!matrix || !qubits) {
+    err = "matrix and qubits must not be null";
+    return false;
+  }
+  if (precision > 1) {
+    err = "precision must be 0 (F32) or 1 (F64)";
+    return false;
+  }
+  if (k == 0 || k > cb2::kMaxGateQubits) {
+    err = "gate must act on 1.." + std::to_string(cb2::kMaxGateQubits) + " qubits";
+    return false;
+  }
+  g.k = k;
+  g.precision = precision;
+  for (uint32_t b = 0; b < k; ++b) {
+    g.qubits[b] = qubits[b];
+    if (b && qubits[b - 1] >= qubits[b]) {
+      err = "qubits must be distinct and ascending";
+      return false;
+    }
+  }
+  cb2::snap_matrix(g, reinterpret_cast<const double *>(matrix), ztol, otol);
+  return true;
+}
+
+struct Program {
+  uint32_t magic = kProgramMagic;
+  uint8_t precision = 1;
+  uint32_t n = 0;
+  double ztol = 0, otol = 0;
+  std::vector<GateData> gates;
+  std::map<std::pair<uint64_t, void *>, cudaGraphExec_t> graphs;
+  std::mutex mu;
+
+  ~Program() {
+    for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+    for (auto &g : gates)
+      if (g.d_mat) cudaFree(g.d_mat);
+  }
+
+  void drop_graphs() {
+    for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+    graphs.clear();
+  }
+
+  bool launch_all(uint64_t sv, cudaStream_t s, std::string &err) {
+    for (auto &g : gates)
+      if (!cb2::launch_gate(g, reinterpret_cast<void *>(sv), n, s, err)) return false;
+    return true;
+  }
+};
+
+Program *as_program(void *p) {
+  Program *pr = static_cast<Program *>(p);
+  return pr && pr->magic == kProgramMagic ? pr : nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cast_b200_set_device(int device, char *err_buf, size_t err_buf_len) {
+  std::string err;
+  if (!cuda_ok(cudaSetDevice(device), "cudaSetDevice", err)) {
+    write_err(err_buf, err_buf_len, err);
+    return 1;
+  }
+  clear_err(err_buf, err_buf_len);
+  return 0;
+}
+
+int cast_b200_set_gate_path(int path) { return cb2::set_gate_path(path); }
+
+int cast_b200_apply_gate(uint64_t sv_dptr, uint32_t sv_n_qubits, uint8_t precision,
+                         const cast_complex64_t *matrix, const uint32_t *qubits,
+                         uint32_t n_gate_qubits, double ztol, double otol, void *stream,
+                         char *err_buf, size_t err_buf_len) {
+  try {
+    GateData g;
+    std::string err;
+    if (!make_gate(precision, matrix, qubits, n_gate_qubits, ztol, otol, g, err) ||
+        !cb2::check_gate(g, sv_n_qubits, err)) {
+      write_err(err_buf, err_buf_len, err);
+      return 1;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    bool ok;
+    if (g.k >= 6) {
+      ok = cb2::upload_gate_matrix(g, err) &&
+           cb2::launch_gate(g, reinterpret_cast<void *>(sv_dptr), sv_n_qubits, s, err) &&
+           cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize", err);
+      if (g.d_mat) cudaFree(g.d_mat);
+    } else {
+      ok = cb2::launch_gate(g, reinterpret_cast<void *>(sv_dptr), sv_n_qubits, s, err);
+    }
+    if (!ok) {
+      write_err(err_buf, err_buf_len, err);
+      return 1;
+    }
+    clear_err(err_buf, err_buf_len);
+    return 0;
+  } catch (const std::exception &ex) {
+    write_err(err_buf, err_buf_len, ex.what());
+    return 1;
+  }
+}
+
+void *cast_b200_program_create(uint8_t precision, uint32_t sv_n_qubits, double ztol, double otol,
+                               char *err_buf, size_t err_buf_len) {
+  if (precision > 1 || sv_n_qubits == 0 || sv_n_qubits > cb2::kMaxSvQubits) {
+    write_err(err_buf, err_buf_len, "invalid precision or statevector size");
+    return nullptr;
+  }
+  try {
+    Program *p = new Program;
+    p->precision = precision;
+    p->n = sv_n_qubits;
+    p->ztol = ztol;
+    p->otol = otol;
+    clear_err(err_buf, err_buf_len);
+    return p;
+  } catch (const std::exception &ex) {
+    write_err(err_buf, err_buf_len, ex.what());
+    return nullptr;
+  }
+}
+
+int cast_b200_program_add_gate(void *program, const cast_complex64_t *matrix,
+                               const uint32_t *qubits, uint32_t n_gate_qubits, char *err_buf,
+                               size_t err_buf_len) {
+  Program *p = as_program(program);
+  if (!p) {
+    write_err(err_buf, err_buf_len, "invalid program handle");
+    return 1;
+  }
+  try {
+    GateData g;
+    std::string err;
+    if (!make_gate(p->precision, matrix, qubits, n_gate_qubits, p->ztol, p->otol, g, err) ||
+        !cb2::check_gate(g, p->n, err) || (g.k >= 6 && !cb2::upload_gate_matrix(g, err))) {
+      write_err(err_buf, err_buf_len, err);
+      return 1;
+    }
+    std::lock_guard<std::mutex> lock(p->mu);
+    p->drop_graphs();
+    p->gates.push_back(std::move(g));
+    clear_err(err_buf, err_buf_len);
+    return 0;
+  } catch (const std::exception &ex) {
+    write_err(err_buf, err_buf_len, ex.what());
+    return 1;
+  }
+}
+
+uint32_t cast_b200_program_num_gates(const void *program) {
+  const Program *p = static_cast<const Program *>(program);
+  return p && p->magic == kProgramMagic ? (uint32_t)p->gates.size() : 0;
+}
+
+int cast_b200_program_run(void *program, uint64_t sv_dptr, void *stream, int use_graph,
+                          char *err_buf, size_t err_buf_len) {
+  Program *p = as_program(program);
+  if (!p || !sv_dptr) {
+    write_err(err_buf, err_buf_len, "invalid program handle or statevector");
+    return 1;
+  }
+  try {
+    std::lock_guard<std::mutex> lock(p->mu);
+    std::string err;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!use_graph || !s || p->gates.empty()) {
+      if (!p->launch_all(sv_dptr, s, err)) {
+        write_err(err_buf, err_buf_len, err);
+        return 1;
+      }
+      clear_err(err_buf, err_buf_len);
+      return 0;
+    }
+    auto key = std::make_pair(sv_dptr, stream);
+    auto it = p->graphs.find(key);
+    if (it == p->graphs.end()) {
+      cudaGraph_t graph = nullptr;
+      cudaGraphExec_t exec = nullptr;
+      if (!cuda_ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal),
+                   "cudaStreamBeginCapture", err)) {
+        write_err(err_buf, err_buf_len, err);
+        return 1;
+      }
+      const bool launched = p->launch_all(sv_dptr, s, err);
+      const cudaError_t end_rc = cudaStreamEndCapture(s, &graph);
+      if (!launched || !cuda_ok(end_rc, "cudaStreamEndCapture", err) ||
+          !cuda_ok(cudaGraphInstantiate(&exec, graph, 0), "cudaGraphInstantiate", err)) {
+        if (graph) cudaGraphDestroy(graph);
+        write_err(err_buf, err_buf_len, err);
+        return 1;
+      }
+      cudaGraphDestroy(graph);
+      it = p->graphs.emplace(key, exec).first;
+    }
+    if (!cuda_ok(cudaGraphLaunch(it->second, s), "cudaGraphLaunch", err)) {
+      write_err(err_buf, err_buf_len, err);
+      return 1;
+    }
+    clear_err(err_buf, err_buf_len);
+    return 0;
+  } catch (const std::exception &ex) {
+    write_err(err_buf, err_buf_len, ex.what());
+    return 1;
+  }
+}
+
+void cast_b200_program_destroy(void *program) {
+  Program *p = as_program(program);
+  if (!p) return;
+  p->magic = 0;
+  delete p;
+}
+
+int cast_b200_inner_product(uint64_t a_dptr, uint64_t b_dptr, uint32_t n_qubits,
+                            uint8_t precision, double *out_re, double *out_im, void *stream,
+                            char *err_buf, size_t err_buf_len) {
+  std::string err;
+  if (!out_re || !out_im || !a_dptr || !b_dptr) {
+    write_err(err_buf, err_buf_len, "arguments must not be null");
+    return 1;
+  }
+  if (!cb2::inner_product(reinterpret_cast<const void *>(a_dptr),
+                          reinterpret_cast<const void *>(b_dptr), n_qubits, precision, out_re,
+                          out_im, static_cast<cudaStream_t>(stream), err)) {
+    write_err(err_buf, err_buf_len, err);
+    return 1;
+  }
+  clear_err(err_buf, err_buf_len);
+  return 0;
+}
+
+int cast_b200_qubit_populations(uint64_t sv_dptr, uint32_t n_qubits, uint8_t precision,
+                                double *out_p1, double *out_norm, void *stream, char *err_buf,
+                                size_t err_buf_len) {
+  std::string err;
+  if (!out_p1 || !sv_dptr) {
+    write_err(err_buf, err_buf_len, "arguments must not be null");
+    return 1;
+  }
+  if (!cb2::qubit_populations(reinterpret_cast<const void *>(sv_dptr), n_qubits, precision, out_p1,
+                              out_norm, static_cast<cudaStream_t>(stream), err)) {
+    write_err(err_buf, err_buf_len, err);
+    return 1;
+  }
+  clear_err(err_buf, err_buf_len);
+  return 0;
+}
+
+int cast_b200_marginal_probabilities(uint64_t sv_dptr, uint32_t n_qubits, uint8_t precision,
+                                     const uint32_t *measured, uint32_t n_measured,
+                                     double *out_probs, void *stream, char *err_buf,
+                                     size_t err_buf_len) {
+  std::string err;
+  if (!out_probs || !measured || !sv_dptr) {
+    write_err(err_buf, err_buf_len, "arguments must not be null");
+    return 1;
+  }
+  if (!cb2::marginal_probabilities(reinterpret_cast<const void *>(sv_dptr), n_qubits, precision,
+                                   measured, n_measured, out_probs,
+                                   static_cast<cudaStream_t>(stream), err)) {
+    write_err(err_buf, err_buf_len, err);
+    return 1;
+  }
+  clear_err(err_buf, err_buf_len);
+  return 0;
+}
+
+int cast_b200_dm_populations(uint64_t rho_dptr, uint32_t n_physical, uint8_t precision,
+                             double *out, void *stream, char *err_buf, size_t err_buf_len) {
+  std::string err;
+  if (!out || !rho_dptr) {
+    write_err(err_buf, err_buf_len, "arguments must not be null");
+    return 1;
+  }
+  if (!cb2::dm_populations(reinterpret_cast<const void *>(rho_dptr), n_physical, precision, out,
+                           static_cast<cudaStream_t>(stream), err)) {
+    write_err(err_buf, err_buf_len, err);
+    return 1;
+  }
+  clear_err(err_buf, err_buf_len);
+  return 0;
+}
+
+}  // extern "C"

@@ -170,7 +170,13 @@ bool parse_descriptor(const char *text, GateData &g, std::string &err) {
   return true;
 }
 
-bool upload_matrix(GateData &g, std::string &err) {
+size_t scalar_bytes(uint8_t precision) { return precision == 0 ? sizeof(float) : sizeof(double); }
+
+}  // namespace
+
+// Shared with the extension TU (cast_b200_*): module -> gate.
+namespace cb2 {
+bool upload_gate_matrix(GateData &g, std::string &err) {
   const size_t ns = g.m64.size();
   const size_t bytes = ns * (g.precision ? sizeof(double) : sizeof(float));
   if (!cuda_ok(cudaMalloc(&g.d_mat, bytes), "cudaMalloc (gate matrix)", err)) return false;
@@ -184,12 +190,7 @@ bool upload_matrix(GateData &g, std::string &err) {
   return true;
 }
 
-size_t scalar_bytes(uint8_t precision) { return precision == 0 ? sizeof(float) : sizeof(double); }
 
-}  // namespace
-
-// Shared with the extension TU (cast_b200_*): module -> gate.
-namespace cb2 {
 const GateData *module_gate(const void *fn_or_module) {
   if (!fn_or_module) return nullptr;
   const uint32_t magic = *static_cast<const uint32_t *>(fn_or_module);
@@ -401,7 +402,7 @@ void *cast_cuda_cubin_load(const uint8_t *cubin_data, size_t cubin_len, char *er
     std::memcpy(m->gate.m64.data(), cubin_data + sizeof(h), h.n_scalars * sizeof(double));
     m->gate.m32.resize(h.n_scalars);
     for (size_t i = 0; i < h.n_scalars; ++i) m->gate.m32[i] = (float)m->gate.m64[i];
-    if (!upload_matrix(m->gate, err)) {
+    if (!cb2::upload_gate_matrix(m->gate, err)) {
       delete m;
       write_err(err_buf, err_buf_len, err);
       return nullptr;

@@ -28,6 +28,9 @@
 #include "internal.hpp"
 
 #include <algorithm>
+#include <atomic>
+#include <cstdlib>
+#include <cstring>
 #include <mutex>
 
 namespace cb2 {
@@ -113,6 +116,101 @@ __global__ void __launch_bounds__(kRegThreads) k_gate_reg(T *__restrict__ sv, ui
       psi[base[u] + member_offset<K>(r, t)] = o;
     }
   }
+}
+
+// Tile kernel for gates with targets among the low (intra-cache-line) qubits.
+// A CTA owns one tile: the 2^(tb + k_hi) amplitudes whose "outer" bits are
+// fixed, i.e. 2^k_hi chunks (one per combination of the targets >= tb) of
+// 2^tb contiguous amplitudes.  The chunks are read and written with fully
+// coalesced 128/64-bit accesses; the gate is applied inside shared memory,
+// where the tile-local layout puts the high targets at bits tb..tb+k_hi-1.
+// Shared memory is XOR-swizzled inside each 128-byte block so that both the
+// contiguous phases and the strided gather of group members avoid bank
+// conflicts.
+template <int K> struct TileThreads { static constexpr int N = K <= 2 ? 256 : 128; };
+constexpr int kTileMaxChunks = 1 << kMaxGateQubits;
+
+struct TileArgs {
+  uint64_t hi_lo_mask[kMaxGateQubits];   // (1 << hq_j) - 1 for the high targets
+  uint64_t chunk_off[kTileMaxChunks];    // chunk c -> sum_j bit_j(c) << hq_j
+  uint32_t loc_lo_mask[kMaxGateQubits];  // tile-local target positions (ascending) as masks
+  uint32_t tb;                           // contiguous low bits per chunk
+  uint32_t k_hi;                         // number of high targets
+};
+
+template <int LOGE>
+__device__ __forceinline__ uint32_t swz(uint32_t i) {
+  return i ^ ((i >> LOGE) & ((1u << LOGE) - 1));
+}
+
+constexpr uint32_t kTileBits = 11;  // 2048 amplitudes per tile: 32 KB (f64) / 16 KB (f32)
+
+template <typename T, int K>
+__global__ void __launch_bounds__(TileThreads<K>::N) k_gate_tile(T *__restrict__ sv, TileArgs a,
+                                                                 MatParam<T, K> M) {
+  constexpr int kTileThreads = TileThreads<K>::N;
+  using V = typename Vec2<T>::type;
+  constexpr int D = 1 << K;
+  constexpr uint32_t TILE = 1u << kTileBits;
+  constexpr int LOGE = sizeof(V) == 16 ? 3 : 4;  // elements per 128-byte block
+  // groups per thread, fully unrolled (a runtime loop would let the compiler
+  // hoist the matrix out of the constant bank into registers)
+  constexpr int GPT = (int)((TILE >> K) + kTileThreads - 1) / kTileThreads;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V *s = reinterpret_cast<V *>(smem_raw);
+  V *psi = reinterpret_cast<V *>(sv);
+  const uint32_t low_mask = (1u << a.tb) - 1;
+  uint64_t tile_base = (uint64_t)blockIdx.x << a.tb;
+  for (uint32_t j = 0; j < a.k_hi; ++j)
+    tile_base = ((tile_base & ~a.hi_lo_mask[j]) << 1) | (tile_base & a.hi_lo_mask[j]);
+#pragma unroll 4
+  for (uint32_t i = threadIdx.x; i < TILE; i += kTileThreads)
+    s[swz<LOGE>(i)] = psi[tile_base + a.chunk_off[i >> a.tb] + (i & low_mask)];
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < GPT; ++u) {
+    const uint32_t gl = threadIdx.x + u * kTileThreads;
+    if (gl < (TILE >> K)) {
+      uint32_t base = gl;
+#pragma unroll
+      for (int b = 0; b < K; ++b)
+        base = ((base & ~a.loc_lo_mask[b]) << 1) | (base & a.loc_lo_mask[b]);
+      V x[D];
+#pragma unroll
+      for (int m = 0; m < D; ++m) {
+        uint32_t o = base;
+#pragma unroll
+        for (int b = 0; b < K; ++b)
+          if ((m >> b) & 1) o += a.loc_lo_mask[b] + 1;
+        x[m] = s[swz<LOGE>(o)];
+      }
+#pragma unroll
+      for (int r = 0; r < D; ++r) {
+        T re = T(0), im = T(0);
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+          const T mr = M.m[2 * (r * D + c)];
+          const T mi = M.m[2 * (r * D + c) + 1];
+          re = fma(mr, x[c].x, re);
+          re = fma(-mi, x[c].y, re);
+          im = fma(mr, x[c].y, im);
+          im = fma(mi, x[c].x, im);
+        }
+        V o;
+        o.x = re;
+        o.y = im;
+        uint32_t po = base;
+#pragma unroll
+        for (int b = 0; b < K; ++b)
+          if ((r >> b) & 1) po += a.loc_lo_mask[b] + 1;
+        s[swz<LOGE>(po)] = o;
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll 4
+  for (uint32_t i = threadIdx.x; i < TILE; i += kTileThreads)
+    psi[tile_base + a.chunk_off[i >> a.tb] + (i & low_mask)] = s[swz<LOGE>(i)];
 }
 
 // Staged kernel for k = 6, 7: tiles of G groups in shared memory.
@@ -204,6 +302,69 @@ bool launch_reg(const GateData &g, void *sv, uint32_t n, const Targets &t, cudaS
                  "gate kernel launch", err);
 }
 
+// Tile geometry for a gate: returns false when the tile kernel does not apply.
+bool tile_geometry(const GateData &g, uint32_t n, TileArgs &a) {
+  const uint32_t target = kTileBits;
+  if (n < target) return false;
+  uint32_t need = 0;  // every target below 5 must sit inside a chunk
+  for (uint32_t b = 0; b < g.k; ++b)
+    if (g.qubits[b] < 5) need = std::max(need, g.qubits[b] + 1);
+  need = std::max<uint32_t>(need, 5);
+  for (uint32_t tb = target; tb >= need; --tb) {
+    uint32_t khi = 0;
+    for (uint32_t b = 0; b < g.k; ++b) khi += g.qubits[b] >= tb;
+    if (tb + khi > target) continue;
+    a.tb = tb;
+    a.k_hi = khi;
+    uint32_t j = 0;
+    uint32_t hq[kMaxGateQubits] = {0};
+    for (uint32_t b = 0; b < g.k; ++b) {
+      if (g.qubits[b] >= tb) {
+        hq[j] = g.qubits[b];
+        a.hi_lo_mask[j] = (1ull << g.qubits[b]) - 1;
+        ++j;
+      }
+    }
+    // tile-local positions: low targets keep their bit, high target j -> tb + j
+    uint32_t h = 0;
+    for (uint32_t b = 0; b < g.k; ++b) {
+      const uint32_t pos = g.qubits[b] < tb ? g.qubits[b] : tb + h++;
+      a.loc_lo_mask[b] = (1u << pos) - 1;
+    }
+    for (uint32_t c = 0; c < (1u << khi); ++c) {
+      uint64_t o = 0;
+      for (uint32_t jj = 0; jj < khi; ++jj)
+        if ((c >> jj) & 1) o += 1ull << hq[jj];
+      a.chunk_off[c] = o;
+    }
+    return true;
+  }
+  return false;
+}
+
+template <typename T, int K>
+bool launch_tile(const GateData &g, void *sv, uint32_t n, const TileArgs &a, cudaStream_t s,
+                 std::string &err) {
+  using V = typename Vec2<T>::type;
+  static std::once_flag once;
+  static cudaError_t attr_rc = cudaSuccess;
+  std::call_once(once, [] {
+    attr_rc = cudaFuncSetAttribute(k_gate_tile<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(V) << kTileBits));
+  });
+  if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(tile gate kernel)", err)) return false;
+  const uint64_t n_tiles = 1ull << (n - kTileBits);
+  const size_t smem = sizeof(V) << kTileBits;
+  const MatParam<T, K> *mp;
+  if constexpr (sizeof(T) == 8) mp = reinterpret_cast<const MatParam<T, K> *>(g.m64.data());
+  else mp = reinterpret_cast<const MatParam<T, K> *>(g.m32.data());
+  T *p = static_cast<T *>(sv);
+  void *args[] = {&p, const_cast<TileArgs *>(&a), const_cast<MatParam<T, K> *>(mp)};
+  return cuda_ok(cudaLaunchKernel((const void *)k_gate_tile<T, K>, dim3((unsigned)n_tiles),
+                                  dim3(TileThreads<K>::N), args, smem, s),
+                 "tile gate kernel launch", err);
+}
+
 template <typename T, int K>
 bool launch_staged(const GateData &g, void *sv, uint32_t n, const Targets &t, cudaStream_t s,
                    std::string &err) {
@@ -231,9 +392,55 @@ bool launch_staged(const GateData &g, void *sv, uint32_t n, const Targets &t, cu
   return cuda_ok(cudaGetLastError(), "staged gate kernel launch", err);
 }
 
+// Path selection between the register and tile kernels (k <= 4);
+// CAST_B200_GATE_PATH=reg|tile forces one path for measurement.
+std::atomic<int> g_gate_path{[] {
+  const char *e = std::getenv("CAST_B200_GATE_PATH");
+  if (!e) return 0;
+  if (!std::strcmp(e, "reg")) return 1;
+  if (!std::strcmp(e, "tile")) return 2;
+  return 0;
+}()};
+
+int gate_path_override() { return g_gate_path.load(std::memory_order_relaxed); }
+
+template <typename T>
+bool try_tile(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::string &err,
+              bool &done) {
+  done = false;
+  if (g.k > 4) return true;
+  const int ov = gate_path_override();
+  if (ov == 1) return true;
+  // Measured on B200 (30 qubits): the register kernel loses 40-70% of its
+  // bandwidth once a warp's loads of one member touch 32 distinct cache lines
+  // (f64: targets {0,1,2} all present) or use 8 of every 32 sector bytes
+  // (f32: targets {0,1} both present); elsewhere it is at or above the tile
+  // kernel.
+  uint32_t low_bits = 0;
+  for (uint32_t b = 0; b < g.k; ++b)
+    if (g.qubits[b] < 5) low_bits |= 1u << g.qubits[b];
+  const uint32_t bad = g.precision == 1 ? 0x7u : 0x3u;
+  if (ov != 2 && (low_bits & bad) != bad) return true;
+  if (ov == 2 && low_bits == 0) return true;
+  TileArgs a;
+  std::memset(&a, 0, sizeof(a));
+  if (!tile_geometry(g, n, a)) return true;
+  done = true;
+  switch (g.k) {
+  case 1: return launch_tile<T, 1>(g, sv, n, a, s, err);
+  case 2: return launch_tile<T, 2>(g, sv, n, a, s, err);
+  case 3: return launch_tile<T, 3>(g, sv, n, a, s, err);
+  case 4: return launch_tile<T, 4>(g, sv, n, a, s, err);
+  default: done = false; return true;
+  }
+}
+
 template <typename T>
 bool launch_t(const GateData &g, void *sv, uint32_t n, const Targets &t, cudaStream_t s,
               std::string &err) {
+  bool done = false;
+  if (!try_tile<T>(g, sv, n, s, err, done)) return false;
+  if (done) return true;
   switch (g.k) {
   case 1: return launch_reg<T, 1>(g, sv, n, t, s, err);
   case 2: return launch_reg<T, 2>(g, sv, n, t, s, err);
@@ -247,6 +454,8 @@ bool launch_t(const GateData &g, void *sv, uint32_t n, const Targets &t, cudaStr
 }
 
 }  // namespace
+
+int set_gate_path(int path) { return g_gate_path.exchange(path < 0 || path > 2 ? 0 : path); }
 
 int sm_count() {
   std::call_once(g_sm_once, [] {

@@ -52,7 +52,23 @@ bool launch_gate(const GateData &g, void *sv, uint32_t n, cudaStream_t stream, s
 // 1/2^k and fills g.m64 / g.m32 (src/cpp/cuda/cuda_gen.cpp:84-103).
 void snap_matrix(GateData &g, const double *interleaved, double ztol, double otol);
 
-// Device helpers shared with the reduction TU.
+// Device helpers shared between translation units.
 int sm_count();
+int set_gate_path(int path);  // 0 auto, 1 register, 2 tile; returns previous
+bool upload_gate_matrix(GateData &g, std::string &err);  // fills g.d_mat
+
+// Reductions (reduce_kernels.cu): synchronous on `s`, except scale (enqueued).
+bool norm_squared(const void *x, uint64_t n_scalars, uint8_t precision, double *out,
+                  cudaStream_t s, std::string &err);
+bool scale(void *x, uint64_t n_scalars, uint8_t precision, double factor, cudaStream_t s,
+           std::string &err);
+bool inner_product(const void *a, const void *b, uint32_t n, uint8_t precision, double *re,
+                   double *im, cudaStream_t s, std::string &err);
+bool qubit_populations(const void *x, uint32_t n, uint8_t precision, double *p1, double *norm,
+                       cudaStream_t s, std::string &err);
+bool marginal_probabilities(const void *x, uint32_t n, uint8_t precision, const uint32_t *measured,
+                            uint32_t m, double *out, cudaStream_t s, std::string &err);
+bool dm_populations(const void *rho, uint32_t n, uint8_t precision, double *out, cudaStream_t s,
+                    std::string &err);
 
 }  // namespace cb2

@@ -12,6 +12,8 @@
 #include "internal.hpp"
 
 #include <mutex>
+#include <type_traits>
+#include <vector>
 
 namespace cb2 {
 
@@ -146,6 +148,211 @@ bool scale_impl(void *x, uint64_t n, double scale, cudaStream_t s, std::string &
   return cuda_ok(cudaGetLastError(), "scale kernel launch", err);
 }
 
+
+// <a|b> partials: (re, im) per block.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_inner_pass1(const T *__restrict__ a,
+                                                            const T *__restrict__ b, uint64_t n_amps,
+                                                            double *__restrict__ partial) {
+  using V = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+  const V *av = reinterpret_cast<const V *>(a);
+  const V *bv = reinterpret_cast<const V *>(b);
+  double re = 0, im = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * kRedThreads;
+  for (uint64_t i = (uint64_t)blockIdx.x * kRedThreads + threadIdx.x; i < n_amps; i += stride) {
+    const V x = av[i], y = bv[i];
+    re += (double)x.x * y.x + (double)x.y * y.y;
+    im += (double)x.x * y.y - (double)x.y * y.x;
+  }
+  re = block_sum(re);
+  __syncthreads();
+  im = block_sum(im);
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = re;
+    partial[2 * blockIdx.x + 1] = im;
+  }
+}
+
+// Sums `cols` interleaved columns of `rows` partial rows: out[c] = sum_r p[r*cols + c].
+__global__ void __launch_bounds__(kRedThreads) k_sum_columns(const double *__restrict__ p, int rows,
+                                                            int cols, double *__restrict__ out) {
+  for (int c = blockIdx.x; c < cols; c += gridDim.x) {
+    double acc = 0;
+    for (int r = threadIdx.x; r < rows; r += kRedThreads) acc += p[(size_t)r * cols + c];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) out[c] = acc;
+    __syncthreads();
+  }
+}
+
+constexpr int kMaxPopQubits = 40;
+
+// Per-qubit populations P(q = 1) and the total norm in one pass.  Each thread
+// walks 8-amplitude chunks: the chunk's high index bits are constant, so the
+// chunk sum is added once per high qubit; the 3 low bits are split per amp.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_populations(const T *__restrict__ x, uint32_t n,
+                                                            double *__restrict__ partial) {
+  using V = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+  const V *xv = reinterpret_cast<const V *>(x);
+  const uint64_t n_amps = 1ull << n;
+  const uint32_t cb = n < 3 ? n : 3;  // chunk bits
+  const uint64_t n_chunks = n_amps >> cb;
+  double acc[kMaxPopQubits + 1];
+#pragma unroll
+  for (int q = 0; q <= kMaxPopQubits; ++q) acc[q] = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * kRedThreads;
+  for (uint64_t c = (uint64_t)blockIdx.x * kRedThreads + threadIdx.x; c < n_chunks; c += stride) {
+    double lo[3] = {0, 0, 0}, tot = 0;
+    for (uint32_t j = 0; j < (1u << cb); ++j) {
+      const V v = xv[(c << cb) + j];
+      const double p = (double)v.x * v.x + (double)v.y * v.y;
+      tot += p;
+      if (j & 1) lo[0] += p;
+      if (j & 2) lo[1] += p;
+      if (j & 4) lo[2] += p;
+    }
+    acc[kMaxPopQubits] += tot;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) acc[q] += lo[q];
+#pragma unroll
+    for (int q = 3; q < kMaxPopQubits; ++q)
+      if ((uint32_t)q < n && ((c >> (q - 3)) & 1)) acc[q] += tot;
+  }
+  __shared__ double red[kRedThreads / 32];
+#pragma unroll
+  for (int q = 0; q <= kMaxPopQubits; ++q) {
+    if (q < (int)n || q == kMaxPopQubits) {
+      double v = warp_sum(acc[q]);
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double t = 0;
+        for (int w = 0; w < kRedThreads / 32; ++w) t += red[w];
+        partial[(size_t)blockIdx.x * (kMaxPopQubits + 1) + q] = t;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Marginal probabilities over m measured qubits: per-block bins in shared
+// memory (FP64 shared atomics), written as per-block partial rows.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_marginal(const T *__restrict__ x, uint32_t n,
+                                                         const uint32_t *__restrict__ measured,
+                                                         uint32_t m, double *__restrict__ partial) {
+  using V = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+  extern __shared__ double bins[];
+  const uint32_t nb = 1u << m;
+  for (uint32_t i = threadIdx.x; i < nb; i += kRedThreads) bins[i] = 0;
+  __shared__ uint32_t mq[16];
+  if (threadIdx.x < m) mq[threadIdx.x] = measured[threadIdx.x];
+  __syncthreads();
+  const V *xv = reinterpret_cast<const V *>(x);
+  const uint64_t n_amps = 1ull << n;
+  const uint64_t stride = (uint64_t)gridDim.x * kRedThreads;
+  for (uint64_t i = (uint64_t)blockIdx.x * kRedThreads + threadIdx.x; i < n_amps; i += stride) {
+    const V v = xv[i];
+    uint32_t bin = 0;
+    for (uint32_t j = 0; j < m; ++j) bin |= (uint32_t)((i >> mq[j]) & 1) << j;
+    atomicAdd(&bins[bin], (double)v.x * v.x + (double)v.y * v.y);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nb; i += kRedThreads)
+    partial[(size_t)blockIdx.x * nb + i] = bins[i];
+}
+
+template <typename T>
+__global__ void k_dm_diag(const T *__restrict__ rho, uint32_t n, double *__restrict__ out) {
+  const uint64_t dim = 1ull << n;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < dim;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = (double)rho[2 * (i | (i << n))];
+}
+
+template <typename T>
+bool inner_impl(const void *a, const void *b, uint32_t n, double *re, double *im, cudaStream_t s,
+                std::string &err) {
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  const uint64_t amps = 1ull << n;
+  const unsigned grid = red_grid(amps);
+  if (!ensure_scratch(2 * (int)grid + 2, err)) return false;
+  k_inner_pass1<T><<<grid, kRedThreads, 0, s>>>(static_cast<const T *>(a), static_cast<const T *>(b),
+                                                 amps, g_scratch);
+  k_sum_columns<<<2, kRedThreads, 0, s>>>(g_scratch, (int)grid, 2, g_scratch + 2 * grid);
+  double host[2];
+  if (!cuda_ok(cudaGetLastError(), "inner product launch", err) ||
+      !cuda_ok(cudaMemcpyAsync(host, g_scratch + 2 * grid, 16, cudaMemcpyDeviceToHost, s),
+               "cudaMemcpyAsync (inner product)", err) ||
+      !cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize (inner product)", err))
+    return false;
+  *re = host[0];
+  *im = host[1];
+  return true;
+}
+
+template <typename T>
+bool pop_impl(const void *x, uint32_t n, double *p1, double *norm, cudaStream_t s,
+              std::string &err) {
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  const uint64_t chunks = (1ull << n) >> (n < 3 ? n : 3);
+  const unsigned grid = std::min<unsigned>(red_grid(chunks), 2 * sm_count());
+  constexpr int W = kMaxPopQubits + 1;
+  if (!ensure_scratch(W * ((int)grid + 1), err)) return false;
+  cudaMemsetAsync(g_scratch, 0, sizeof(double) * W * grid, s);
+  k_populations<T><<<grid, kRedThreads, 0, s>>>(static_cast<const T *>(x), n, g_scratch);
+  k_sum_columns<<<W, kRedThreads, 0, s>>>(g_scratch, (int)grid, W, g_scratch + (size_t)W * grid);
+  std::vector<double> host(W);
+  if (!cuda_ok(cudaGetLastError(), "populations launch", err) ||
+      !cuda_ok(cudaMemcpyAsync(host.data(), g_scratch + (size_t)W * grid, sizeof(double) * W,
+                               cudaMemcpyDeviceToHost, s),
+               "cudaMemcpyAsync (populations)", err) ||
+      !cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize (populations)", err))
+    return false;
+  for (uint32_t q = 0; q < n; ++q) p1[q] = host[q];
+  if (norm) *norm = host[kMaxPopQubits];
+  return true;
+}
+
+template <typename T>
+bool marg_impl(const void *x, uint32_t n, const uint32_t *measured, uint32_t m, double *out,
+               cudaStream_t s, std::string &err) {
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  const uint32_t nb = 1u << m;
+  const unsigned grid = std::min<unsigned>(red_grid(1ull << n), 2 * sm_count());
+  const int need = (int)(nb * (grid + 1)) + 16;
+  if (!ensure_scratch(need, err)) return false;
+  uint32_t *dq = reinterpret_cast<uint32_t *>(g_scratch + (size_t)nb * (grid + 1));
+  if (!cuda_ok(cudaMemcpyAsync(dq, measured, sizeof(uint32_t) * m, cudaMemcpyHostToDevice, s),
+               "cudaMemcpyAsync (measured qubits)", err))
+    return false;
+  k_marginal<T><<<grid, kRedThreads, sizeof(double) * nb, s>>>(static_cast<const T *>(x), n, dq, m,
+                                                              g_scratch);
+  k_sum_columns<<<std::min<uint32_t>(nb, 1024), kRedThreads, 0, s>>>(g_scratch, (int)grid, (int)nb,
+                                                                      g_scratch + (size_t)nb * grid);
+  return cuda_ok(cudaGetLastError(), "marginal launch", err) &&
+         cuda_ok(cudaMemcpyAsync(out, g_scratch + (size_t)nb * grid, sizeof(double) * nb,
+                                 cudaMemcpyDeviceToHost, s),
+                 "cudaMemcpyAsync (marginal)", err) &&
+         cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize (marginal)", err);
+}
+
+template <typename T>
+bool dm_impl(const void *rho, uint32_t n, double *out, cudaStream_t s, std::string &err) {
+  double *d = nullptr;
+  const size_t bytes = sizeof(double) << n;
+  if (!cuda_ok(cudaMallocAsync(&d, bytes, s), "cudaMallocAsync (dm diagonal)", err)) return false;
+  const uint64_t dim = 1ull << n;
+  const unsigned grid = (unsigned)std::min<uint64_t>((dim + 255) / 256, 4ull * sm_count());
+  k_dm_diag<T><<<grid, 256, 0, s>>>(static_cast<const T *>(rho), n, d);
+  const bool ok = cuda_ok(cudaGetLastError(), "dm diagonal launch", err) &&
+                  cuda_ok(cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, s),
+                          "cudaMemcpyAsync (dm diagonal)", err);
+  cudaFreeAsync(d, s);
+  return ok && cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize (dm diagonal)", err);
+}
+
 }  // namespace
 
 bool norm_squared(const void *x, uint64_t n_scalars, uint8_t precision, double *out,
@@ -158,6 +365,46 @@ bool scale(void *x, uint64_t n_scalars, uint8_t precision, double factor, cudaSt
            std::string &err) {
   return precision == 0 ? scale_impl<float>(x, n_scalars, factor, s, err)
                         : scale_impl<double>(x, n_scalars, factor, s, err);
+}
+
+bool inner_product(const void *a, const void *b, uint32_t n, uint8_t precision, double *re,
+                   double *im, cudaStream_t s, std::string &err) {
+  return precision == 0 ? inner_impl<float>(a, b, n, re, im, s, err)
+                        : inner_impl<double>(a, b, n, re, im, s, err);
+}
+
+bool qubit_populations(const void *x, uint32_t n, uint8_t precision, double *p1, double *norm,
+                       cudaStream_t s, std::string &err) {
+  if (n > kMaxPopQubits) {
+    err = "populations support at most 40 qubits";
+    return false;
+  }
+  return precision == 0 ? pop_impl<float>(x, n, p1, norm, s, err)
+                        : pop_impl<double>(x, n, p1, norm, s, err);
+}
+
+bool marginal_probabilities(const void *x, uint32_t n, uint8_t precision, const uint32_t *measured,
+                            uint32_t m, double *out, cudaStream_t s, std::string &err) {
+  if (m == 0 || m > 12) {
+    err = "between 1 and 12 measured qubits are supported";
+    return false;
+  }
+  for (uint32_t j = 0; j < m; ++j)
+    if (measured[j] >= n) {
+      err = "measured qubit out of range";
+      return false;
+    }
+  return precision == 0 ? marg_impl<float>(x, n, measured, m, out, s, err)
+                        : marg_impl<double>(x, n, measured, m, out, s, err);
+}
+
+bool dm_populations(const void *rho, uint32_t n, uint8_t precision, double *out, cudaStream_t s,
+                    std::string &err) {
+  if (2 * n > kMaxSvQubits) {
+    err = "density matrix too large";
+    return false;
+  }
+  return precision == 0 ? dm_impl<float>(rho, n, out, s, err) : dm_impl<double>(rho, n, out, s, err);
 }
 
 }  // namespace cb2

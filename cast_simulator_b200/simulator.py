@@ -1,0 +1,306 @@
+"""Simulator API: host-side mirror of src/simulator/{mod,bench,measure}.rs.
+
+``Simulator`` (mod.rs:446-547) owns the precision / tolerance spec and runs a
+``CircuitGraph``: ``simulate`` returns a ``QuantumState`` for the state-vector
+or density-matrix representation (mod.rs:523-547, prepare_gates at
+mod.rs:586-613); ``bench`` compiles once and times repeated executions with
+device events (bench.rs:136-167, timing.rs:88-130).  Gates go to the GPU as a
+``GateProgram`` (include/cast_b200.h), replayed as a CUDA graph.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+from .cuda import CudaKernelGenSpec, CudaPrecision, CudaStatevector
+from .fusion import CircuitGraph
+
+
+class Representation(enum.Enum):
+    StateVector = 0
+    DensityMatrix = 1
+
+
+class Stream:
+    """An owned CUDA stream (cast_cuda_stream_create)."""
+
+    def __init__(self):
+        eb = L.errbuf()
+        self.handle = L.check_ptr(L.lib().cast_cuda_stream_create(eb, L.ERR_LEN), eb, "stream")
+
+    def sync(self):
+        eb = L.errbuf()
+        L.check(L.lib().cast_cuda_stream_sync(self.handle, eb, L.ERR_LEN), eb, "stream sync")
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            try:
+                L.lib().cast_cuda_stream_destroy(h)
+            except Exception:
+                pass
+
+
+class Event:
+    def __init__(self):
+        eb = L.errbuf()
+        self.handle = L.check_ptr(L.lib().cast_cuda_event_create(eb, L.ERR_LEN), eb, "event")
+
+    def record(self, stream):
+        """Record on a Stream or on a raw stream handle."""
+        h = stream.handle if isinstance(stream, Stream) else stream
+        eb = L.errbuf()
+        L.check(L.lib().cast_cuda_event_record(self.handle, h, eb, L.ERR_LEN), eb, "record")
+
+    def elapsed_s(self, start: "Event") -> float:
+        eb = L.errbuf()
+        ms = C.c_float()
+        L.check(L.lib().cast_cuda_event_elapsed_ms(start.handle, self.handle, C.byref(ms), eb,
+                                                   L.ERR_LEN), eb, "elapsed")
+        return ms.value * 1e-3
+
+    def sync(self):
+        eb = L.errbuf()
+        L.check(L.lib().cast_cuda_event_synchronize(self.handle, eb, L.ERR_LEN), eb, "event sync")
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            try:
+                L.lib().cast_cuda_event_destroy(h)
+            except Exception:
+                pass
+
+
+class GateProgram:
+    """Ordered gates for one statevector size, uploaded once (cast_b200_program_*)."""
+
+    def __init__(self, precision: CudaPrecision, n_qubits: int, ztol: float, otol: float):
+        eb = L.errbuf()
+        self.handle = L.check_ptr(
+            L.lib().cast_b200_program_create(int(precision), n_qubits, ztol, otol, eb, L.ERR_LEN), eb,
+            "program_create")
+        self.n_qubits = n_qubits
+        self.precision = CudaPrecision(precision)
+        self.gate_sizes: list[int] = []
+
+    def add(self, matrix: np.ndarray, qubits) -> None:
+        m = np.ascontiguousarray(matrix, dtype=np.complex128)
+        q = np.ascontiguousarray(qubits, dtype=np.uint32)
+        eb = L.errbuf()
+        L.check(L.lib().cast_b200_program_add_gate(
+            self.handle, m.view(np.float64).ctypes.data_as(C.POINTER(L.Complex64)),
+            q.ctypes.data_as(L.c_u32p), q.size, eb, L.ERR_LEN), eb, "program_add_gate")
+        self.gate_sizes.append(int(q.size))
+
+    def __len__(self):
+        return int(L.lib().cast_b200_program_num_gates(self.handle))
+
+    def run(self, sv: CudaStatevector, stream: Stream | None = None, use_graph: bool = True) -> None:
+        if sv.n_qubits() != self.n_qubits or sv.precision() != self.precision:
+            raise ValueError("statevector does not match the program")
+        eb = L.errbuf()
+        L.check(L.lib().cast_b200_program_run(self.handle, sv.dptr, stream.handle if stream else None,
+                                              int(use_graph), eb, L.ERR_LEN), eb, "program_run")
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            try:
+                L.lib().cast_b200_program_destroy(h)
+            except Exception:
+                pass
+
+
+def inner_product(a: CudaStatevector, b: CudaStatevector, stream: Stream | None = None) -> complex:
+    if a.n_qubits() != b.n_qubits() or a.precision() != b.precision():
+        raise ValueError("statevector size/precision mismatch")
+    re, im = C.c_double(), C.c_double()
+    eb = L.errbuf()
+    L.check(L.lib().cast_b200_inner_product(a.dptr, b.dptr, a.n_qubits(), int(a.precision()),
+                                            C.byref(re), C.byref(im),
+                                            stream.handle if stream else None, eb, L.ERR_LEN), eb,
+            "inner_product")
+    return complex(re.value, im.value)
+
+
+def qubit_populations(sv: CudaStatevector, stream: Stream | None = None) -> tuple[np.ndarray, float]:
+    """(P(q=1) for every qubit, norm^2), one FP64 device pass."""
+    out = np.zeros(sv.n_qubits())
+    nrm = C.c_double()
+    eb = L.errbuf()
+    L.check(L.lib().cast_b200_qubit_populations(sv.dptr, sv.n_qubits(), int(sv.precision()),
+                                                out.ctypes.data_as(L.c_dp), C.byref(nrm),
+                                                stream.handle if stream else None, eb, L.ERR_LEN),
+            eb, "qubit_populations")
+    return out, nrm.value
+
+
+def marginal_probabilities(sv: CudaStatevector, measured, stream: Stream | None = None) -> np.ndarray:
+    q = np.ascontiguousarray(measured, dtype=np.uint32)
+    out = np.zeros(1 << q.size)
+    eb = L.errbuf()
+    L.check(L.lib().cast_b200_marginal_probabilities(
+        sv.dptr, sv.n_qubits(), int(sv.precision()), q.ctypes.data_as(L.c_u32p), q.size,
+        out.ctypes.data_as(L.c_dp), stream.handle if stream else None, eb, L.ERR_LEN), eb,
+        "marginal_probabilities")
+    return out
+
+
+def prepare_gates(graph: CircuitGraph, n_physical: int, repr_: Representation):
+    """mod.rs:586-613: SV needs unitary gates; DM lifts each gate to a
+    superoperator on 2n virtual qubits."""
+    gates = graph.gates_in_row_order()
+    if repr_ == Representation.StateVector:
+        for i, g in enumerate(gates):
+            if not g.is_unitary():
+                raise ValueError(
+                    f"gate index {i} is non-unitary; Representation.StateVector requires unitary "
+                    "gates (use DensityMatrix or sample_trajectory for noisy circuits)")
+        return gates, n_physical
+    return [g.to_density_matrix_gate(n_physical) for g in gates], 2 * n_physical
+
+
+class QuantumState:
+    """mod.rs:320-414 (CUDA inspection methods)."""
+
+    def __init__(self, sv: CudaStatevector, n_physical: int, repr_: Representation):
+        self.sv, self._n, self._repr = sv, n_physical, repr_
+
+    def n_qubits(self) -> int:
+        return self._n
+
+    def is_pure(self) -> bool:
+        return self._repr == Representation.StateVector
+
+    def download_amplitudes(self) -> np.ndarray:
+        return self.sv.download()
+
+    def populations(self) -> np.ndarray:
+        if self.is_pure():
+            return np.abs(self.sv.download()) ** 2
+        out = np.zeros(1 << self._n)
+        eb = L.errbuf()
+        L.check(L.lib().cast_b200_dm_populations(self.sv.dptr, self._n, int(self.sv.precision()),
+                                                 out.ctypes.data_as(L.c_dp), None, eb, L.ERR_LEN),
+                eb, "dm_populations")
+        return out
+
+    def trace(self) -> float:
+        if self.is_pure():
+            return self.sv.norm_squared()
+        return float(self.populations().sum())
+
+    def expectation_z(self) -> np.ndarray:
+        """<Z_q> for every physical qubit (pure states), FP64 on the device."""
+        if not self.is_pure():
+            p = self.populations()
+            idx = np.arange(p.size)
+            return np.array([1 - 2 * p[(idx >> q) & 1 == 1].sum() for q in range(self._n)])
+        p1, nrm = qubit_populations(self.sv)
+        return (nrm - 2 * p1) / nrm
+
+
+@dataclass
+class PhaseTiming:
+    """bench.rs:42-110: raw samples of one phase (seconds)."""
+
+    samples_s: list = field(default_factory=list)
+    source: str = "gpu_events"
+
+    def mean_s(self):
+        return float(np.mean(self.samples_s)) if self.samples_s else 0.0
+
+    def stddev_s(self):
+        return float(np.std(self.samples_s, ddof=1)) if len(self.samples_s) > 1 else 0.0
+
+    def min_s(self):
+        return float(np.min(self.samples_s)) if self.samples_s else 0.0
+
+
+@dataclass
+class RunTiming:
+    compile: PhaseTiming
+    exec: PhaseTiming
+    n_gates: int
+    n_qubits: int
+
+
+class Simulator:
+    """Simulator<Cuda> (mod.rs:446-547)."""
+
+    def __init__(self, spec: CudaKernelGenSpec | None = None, use_graph: bool = True):
+        self.spec = spec or CudaKernelGenSpec.f64()
+        self.use_graph = use_graph
+        self._stream = None
+
+    @classmethod
+    def f64(cls) -> "Simulator":
+        return cls(CudaKernelGenSpec.f64())
+
+    @classmethod
+    def f32(cls) -> "Simulator":
+        return cls(CudaKernelGenSpec.f32())
+
+    @property
+    def stream(self) -> Stream:
+        if self._stream is None:
+            self._stream = Stream()
+        return self._stream
+
+    def compile_batch(self, gates, n_sv: int) -> GateProgram:
+        prog = GateProgram(self.spec.precision, n_sv, self.spec.ztol, self.spec.otol)
+        for i, g in enumerate(gates):
+            try:
+                prog.add(g.matrix(), g.qubits())
+            except L.CudaError as e:
+                raise L.CudaError(f"generating kernel for gate index {i}: {e}") from e
+        return prog
+
+    def simulate(self, graph: CircuitGraph, repr_: Representation = Representation.StateVector,
+                 initial: np.ndarray | None = None) -> QuantumState:
+        n_phys = graph.n_qubits()
+        gates, n_sv = prepare_gates(graph, n_phys, repr_)
+        prog = self.compile_batch(gates, n_sv)
+        sv = CudaStatevector(n_sv, self.spec.precision)
+        if initial is None:
+            sv.zero()
+        else:
+            sv.upload(initial)
+        prog.run(sv, self.stream, self.use_graph)
+        self.stream.sync()
+        return QuantumState(sv, n_phys, repr_)
+
+    def bench(self, graph: CircuitGraph, repr_: Representation = Representation.StateVector,
+              budget_s: float = 1.0, min_iters: int = 3) -> RunTiming:
+        """Compile once, then time zero + apply-all on the device until the
+        budget is spent (25% of it as warm-up, timing.rs:88-130)."""
+        n_phys = graph.n_qubits()
+        t0 = time.perf_counter()
+        gates, n_sv = prepare_gates(graph, n_phys, repr_)
+        prog = self.compile_batch(gates, n_sv)
+        comp = PhaseTiming([time.perf_counter() - t0], "wall")
+        sv = CudaStatevector(n_sv, self.spec.precision)
+        st = self.stream
+        e0, e1 = Event(), Event()
+
+        def one():
+            sv.zero()
+            e0.record(st)
+            prog.run(sv, st, self.use_graph)
+            e1.record(st)
+            e1.sync()
+            return e1.elapsed_s(e0)
+
+        probe = one()
+        n_total = max(min_iters, int(budget_s / max(probe, 1e-6)))
+        n_warm = max(1, n_total // 4)
+        for _ in range(n_warm):
+            one()
+        samples = [one() for _ in range(max(min_iters, n_total - n_warm))]
+        return RunTiming(comp, PhaseTiming(samples), len(prog), n_sv)

@@ -1,0 +1,92 @@
+/*
+ * Extension C ABI of libcast_b200.so: entry points with no counterpart in the
+ * reference's ffi_cuda.h, added beside it (the drop-in ABI is unchanged).
+ * Same conventions as ffi_cuda.h: int 0 = success / 1 = failure (NULL for
+ * handle-returning calls), message in err_buf, err_buf[0] = '\0' on success.
+ * Statevectors are device pointers to 2^n interleaved (re, im) amplitudes of
+ * the given precision (0 = F32, 1 = F64); gate matrices are host arrays of
+ * 4^k cast_complex64_t, row-major, with qubits ascending and qubits[b] = bit b
+ * of the matrix index (the reference convention, src/cpp/cuda/cuda_gen.cpp:241-246).
+ * Each entry names the reference code whose job it takes over.
+ */
+#ifndef CAST_B200_H
+#define CAST_B200_H
+
+#include "ffi_types.h"
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* -- Device selection -----------------------------------------------------------
+ * Makes `device` current for the calling thread in this library's CUDA runtime
+ * (one process per GPU).  The reference hard-wires device 0
+ * (src/cpp/cuda/cuda_exec.cpp:50). */
+int cast_b200_set_device(int device, char *err_buf, size_t err_buf_len);
+
+/* -- Kernel path control ------------------------------------------------------
+ * 0 = automatic (default), 1 = register kernel only, 2 = shared-memory tile
+ * kernel wherever it applies.  For measurement and tests; returns the previous
+ * setting.  No reference counterpart (the reference has one code generator). */
+int cast_b200_set_gate_path(int path);
+
+/* -- One-call gate application ------------------------------------------------
+ * Snap (ztol/otol scaled by 1/2^k, as cuda_gen.cpp:84-103) and apply one gate
+ * in place on `stream`.  Takes over the compile -> load -> launch sequence of
+ * CudaKernelManager::{generate,apply} (src/cuda/kernel.rs:778-924) for callers
+ * that hold the matrix as data.  k <= 7; for k >= 6 the matrix is staged in a
+ * device buffer owned by the library, so the call is synchronous. */
+int cast_b200_apply_gate(uint64_t sv_dptr, uint32_t sv_n_qubits, uint8_t precision,
+                         const cast_complex64_t *matrix, const uint32_t *qubits,
+                         uint32_t n_gate_qubits, double ztol, double otol, void *stream,
+                         char *err_buf, size_t err_buf_len);
+
+/* -- Gate programs ---------------------------------------------------------------
+ * An ordered list of gates for one statevector size and precision, uploaded
+ * once and replayed many times: the device-side analogue of the reference's
+ * compile_batch + apply-all + sync loop (src/simulator/mod.rs:523-562,
+ * src/simulator/bench.rs:136-167).  With use_graph != 0 the launches are
+ * captured once per (statevector, stream) into a CUDA graph and replayed. */
+void *cast_b200_program_create(uint8_t precision, uint32_t sv_n_qubits, double ztol, double otol,
+                               char *err_buf, size_t err_buf_len);
+int cast_b200_program_add_gate(void *program, const cast_complex64_t *matrix,
+                               const uint32_t *qubits, uint32_t n_gate_qubits, char *err_buf,
+                               size_t err_buf_len);
+uint32_t cast_b200_program_num_gates(const void *program);
+int cast_b200_program_run(void *program, uint64_t sv_dptr, void *stream, int use_graph,
+                          char *err_buf, size_t err_buf_len);
+void cast_b200_program_destroy(void *program);
+
+/* -- FP64 reductions ---------------------------------------------------------------
+ * <a|b> over 2^n amplitudes, FP64 accumulation; synchronous on `stream`.
+ * Replaces the host loop of CPUStatevector::fidelity (src/cpu/statevector.rs:363-374)
+ * for device states. */
+int cast_b200_inner_product(uint64_t a_dptr, uint64_t b_dptr, uint32_t n_qubits,
+                            uint8_t precision, double *out_re, double *out_im, void *stream,
+                            char *err_buf, size_t err_buf_len);
+/* out_p1[q] = P(qubit q = 1) for q < n (so <Z_q> = 1 - 2 out_p1[q]) and
+ * *out_norm = sum |a|^2, in one FP64 pass; synchronous. */
+int cast_b200_qubit_populations(uint64_t sv_dptr, uint32_t n_qubits, uint8_t precision,
+                                double *out_p1, double *out_norm, void *stream, char *err_buf,
+                                size_t err_buf_len);
+/* Marginal probabilities over `measured` qubits (bin index bit j = qubit
+ * measured[j]), 2^n_measured bins, FP64; replaces the download-then-bin of
+ * marginal_probabilities / accumulate_marginal_probs (src/simulator/mod.rs:282-291,
+ * src/simulator/measure.rs:15-41).  n_measured <= 12. */
+int cast_b200_marginal_probabilities(uint64_t sv_dptr, uint32_t n_qubits, uint8_t precision,
+                                     const uint32_t *measured, uint32_t n_measured,
+                                     double *out_probs, void *stream, char *err_buf,
+                                     size_t err_buf_len);
+/* Density-matrix diagonal: out[i] = Re rho[i | i << n] for the vectorised
+ * 2n-qubit state (QuantumState::populations / trace, src/simulator/mod.rs:387-413). */
+int cast_b200_dm_populations(uint64_t rho_dptr, uint32_t n_physical, uint8_t precision,
+                             double *out, void *stream, char *err_buf, size_t err_buf_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CAST_B200_H */
