@@ -109,6 +109,8 @@ CAST_B200 = [
       C.c_size_t]),
     ("cast_b200_dm_populations", C.c_int,
      [C.c_uint64, C.c_uint32, C.c_uint8, c_dp, C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("cast_b200_norm_squared_noalloc", C.c_int,
+     [C.c_uint64, C.c_size_t, C.c_uint8, c_dp, C.c_void_p, C.c_char_p, C.c_size_t]),
 ]
 
 

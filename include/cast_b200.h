@@ -85,6 +85,23 @@ int cast_b200_marginal_probabilities(uint64_t sv_dptr, uint32_t n_qubits, uint8_
 int cast_b200_dm_populations(uint64_t rho_dptr, uint32_t n_physical, uint8_t precision,
                              double *out, void *stream, char *err_buf, size_t err_buf_len);
 
+/* -- Allocation-free norm^2 -------------------------------------------------------
+ * No counterpart in the reference: an extra variant of cast_cuda_norm_squared
+ * for callers that cannot let a library allocate device memory (work recorded
+ * inside a CUDA stream capture, memory owned by a pool or arena that accounts
+ * for every byte, hosts that forbid allocations after start-up).  Same result
+ * (sum of squares of n_elements scalars, FP64 accumulation, written to the host
+ * double *out_norm_sq; synchronous on `stream`, NULL = legacy default stream),
+ * but the scratch is a fixed array inside the library (about 1 MiB per GPU,
+ * held until the process exits) and no memory is allocated.  Limit:
+ * n_elements <= 2^32 (F64) / 2^33 (F32), i.e. 32 GiB of amplitudes; larger
+ * inputs are rejected with an error.  The first call on each device resolves
+ * the array's device address (do it before any stream capture).  Calls whose
+ * kernels may overlap on the GPU share the array and race; order them. */
+int cast_b200_norm_squared_noalloc(uint64_t dptr, size_t n_elements, uint8_t precision,
+                                   double *out_norm_sq, void *stream, char *err_buf,
+                                   size_t err_buf_len);
+
 #ifdef __cplusplus
 }
 #endif
