@@ -109,6 +109,20 @@ CAST_B200 = [
       C.c_size_t]),
     ("cast_b200_dm_populations", C.c_int,
      [C.c_uint64, C.c_uint32, C.c_uint8, c_dp, C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("cast_b200_traj_create", C.c_void_p, [C.c_uint32, C.c_char_p, C.c_size_t]),
+    ("cast_b200_traj_destroy", None, [C.c_void_p]),
+    ("cast_b200_traj_add_gate", C.c_int,
+     [C.c_void_p, C.POINTER(Complex64), c_u32p, C.c_uint32, C.c_char_p, C.c_size_t]),
+    ("cast_b200_traj_add_pauli_error", C.c_int,
+     [C.c_void_p, C.c_double, C.POINTER(Complex64), C.c_char_p, C.c_size_t]),
+    ("cast_b200_traj_add_damping", C.c_int,
+     [C.c_void_p, C.c_uint32, C.c_double, C.c_char_p, C.c_size_t]),
+    ("cast_b200_traj_add_channel", C.c_int,
+     [C.c_void_p, C.c_uint32, C.POINTER(Complex64), C.c_uint32, C.c_char_p, C.c_size_t]),
+    ("cast_b200_traj_num_ops", C.c_uint32, [C.c_void_p]),
+    ("cast_b200_traj_run", C.c_int,
+     [C.c_void_p, C.c_uint32, C.c_uint64, c_dp, c_u32p, C.c_void_p, C.c_int, C.c_char_p,
+      C.c_size_t]),
     ("cast_b200_norm_squared_noalloc", C.c_int,
      [C.c_uint64, C.c_size_t, C.c_uint8, c_dp, C.c_void_p, C.c_char_p, C.c_size_t]),
 ]

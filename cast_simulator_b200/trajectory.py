@@ -1,0 +1,321 @@
+"""Batched noisy trajectories: host-side program builder and run API.
+
+Mirror of the reference's ``Simulator::sample_trajectory`` entry point
+(src/simulator/trajectory.rs:85-130: ``TrajectoryOpts`` with measured qubits,
+sample count and seed; a ``TrajectoryResult`` with a histogram), re-based on
+Monte-Carlo quantum-jump trajectories run in one persistent kernel
+(``cast_b200_traj_*`` in include/cast_b200.h).
+
+Program construction from a noisy ``QuantumCircuit``:
+  * unitary gates between non-Pauli noise operations form a segment that is
+    fused with the reference's planner (``fusion.optimize``, size_only(k));
+    every gate is tagged with its index, and fused blocks carry the tags of the
+    gates they contain in application order;
+  * a depolarizing (or bit/phase-flip) channel after gate j on qubit q becomes a
+    Pauli error attached to the block containing j, pre-propagated to the end of
+    the block: U_j P U_j^dagger with U_j the product of the block's gates after
+    j - so errors never split the fusion;
+  * consecutive single-qubit amplitude-damping channels with one rate become one
+    damping op on a qubit mask; any other single-qubit channel becomes a general
+    channel op.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+from .fusion import CircuitGraph, FusionConfig, optimize
+from .types import QuantumCircuit, QuantumGate, eye, expand_matrix, mat_x, mat_y, mat_z
+
+_PAULIS = (mat_x(), mat_y(), mat_z())
+
+
+def _is_pauli_channel(g: QuantumGate):
+    """(p, [matrices]) for depolarizing / bit-flip / phase-flip channels on an
+    identity base gate, else None."""
+    if g.is_unitary() or g.n_qubits() != 1 or not np.allclose(g.matrix(), eye(2)):
+        return None
+    br = g.noise_model().branches
+    if not np.allclose(br[0][1], eye(2)):
+        return None
+    errs = br[1:]
+    ps = [p for p, _ in errs]
+    mats = [m for _, m in errs]
+    for m in mats:
+        if not any(np.allclose(m, P) for P in _PAULIS):
+            return None
+    if len(errs) == 3 and np.allclose(ps, ps[0]):
+        return float(sum(ps)), mats
+    if len(errs) == 1:
+        return float(ps[0]), mats * 3
+    return None
+
+
+def _damping_rate(g: QuantumGate):
+    """gamma for an amplitude-damping channel in the weighted-Kraus form
+    (weights 1/2, operators sqrt(2) K0, sqrt(2) K1), else None."""
+    if g.is_unitary() or g.n_qubits() != 1 or not np.allclose(g.matrix(), eye(2)):
+        return None
+    br = g.noise_model().branches
+    if len(br) != 2:
+        return None
+    (p0, a), (p1, b) = br
+    k0 = math.sqrt(p0) * a
+    k1 = math.sqrt(p1) * b
+    if abs(k0[0, 1]) > 1e-12 or abs(k0[1, 0]) > 1e-12 or abs(k0[0, 0] - 1) > 1e-12:
+        return None
+    gamma = 1.0 - abs(k0[1, 1]) ** 2
+    exp1 = np.array([[0, math.sqrt(gamma)], [0, 0]])
+    if not np.allclose(k1, exp1, atol=1e-12):
+        return None
+    return gamma
+
+
+@dataclass
+class TrajectoryProgramStats:
+    n_blocks: int = 0
+    n_errors: int = 0
+    n_damping: int = 0
+    n_channels: int = 0
+    block_sizes: list = field(default_factory=list)
+
+
+class TrajectoryProgram:
+    def __init__(self, circuit: QuantumCircuit, fusion_k: int = 4):
+        if not 1 <= fusion_k <= 4:
+            raise ValueError("trajectory fusion width must be 1..4")
+        self.n = circuit.n_qubits()
+        eb = L.errbuf()
+        self.handle = L.check_ptr(L.lib().cast_b200_traj_create(self.n, eb, L.ERR_LEN), eb,
+                                  "traj_create")
+        self.stats = TrajectoryProgramStats()
+        self._k = fusion_k
+        self._build(circuit)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            try:
+                L.lib().cast_b200_traj_destroy(h)
+            except Exception:
+                pass
+
+    # -- C ABI helpers
+    def _add_gate(self, m, q):
+        m = np.ascontiguousarray(m, dtype=np.complex128)
+        qq = np.ascontiguousarray(q, dtype=np.uint32)
+        eb = L.errbuf()
+        L.check(L.lib().cast_b200_traj_add_gate(self.handle, m.view(np.float64).ctypes.data_as(
+            C.POINTER(L.Complex64)), qq.ctypes.data_as(L.c_u32p), qq.size, eb, L.ERR_LEN), eb,
+            "traj_add_gate")
+        self.stats.n_blocks += 1
+        self.stats.block_sizes.append(len(q))
+
+    def _add_error(self, p, mats):
+        m = np.ascontiguousarray(np.stack(mats), dtype=np.complex128)
+        eb = L.errbuf()
+        L.check(L.lib().cast_b200_traj_add_pauli_error(self.handle, p, m.view(np.float64).ctypes.data_as(
+            C.POINTER(L.Complex64)), eb, L.ERR_LEN), eb, "traj_add_pauli_error")
+        self.stats.n_errors += 1
+
+    def _add_damping(self, mask, gamma):
+        eb = L.errbuf()
+        L.check(L.lib().cast_b200_traj_add_damping(self.handle, mask, gamma, eb, L.ERR_LEN), eb,
+                "traj_add_damping")
+        self.stats.n_damping += 1
+
+    def _add_channel(self, q, kraus):
+        m = np.ascontiguousarray(np.stack(kraus), dtype=np.complex128)
+        eb = L.errbuf()
+        L.check(L.lib().cast_b200_traj_add_channel(self.handle, q, m.view(np.float64).ctypes.data_as(
+            C.POINTER(L.Complex64)), len(kraus), eb, L.ERR_LEN), eb, "traj_add_channel")
+        self.stats.n_channels += 1
+
+    # -- construction
+    def _flush(self, seg, markers):
+        if not seg:
+            return
+        g = CircuitGraph.from_gates(self.n, seg)
+        optimize(g, FusionConfig.size_only(self._k))
+        for block in g.gates_in_row_order():
+            prov = block.provenance()
+            bq = block.qubits()
+            self._add_gate(block.matrix(), bq)
+            for pos, j in enumerate(prov):
+                for q, p, mats in markers.get(j, ()):
+                    u = eye(1 << len(bq))
+                    for i in prov[pos + 1:]:
+                        gi = seg[i]
+                        u = expand_matrix(gi.matrix(), gi.qubits(), bq) @ u
+                    ud = u.conj().T
+                    prop = [u @ expand_matrix(P, (q,), bq) @ ud for P in mats]
+                    self._add_error(p, prop)
+
+    def _build(self, circ: QuantumCircuit):
+        seg: list[QuantumGate] = []
+        markers: dict[int, list] = {}
+        last_on: dict[int, int] = {}
+        damp_mask, damp_gamma = 0, None
+
+        def flush_damp():
+            nonlocal damp_mask, damp_gamma
+            if damp_mask:
+                self._add_damping(damp_mask, damp_gamma)
+            damp_mask, damp_gamma = 0, None
+
+        for g in circ.gates():
+            if g.is_unitary():
+                if damp_mask:
+                    flush_damp()
+                idx = len(seg)
+                seg.append(g.with_provenance(idx))
+                for q in g.qubits():
+                    last_on[q] = idx
+                continue
+            pc = _is_pauli_channel(g)
+            if pc is not None:
+                if damp_mask:
+                    flush_damp()
+                q = g.qubits()[0]
+                if q not in last_on:
+                    idx = len(seg)
+                    seg.append(QuantumGate(eye(2), [q]).with_provenance(idx))
+                    last_on[q] = idx
+                markers.setdefault(last_on[q], []).append((q, pc[0], pc[1]))
+                continue
+            # non-Pauli noise closes the unitary segment
+            self._flush(seg, markers)
+            seg, markers, last_on = [], {}, {}
+            gamma = _damping_rate(g)
+            q = g.qubits()[0] if g.n_qubits() == 1 else None
+            if gamma is not None:
+                if damp_mask and (abs(gamma - damp_gamma) > 1e-15 or (damp_mask >> q) & 1):
+                    flush_damp()
+                damp_mask |= 1 << q
+                damp_gamma = gamma
+                continue
+            if damp_mask:
+                flush_damp()
+            if g.n_qubits() != 1 or len(g.noise_model()) > 4:
+                raise ValueError("trajectory mode supports single-qubit channels with <= 4 Kraus "
+                                 "operators")
+            kraus = [math.sqrt(p) * k for p, k in g.noise_model().branches]
+            self._add_channel(q, kraus)
+        self._flush(seg, markers)
+        flush_damp()
+
+    def __len__(self):
+        return int(L.lib().cast_b200_traj_num_ops(self.handle))
+
+    def run(self, n_traj: int, seed: int, stream=None, use_graph: bool = True):
+        """(z, samples): <Z_q> per trajectory (n_traj x n) and one bitstring each."""
+        z = np.zeros((n_traj, self.n))
+        smp = np.zeros(n_traj, dtype=np.uint32)
+        eb = L.errbuf()
+        h = stream.handle if stream is not None else None
+        L.check(L.lib().cast_b200_traj_run(self.handle, n_traj, seed & ((1 << 64) - 1),
+                                           z.ctypes.data_as(L.c_dp), smp.ctypes.data_as(L.c_u32p),
+                                           h, int(use_graph and h is not None), eb, L.ERR_LEN), eb,
+                "traj_run")
+        return z, smp
+
+
+@dataclass
+class TrajectoryOpts:
+    """trajectory.rs:18-33 (measured qubits, sample count, seed)."""
+
+    measured_qubits: list
+    n_samples: int
+    seed: int = 0
+    fusion_k: int = 4
+
+
+@dataclass
+class TrajectoryResult:
+    histogram: dict
+    n_samples: int
+    z_mean: np.ndarray
+    z_stderr: np.ndarray
+
+
+def sample_trajectory(circuit: QuantumCircuit, opts: TrajectoryOpts, stream=None) -> TrajectoryResult:
+    """One Monte-Carlo trajectory per sample; the histogram counts the measured
+    qubits' bitstrings (bit j of the key = measured_qubits[j])."""
+    prog = TrajectoryProgram(circuit, opts.fusion_k)
+    z, smp = prog.run(opts.n_samples, opts.seed, stream)
+    hist: dict[int, int] = {}
+    for s in smp.tolist():
+        key = 0
+        for j, q in enumerate(opts.measured_qubits):
+            key |= ((s >> q) & 1) << j
+        hist[key] = hist.get(key, 0) + 1
+    return TrajectoryResult(hist, opts.n_samples, z.mean(axis=0),
+                            z.std(axis=0, ddof=1) / math.sqrt(max(1, opts.n_samples)))
+
+
+def run_plain(circuit: QuantumCircuit, n_traj: int, seed: int, precision=None) -> np.ndarray:
+    """Quantum-jump trajectories on the plain per-gate path, one trajectory at a
+    time, with every noise decision taken on the host - the execution style of
+    the reference's ensemble loop (one launch per gate, a host synchronisation
+    at every noisy gate, src/simulator/trajectory.rs:180-265).  Used as the
+    baseline that the persistent kernel is measured against.  Returns <Z_q>
+    per trajectory (n_traj x n)."""
+    from .cuda import CudaPrecision, CudaStatevector
+    from .simulator import qubit_populations
+    from .types import SplitMix64
+
+    prec = CudaPrecision.F32 if precision is None else precision
+    lib = L.lib()
+    n = circuit.n_qubits()
+    rng = SplitMix64(seed)
+    out = np.zeros((n_traj, n))
+    tol = 1e-6 if prec == CudaPrecision.F32 else 1e-12
+
+    def apply(sv, m, q):
+        mm = np.ascontiguousarray(m, dtype=np.complex128)
+        qq = np.ascontiguousarray(q, dtype=np.uint32)
+        eb = L.errbuf()
+        L.check(lib.cast_b200_apply_gate(sv.dptr, n, int(prec), mm.view(np.float64).ctypes.data_as(
+            C.POINTER(L.Complex64)), qq.ctypes.data_as(L.c_u32p), qq.size, tol, tol, None, eb,
+            L.ERR_LEN), eb, "apply_gate")
+
+    for t in range(n_traj):
+        sv = CudaStatevector(n, prec)
+        sv.zero()
+        for g in circuit.gates():
+            if g.is_unitary():
+                apply(sv, g.matrix(), g.qubits())
+                continue
+            pc = _is_pauli_channel(g)
+            if pc is not None:
+                u = rng.uniform()
+                if u < pc[0]:
+                    apply(sv, pc[1][min(2, int(u / pc[0] * 3))], g.qubits())
+                continue
+            q = g.qubits()[0]
+            p1, nrm = qubit_populations(sv)  # host sync at every noisy gate
+            kraus = [math.sqrt(p) * k for p, k in g.noise_model().branches]
+            probs = []
+            for k in kraus:  # ||K psi||^2 from the qubit's populations (K acts on one qubit)
+                w0 = abs(k[0, 0]) ** 2 + abs(k[1, 0]) ** 2
+                w1 = abs(k[0, 1]) ** 2 + abs(k[1, 1]) ** 2
+                cross = 0.0 if abs(np.vdot(k[:, 0], k[:, 1])) < 1e-15 else None
+                probs.append(None if cross is None else w0 * (nrm - p1[q]) + w1 * p1[q])
+            if any(p is None for p in probs):
+                raise ValueError("plain trajectories support channels with orthogonal Kraus columns")
+            u = rng.uniform() * sum(probs)
+            acc, pick = 0.0, len(kraus) - 1
+            for i, p in enumerate(probs):
+                acc += p
+                if u < acc:
+                    pick = i
+                    break
+            apply(sv, kraus[pick] / math.sqrt(probs[pick] / nrm), g.qubits())
+            sv.normalize()
+        p1, nrm = qubit_populations(sv)
+        out[t] = 1.0 - 2.0 * p1 / nrm
+    return out

@@ -186,7 +186,7 @@ class NoiseModel:
 
 
 class QuantumGate:
-    __slots__ = ("_m", "_q", "_noise", "_name")
+    __slots__ = ("_m", "_q", "_noise", "_name", "_prov")
 
     def __init__(self, matrix, qubits, noise: NoiseModel | None = None, name: str = ""):
         m = np.ascontiguousarray(np.asarray(matrix, dtype=np.complex128))
@@ -194,6 +194,17 @@ class QuantumGate:
         self._m = np.ascontiguousarray(self._m)
         self._noise = noise
         self._name = name
+        self._prov = None
+
+    def with_provenance(self, index: int) -> "QuantumGate":
+        """Copy tagged with a source index; matmul concatenates the tags in
+        application order, so a fused gate knows which gates it contains."""
+        g = QuantumGate.__new__(QuantumGate)
+        g._m, g._q, g._noise, g._name, g._prov = self._m, self._q, self._noise, self._name, [index]
+        return g
+
+    def provenance(self):
+        return self._prov
 
     # factories
     @classmethod
@@ -259,7 +270,7 @@ class QuantumGate:
                 raise ValueError("noise operator dimension must match gate dimension")
             br.append((float(p), v @ self._m))
         g = QuantumGate.__new__(QuantumGate)
-        g._m, g._q, g._noise, g._name = self._m, self._q, NoiseModel(br), self._name
+        g._m, g._q, g._noise, g._name, g._prov = self._m, self._q, NoiseModel(br), self._name, None
         return g
 
     def with_kraus(self, kraus_ops) -> "QuantumGate":
@@ -270,7 +281,7 @@ class QuantumGate:
         m = len(kraus_ops)
         br = [(1.0 / m, math.sqrt(m) * np.asarray(k, dtype=np.complex128)) for k in kraus_ops]
         g = QuantumGate.__new__(QuantumGate)
-        g._m, g._q, g._noise, g._name = self._m, self._q, NoiseModel(br), self._name
+        g._m, g._q, g._noise, g._name, g._prov = self._m, self._q, NoiseModel(br), self._name, None
         return g
 
     def with_depolarizing(self, p: float) -> "QuantumGate":
@@ -354,6 +365,7 @@ class QuantumGate:
             noise = NoiseModel(br)
         g = QuantumGate.__new__(QuantumGate)
         g._m, g._q, g._noise, g._name = np.ascontiguousarray(fused), uq, noise, "fused"
+        g._prov = (other._prov + self._prov) if (self._prov is not None and other._prov is not None) else None
         return g
 
     def to_density_matrix_gate(self, n_total: int) -> "QuantumGate":

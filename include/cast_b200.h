@@ -85,6 +85,33 @@ int cast_b200_marginal_probabilities(uint64_t sv_dptr, uint32_t n_qubits, uint8_
 int cast_b200_dm_populations(uint64_t rho_dptr, uint32_t n_physical, uint8_t precision,
                              double *out, void *stream, char *err_buf, size_t err_buf_len);
 
+/* -- Batched noisy trajectories ---------------------------------------------------
+ * A trajectory program for n <= 22 qubits (complex64 amplitudes, FP64 branch
+ * sums): fused unitary blocks (k <= 4), Pauli errors attached to the block they
+ * follow (three k-qubit matrices U P U^dagger for X, Y, Z, each fired with
+ * probability prob / 3), amplitude damping on a qubit mask, and general
+ * single-qubit channels (1..4 Kraus operators, 2x2 each).  cast_b200_traj_run
+ * samples n_traj Monte-Carlo quantum-jump trajectories from |0...0> in one
+ * persistent kernel launch (captured once into a CUDA graph when use_graph and
+ * stream is non-NULL) and returns <Z_q> per trajectory (n_traj x n doubles) and
+ * one sampled bitstring per trajectory.  Replaces the deterministic ensemble
+ * branching of src/simulator/trajectory.rs:180-312, whose branch weights are the
+ * fixed p_i rather than ||K_i psi||^2. */
+void *cast_b200_traj_create(uint32_t n_qubits, char *err_buf, size_t err_buf_len);
+void cast_b200_traj_destroy(void *program);
+int cast_b200_traj_add_gate(void *program, const cast_complex64_t *matrix, const uint32_t *qubits,
+                            uint32_t n_gate_qubits, char *err_buf, size_t err_buf_len);
+int cast_b200_traj_add_pauli_error(void *program, double prob, const cast_complex64_t *matrices,
+                                   char *err_buf, size_t err_buf_len);
+int cast_b200_traj_add_damping(void *program, uint32_t qubit_mask, double gamma, char *err_buf,
+                               size_t err_buf_len);
+int cast_b200_traj_add_channel(void *program, uint32_t qubit, const cast_complex64_t *kraus,
+                               uint32_t n_kraus, char *err_buf, size_t err_buf_len);
+uint32_t cast_b200_traj_num_ops(const void *program);
+int cast_b200_traj_run(void *program, uint32_t n_traj, uint64_t seed, double *out_z,
+                       uint32_t *out_samples, void *stream, int use_graph, char *err_buf,
+                       size_t err_buf_len);
+
 /* -- Allocation-free norm^2 -------------------------------------------------------
  * No counterpart in the reference: an extra variant of cast_cuda_norm_squared
  * for callers that cannot let a library allocate device memory (work recorded

@@ -1,0 +1,150 @@
+"""Monte-Carlo trajectories on the GPU vs density-matrix evolution on the CPU
+oracle (the reference checks trajectories against its DM simulator at 0.01-0.02,
+src/simulator/tests.rs:153-190, 274-316).  Statistical checks use 5 standard
+errors of the trajectory mean plus a small floor."""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mods(cblib):
+    from cast_simulator_b200 import simulator, trajectory, types
+
+    return types, trajectory, simulator
+
+
+def z_from_pops(pops, n):
+    idx = np.arange(pops.size)
+    return np.array([1 - 2 * pops[(idx >> q) & 1 == 1].sum() for q in range(n)])
+
+
+def dm_reference(oracle, circ):
+    """Channel-by-channel DM evolution; a unitary gate is merged with the Pauli
+    channels that directly follow it so that each superoperator is applied once."""
+    n = circ.n_qubits()
+    rho = oracle.dm_zero(n)
+    gates = circ.gates()
+    i = 0
+    while i < len(gates):
+        g = gates[i]
+        if g.is_unitary():
+            kraus, weights, qs = [g.matrix()], [1.0], g.qubits()
+            j = i + 1
+            while j < len(gates) and not gates[j].is_unitary() and set(gates[j].qubits()) <= set(qs) \
+                    and len(gates[j].noise_model()) == 4:
+                nk, nw = [], []
+                pos = qs.index(gates[j].qubits()[0])
+                for w0, k0 in zip(weights, kraus):
+                    for w1, k1 in gates[j].noise_model().branches:
+                        full = _embed(k1, pos, len(qs))
+                        nk.append(full @ k0)
+                        nw.append(w0 * w1)
+                kraus, weights = nk, nw
+                j += 1
+            oracle.dm_apply_channel(rho, n, kraus, weights, qs)
+            i = j
+        else:
+            br = g.noise_model().branches
+            oracle.dm_apply_channel(rho, n, [k for _, k in br], [p for p, _ in br], g.qubits())
+            i += 1
+    return z_from_pops(oracle.dm_populations(rho, n), n)
+
+
+def _embed(m1, pos, k):
+    out = np.array([[1.0]], dtype=complex)
+    for b in range(k - 1, -1, -1):
+        out = np.kron(out, m1 if b == pos else np.eye(2))
+    return out
+
+
+def test_noise_free_trajectories_equal_statevector(mods, oracle):
+    T, TR, S = mods
+    circ = T.QuantumCircuit.brickwork(9, 6, 3)
+    sv = oracle.simulate(9, [(g.matrix(), g.qubits()) for g in circ.gates()])
+    z_ref = z_from_pops(np.abs(sv) ** 2, 9)
+    prog = TR.TrajectoryProgram(circ, 4)
+    z, smp = prog.run(64, 1)
+    assert np.max(np.abs(z - z_ref[None, :])) < 2e-5
+    assert smp.max() < (1 << 9)
+
+
+@pytest.mark.parametrize("fusion_k", [2, 4])
+def test_depolarizing_and_damping_match_dm(mods, oracle, fusion_k):
+    T, TR, S = mods
+    n = 5
+    circ = T.QuantumCircuit.brickwork(n, 4, 17, depolarizing=0.04, damping=0.08)
+    z_ref = dm_reference(oracle, circ)
+    prog = TR.TrajectoryProgram(circ, fusion_k)
+    n_traj = 16384
+    st = S.Stream()
+    z, _ = prog.run(n_traj, 99, st)
+    mean = z.mean(axis=0)
+    se = z.std(axis=0, ddof=1) / math.sqrt(n_traj)
+    assert np.all(np.abs(mean - z_ref) < 5 * se + 2e-3), (mean, z_ref, se)
+
+
+def test_strong_damping_rare_path(mods, oracle):
+    """Every qubit in |1>, then damping 0.3 on all: the no-jump branch has
+    probability 0.7^n, so the exact conditioned sequential path dominates."""
+    T, TR, S = mods
+    n = 6
+    circ = T.QuantumCircuit(n)
+    for q in range(n):
+        circ.add(T.QuantumGate.x(q))
+    for q in range(n):
+        circ.add(T.QuantumGate.amplitude_damping(q, 0.3))
+    n_traj = 20000
+    z, smp = TR.TrajectoryProgram(circ, 2).run(n_traj, 5)
+    mean = z.mean(axis=0)
+    # each qubit independently decays: P(1) = 0.7 -> <Z> = -0.4
+    se = z.std(axis=0, ddof=1) / math.sqrt(n_traj)
+    assert np.all(np.abs(mean + 0.4) < 5 * se + 1e-3), mean
+    ones = np.array([bin(int(s)).count("1") for s in smp])
+    assert abs(ones.mean() - 0.7 * n) < 0.05
+
+
+def test_general_channel_matches_dm(mods, oracle):
+    T, TR, S = mods
+    n = 4
+    circ = T.QuantumCircuit.brickwork(n, 2, 8)
+    # an unequal Pauli channel (not a depolarizing form) -> general channel op
+    circ.add(T.QuantumGate.pauli_channel(1, 0.1, 0.05, 0.2))
+    circ.add(T.QuantumGate.u3(0.7, 0.1, 0.3, 1))
+    z_ref = dm_reference(oracle, circ)
+    prog = TR.TrajectoryProgram(circ, 3)
+    assert prog.stats.n_channels == 1
+    n_traj = 20000
+    z, _ = prog.run(n_traj, 3)
+    se = z.std(axis=0, ddof=1) / math.sqrt(n_traj)
+    assert np.all(np.abs(z.mean(axis=0) - z_ref) < 5 * se + 1e-3)
+
+
+@pytest.mark.timeout(600)
+def test_trajectory_config_10q_instance_vs_dm(mods, oracle):
+    """The trajectory configuration's construction (brickwork depth 30, depolarizing
+    1e-3 after every gate, damping 5e-4 per qubit per layer) at 10 qubits, 4096
+    trajectories vs the DM oracle."""
+    T, TR, S = mods
+    n = 10
+    circ = T.QuantumCircuit.brickwork(n, 30, 2024, depolarizing=1e-3, damping=5e-4)
+    z_ref = dm_reference(oracle, circ)
+    z, _ = TR.TrajectoryProgram(circ, 4).run(4096, 7, S.Stream())
+    mean = z.mean(axis=0)
+    se = z.std(axis=0, ddof=1) / math.sqrt(4096)
+    assert np.all(np.abs(mean - z_ref) < 5 * se + 2e-3), (np.abs(mean - z_ref).max(), se.max())
+
+
+def test_graph_replay_is_deterministic(mods):
+    T, TR, S = mods
+    circ = T.QuantumCircuit.brickwork(8, 5, 1, depolarizing=0.02, damping=0.02)
+    prog = TR.TrajectoryProgram(circ, 4)
+    st = S.Stream()
+    a, sa = prog.run(300, 11, st)
+    b, sb = prog.run(300, 11, st)
+    c, _ = prog.run(300, 12, st)
+    assert np.array_equal(a, b) and np.array_equal(sa, sb)
+    assert not np.array_equal(a, c)
