@@ -44,6 +44,21 @@ class KernelGenSpec(C.Structure):
     ]
 
 
+class FusionConfigC(C.Structure):
+    """cast_b200_fusion_config_t (include/cast_b200.h)."""
+
+    _fields_ = [
+        ("size_max", C.c_uint32),
+        ("cost_kind", C.c_uint32),
+        ("benefit_margin", C.c_double),
+        ("zero_tol", C.c_double),
+        ("crossover_ai", C.c_double),
+        ("tensor_crossover_ai", C.c_double),
+        ("tensor_min_k", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
 # (name, restype, argtypes) of every exported symbol, in header order.
 FFI_CUDA = [
     ("cast_cuda_compile_gate_ptx", C.c_int,
@@ -109,6 +124,13 @@ CAST_B200 = [
       C.c_size_t]),
     ("cast_b200_dm_populations", C.c_int,
      [C.c_uint64, C.c_uint32, C.c_uint8, c_dp, C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("cast_b200_fuse", C.c_void_p,
+     [C.c_uint32, C.c_uint32, c_u32p, c_u32p, C.POINTER(Complex64), C.POINTER(FusionConfigC),
+      C.c_char_p, C.c_size_t]),
+    ("cast_b200_fused_num_gates", C.c_uint32, [C.c_void_p]),
+    ("cast_b200_fused_gate", C.c_int, [C.c_void_p, C.c_uint32, c_u32p, c_u32p, C.POINTER(Complex64)]),
+    ("cast_b200_program_add_fused", C.c_int, [C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("cast_b200_fused_free", None, [C.c_void_p]),
     ("cast_b200_traj_create", C.c_void_p, [C.c_uint32, C.c_char_p, C.c_size_t]),
     ("cast_b200_traj_destroy", None, [C.c_void_p]),
     ("cast_b200_traj_add_gate", C.c_int,

@@ -497,3 +497,90 @@ def optimize_with_log(cg: CircuitGraph, config: FusionConfig) -> list:
         while apply_gate_fusion(cg, config, cdd, log) > 0:
             pass
     return log
+
+
+# ── native planner (csrc/fusion.cpp, cast_b200_fuse) ────────────────────────
+
+
+def _native_config(config: FusionConfig):
+    from . import _lib as L
+
+    cm = config.cost_model
+    if isinstance(cm, SizeOnlyCostModel):
+        if cm.max_ai != float("inf") or cm.trajectory_mode:
+            raise ValueError("the native planner supports size-only models without an AI cap")
+        return L.FusionConfigC(config.size_max, 0, config.benefit_margin, 0.0, 0.0, 0.0, 0, 0)
+    if isinstance(cm, HardwareAdaptiveCostModel):
+        p = cm.profile
+        txo = p.tensor_gflops_s / p.bw_slope if (p.tensor_min_k and p.tensor_gflops_s > 0) else 0.0
+        return L.FusionConfigC(config.size_max, 1, config.benefit_margin, cm.zero_tol,
+                               p.crossover_ai, txo, p.tensor_min_k, 0)
+    raise ValueError("unsupported cost model for the native planner")
+
+
+class FusedCircuit:
+    """Result of the native planner: fused unitary gates in row order."""
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    def __len__(self):
+        from . import _lib as L
+
+        return int(L.lib().cast_b200_fused_num_gates(self.handle))
+
+    def gates(self) -> list[QuantumGate]:
+        import ctypes as C
+
+        import numpy as np
+
+        from . import _lib as L
+
+        out = []
+        k = C.c_uint32()
+        q = (C.c_uint32 * 7)()
+        for i in range(len(self)):
+            L.lib().cast_b200_fused_gate(self.handle, i, C.byref(k), q, None)
+            m = np.zeros(1 << (2 * k.value), dtype=np.complex128)
+            L.lib().cast_b200_fused_gate(self.handle, i, C.byref(k), q,
+                                         m.view(np.float64).ctypes.data_as(C.POINTER(L.Complex64)))
+            d = 1 << k.value
+            out.append(QuantumGate(m.reshape(d, d), [q[j] for j in range(k.value)], name="fused"))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            try:
+                from . import _lib as L
+
+                L.lib().cast_b200_fused_free(h)
+            except Exception:
+                pass
+
+
+def optimize_native(n_qubits: int, gates, config: FusionConfig | None = None) -> FusedCircuit:
+    """Fuse a unitary gate list (circuit order) with the native planner; same
+    decisions as ``optimize`` on ``CircuitGraph.from_gates(n_qubits, gates)``."""
+    import ctypes as C
+
+    import numpy as np
+
+    from . import _lib as L
+
+    config = config or FusionConfig.default()
+    gates = list(gates)
+    for g in gates:
+        if not g.is_unitary():
+            raise ValueError("the native planner fuses unitary gates only")
+    ks = np.array([g.n_qubits() for g in gates], dtype=np.uint32)
+    qs = np.array([q for g in gates for q in g.qubits()], dtype=np.uint32)
+    ms = (np.concatenate([np.ascontiguousarray(g.matrix()).reshape(-1) for g in gates])
+          if gates else np.zeros(1, dtype=np.complex128))
+    cfg = _native_config(config)
+    eb = L.errbuf()
+    h = L.lib().cast_b200_fuse(n_qubits, len(gates), ks.ctypes.data_as(L.c_u32p),
+                               qs.ctypes.data_as(L.c_u32p),
+                               ms.view(np.float64).ctypes.data_as(C.POINTER(L.Complex64)),
+                               C.byref(cfg), eb, L.ERR_LEN)
+    return FusedCircuit(L.check_ptr(h, eb, "fuse"))

@@ -85,6 +85,41 @@ int cast_b200_marginal_probabilities(uint64_t sv_dptr, uint32_t n_qubits, uint8_
 int cast_b200_dm_populations(uint64_t rho_dptr, uint32_t n_physical, uint8_t precision,
                              double *out, void *stream, char *err_buf, size_t err_buf_len);
 
+/* -- Native fusion planner -----------------------------------------------------------
+ * Runs the reference's optimiser - phase 1 size-2 canonicalisation and phase 2
+ * agglomerative fusion for candidate sizes 3..size_max with cost-model
+ * accept/rollback (src/fusion.rs:14-345 over the CircuitGraph of
+ * src/circuit_graph.rs:107-504) - on a unitary gate list given in circuit
+ * order (gate_k[i] qubits each, ascending, concatenated in `qubits`; 4^k
+ * matrix entries each, concatenated in `matrices`).  cost_kind 0 is
+ * SizeOnlyCostModel (cost_model.rs:20-44), 1 is HardwareAdaptiveCostModel
+ * (cost_model.rs:238-275: cost = max(1, AI / crossover)); gates with
+ * k >= tensor_min_k (when non-zero) use tensor_crossover_ai instead, the
+ * crossover of the tensor-core contraction path.  The result lists the fused
+ * gates in row order (the reference's gates_in_row_order). */
+typedef struct cast_b200_fusion_config_t {
+  uint32_t size_max;
+  uint32_t cost_kind;
+  double benefit_margin;
+  double zero_tol;
+  double crossover_ai;
+  double tensor_crossover_ai;
+  uint32_t tensor_min_k;
+  uint32_t reserved;
+} cast_b200_fusion_config_t;
+
+void *cast_b200_fuse(uint32_t n_qubits, uint32_t n_gates, const uint32_t *gate_k,
+                     const uint32_t *qubits, const cast_complex64_t *matrices,
+                     const cast_b200_fusion_config_t *config, char *err_buf, size_t err_buf_len);
+uint32_t cast_b200_fused_num_gates(const void *fused);
+/* Copies fused gate `index`: its size, ascending qubits (<= 7) and 4^k entries. */
+int cast_b200_fused_gate(const void *fused, uint32_t index, uint32_t *out_k, uint32_t *out_qubits,
+                         cast_complex64_t *out_matrix);
+/* Appends every fused gate to a gate program (cast_b200_program_add_gate). */
+int cast_b200_program_add_fused(void *program, const void *fused, char *err_buf,
+                                size_t err_buf_len);
+void cast_b200_fused_free(void *fused);
+
 /* -- Batched noisy trajectories ---------------------------------------------------
  * A trajectory program for n <= 22 qubits (complex64 amplitudes, FP64 branch
  * sums): fused unitary blocks (k <= 4), Pauli errors attached to the block they
