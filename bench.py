@@ -186,6 +186,131 @@ def run_reference(args):
     return 0
 
 
+def trajectory_leg(n: int = 16, depth: int = 30, n_traj: int = 4096, k: int = 3):
+    """Noisy-trajectory configuration: brickwork depth 30 with depolarizing 1e-3
+    after every gate and amplitude damping 5e-4 per qubit per layer; 4096
+    trajectories in one persistent launch (CUDA graph) vs the plain per-gate
+    path with host-side noise decisions on a few trajectories."""
+    from cast_simulator_b200.simulator import Stream
+    from cast_simulator_b200.trajectory import TrajectoryProgram, run_plain
+    from cast_simulator_b200.types import QuantumCircuit
+
+    circ = QuantumCircuit.brickwork(n, depth, 31337, depolarizing=1e-3, damping=5e-4)
+    prog = TrajectoryProgram(circ, k)
+    st = Stream()
+    prog.run(n_traj, 1, st)
+    times = []
+    for r in range(3):
+        t0 = time.perf_counter()
+        z, _ = prog.run(n_traj, 2 + r, st)
+        times.append(time.perf_counter() - t0)
+    t = float(np.median(times))
+    n_plain = 4
+    t0 = time.perf_counter()
+    run_plain(circ, n_plain, 5)
+    tp = (time.perf_counter() - t0) / n_plain
+    return {"config": f"brickwork-{n}q-d{depth}, depolarizing 1e-3, damping 5e-4, c64, k={k}",
+            "n_traj": n_traj, "seconds": t, "traj_per_s": n_traj / t,
+            "plain_traj_per_s": 1.0 / tp, "speedup_vs_plain": (n_traj / t) * tp,
+            "blocks": prog.stats.n_blocks, "error_sites": prog.stats.n_errors,
+            "z_mean_first4": [float(x) for x in z.mean(axis=0)[:4]]}
+
+
+def serving_leg(n_req: int):
+    """Serving stream (bounded sample): Poisson arrivals of random brickwork
+    circuits, 10..24 qubits (noisy: 10..16 with 256 trajectories), depth 5..40,
+    half complex64 / half complex128, 20% noisy; p50/p99 latency and circuits/s
+    at two arrival rates, against a sequential FIFO of plain-path service times
+    (per-gate C-ABI launches; noisy requests scaled from 8 host-driven
+    trajectories)."""
+    from cast_simulator_b200 import serving as S
+
+    out = {"requests": n_req, "rates": []}
+    for rate in (40.0, 160.0):
+        reqs = S.make_stream(n_req, rate, 7, n_range=(10, 24))
+        eng = S.ServingEngine(max_slots=8)
+        try:
+            t0 = time.perf_counter()
+            res = eng.run_stream(reqs)
+            wall = time.perf_counter() - t0
+            conc = eng.max_concurrent
+        finally:
+            eng.shutdown()
+        lat = [r.latency for r in res]
+        out["rates"].append({"rate_hz": rate, **S.latency_summary(lat),
+                             "circuits_per_s": n_req / wall, "max_concurrent": conc})
+    # plain sequential baseline on the same requests (service times measured alone)
+    reqs = S.make_stream(n_req, 40.0, 7, n_range=(10, 24))
+    svc = []
+    for r in reqs:
+        if r.n_traj:
+            sub = S.Request(r.circuit, r.precision, 8, r.seed, r.arrival, r.rid)
+            svc.append(S.plain_service_time(sub) * r.n_traj / 8)
+        else:
+            svc.append(S.plain_service_time(r))
+    for entry in out["rates"]:
+        arr = [r.arrival * 40.0 / entry["rate_hz"] for r in reqs]
+        seq = S.sequential_latencies(arr, svc)
+        entry["plain_sequential"] = {**S.latency_summary(seq),
+                                     "circuits_per_s": n_req / max(arr[-1], float(np.sum(svc)))}
+    out["plain_service_s_total"] = float(np.sum(svc))
+    return out
+
+
+def tensor_leg(n: int, depth: int):
+    """Tensor-core fused path (complex64, split BF16, k = 5 and 6) vs the plain
+    CUDA-core path at its best width (k = 4): time per circuit on the full
+    30-qubit brickwork, and 1-|<psi_64|psi>| against the complex128 plain path on
+    a 24-qubit brickwork of the same construction."""
+    from cast_simulator_b200 import cuda as cu
+    from cast_simulator_b200.fusion import CircuitGraph, FusionConfig, optimize_native
+    from cast_simulator_b200.simulator import Event, GateProgram, Simulator, Stream
+    from cast_simulator_b200.types import QuantumCircuit
+
+    out = {"workload": f"brickwork-{n}q-d{depth}-c64", "runs": []}
+    circ = QuantumCircuit.brickwork(n, depth, 2024)
+    st = Stream()
+    for k, split in ((4, False), (5, True), (6, True)):
+        gates = optimize_native(n, circ.gates(), FusionConfig.size_only(k)).gates()
+        prog = GateProgram(cu.CudaPrecision.F32, n, 1e-6, 1e-6, split)
+        for g in gates:
+            prog.add(g.matrix(), g.qubits())
+        sv = cu.CudaStatevector(n, cu.CudaPrecision.F32)
+        e0, e1 = Event(), Event()
+        ts = []
+        for rep in range(4):
+            sv.zero(st)
+            e0.record(st)
+            prog.run(sv, st, use_graph=True)
+            e1.record(st)
+            e1.sync()
+            if rep:
+                ts.append(e1.elapsed_s(e0))
+        t = float(np.median(ts))
+        out["runs"].append({"fusion_k": k, "tensor_cores": split, "fused_gates": len(gates),
+                            "ms_per_circuit": t * 1e3,
+                            "hbm_gbs": len(gates) * 2 * (1 << n) * 8 / t / 1e9})
+        del sv, prog
+    base = out["runs"][0]["ms_per_circuit"]
+    for r in out["runs"]:
+        r["speedup_vs_plain_k4"] = base / r["ms_per_circuit"]
+    # fidelity on a 24-qubit instance against complex128
+    nf = 24
+    small = QuantumCircuit.brickwork(nf, depth, 2024)
+    ref = Simulator(cu.CudaKernelGenSpec.f64()).simulate(
+        CircuitGraph.from_gates(nf, optimize_native(nf, small.gates(), FusionConfig.size_only(4)).gates())
+    ).download_amplitudes()
+    fid = {}
+    for k in (5, 6):
+        g = CircuitGraph.from_gates(nf, optimize_native(nf, small.gates(), FusionConfig.size_only(k)).gates())
+        psi = Simulator(cu.CudaKernelGenSpec.f32(), split_precision=True).simulate(g).download_amplitudes()
+        ov = np.vdot(ref, psi)
+        fid[f"k{k}"] = {"one_minus_abs_overlap": float(1 - abs(ov)),
+                        "max_abs_err": float(np.max(np.abs(ref - psi)))}
+    out["fidelity_24q_vs_c128"] = fid
+    return out
+
+
 def traffic_from_profile(n: int, precision: str, k: int):
     """DRAM bytes per launch of the dominant kernel from the committed ncu
     summary (captured on a smaller statevector and scaled by amplitudes)."""
@@ -212,6 +337,8 @@ def main(argv=None):
     ap.add_argument("--cpu-n", type=int, default=28)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip trajectory and serving legs")
+    ap.add_argument("--serve-requests", type=int, default=60)
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
@@ -348,6 +475,10 @@ def main(argv=None):
         line["cpu_baseline"] = {
             "value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
             "sample": f"{passes} fused-gate passes of the {n_cpu}-qubit brickwork (k={args.k}) in {el:.1f} s"}
+    if rank == 0 and not args.no_extras:
+        line["tensor_path"] = tensor_leg(n, args.depth)
+        line["trajectories"] = trajectory_leg()
+        line["serving"] = serving_leg(args.serve_requests)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg:

@@ -103,6 +103,9 @@ FFI_CUDA = [
 # Extension entry points (include/cast_b200.h).
 CAST_B200 = [
     ("cast_b200_set_device", C.c_int, [C.c_int, C.c_char_p, C.c_size_t]),
+    ("cast_b200_stream_create_nonblocking", C.c_void_p, [C.c_char_p, C.c_size_t]),
+    ("cast_b200_sv_zero_async", C.c_int,
+     [C.c_uint64, C.c_size_t, C.c_uint8, C.c_void_p, C.c_char_p, C.c_size_t]),
     ("cast_b200_set_gate_path", C.c_int, [C.c_int]),
     ("cast_b200_apply_gate", C.c_int,
      [C.c_uint64, C.c_uint32, C.c_uint8, C.POINTER(Complex64), c_u32p, C.c_uint32, C.c_double,
@@ -111,6 +114,8 @@ CAST_B200 = [
      [C.c_uint8, C.c_uint32, C.c_double, C.c_double, C.c_char_p, C.c_size_t]),
     ("cast_b200_program_add_gate", C.c_int,
      [C.c_void_p, C.POINTER(Complex64), c_u32p, C.c_uint32, C.c_char_p, C.c_size_t]),
+    ("cast_b200_program_set_split_precision", C.c_int,
+     [C.c_void_p, C.c_int, C.c_char_p, C.c_size_t]),
     ("cast_b200_program_num_gates", C.c_uint32, [C.c_void_p]),
     ("cast_b200_program_run", C.c_int,
      [C.c_void_p, C.c_uint64, C.c_void_p, C.c_int, C.c_char_p, C.c_size_t]),

@@ -49,14 +49,17 @@ struct Program {
   uint8_t precision = 1;
   uint32_t n = 0;
   double ztol = 0, otol = 0;
+  bool split = false;  // complex64 gates with 4..6 qubits run on the tensor cores
   std::vector<GateData> gates;
   std::map<std::pair<uint64_t, void *>, cudaGraphExec_t> graphs;
   std::mutex mu;
 
   ~Program() {
     for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
-    for (auto &g : gates)
+    for (auto &g : gates) {
       if (g.d_mat) cudaFree(g.d_mat);
+      if (g.d_tc) cudaFree(g.d_tc);
+    }
   }
 
   void drop_graphs() {
@@ -76,9 +79,50 @@ Program *as_program(void *p) {
   return pr && pr->magic == kProgramMagic ? pr : nullptr;
 }
 
+__global__ void k_set_one(void *p, int f64) {
+  if (f64) *static_cast<double *>(p) = 1.0;
+  else *static_cast<float *>(p) = 1.0f;
+}
+
 }  // namespace
 
 extern "C" {
+
+void *cast_b200_stream_create_nonblocking(char *err_buf, size_t err_buf_len) {
+  std::string err;
+  cudaStream_t s = nullptr;
+  if (!cuda_ok(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate", err)) {
+    write_err(err_buf, err_buf_len, err);
+    return nullptr;
+  }
+  clear_err(err_buf, err_buf_len);
+  return s;
+}
+
+int cast_b200_sv_zero_async(uint64_t dptr, size_t n_elements, uint8_t precision, void *stream,
+                            char *err_buf, size_t err_buf_len) {
+  std::string err;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  void *d = reinterpret_cast<void *>(dptr);
+  if (!d || precision > 1) {
+    write_err(err_buf, err_buf_len, "invalid statevector or precision");
+    return 1;
+  }
+  const size_t sb = precision ? sizeof(double) : sizeof(float);
+  if (!cuda_ok(cudaMemsetAsync(d, 0, n_elements * sb, s), "cudaMemsetAsync", err)) {
+    write_err(err_buf, err_buf_len, err);
+    return 1;
+  }
+  if (n_elements) {
+    k_set_one<<<1, 1, 0, s>>>(d, precision);
+    if (!cuda_ok(cudaGetLastError(), "zero-state kernel launch", err)) {
+      write_err(err_buf, err_buf_len, err);
+      return 1;
+    }
+  }
+  clear_err(err_buf, err_buf_len);
+  return 0;
+}
 
 int cast_b200_set_device(int device, char *err_buf, size_t err_buf_len) {
   std::string err;
@@ -158,7 +202,8 @@ int cast_b200_program_add_gate(void *program, const cast_complex64_t *matrix,
     GateData g;
     std::string err;
     if (!make_gate(p->precision, matrix, qubits, n_gate_qubits, p->ztol, p->otol, g, err) ||
-        !cb2::check_gate(g, p->n, err) || (g.k >= 6 && !cb2::upload_gate_matrix(g, err))) {
+        !cb2::check_gate(g, p->n, err) || (g.k >= 6 && !cb2::upload_gate_matrix(g, err)) ||
+        (p->split && cb2::tensor_path_supported(g) && !cb2::prepare_tensor_gate(g, err))) {
       write_err(err_buf, err_buf_len, err);
       return 1;
     }
@@ -171,6 +216,23 @@ int cast_b200_program_add_gate(void *program, const cast_complex64_t *matrix,
     write_err(err_buf, err_buf_len, ex.what());
     return 1;
   }
+}
+
+int cast_b200_program_set_split_precision(void *program, int enable, char *err_buf,
+                                          size_t err_buf_len) {
+  Program *p = as_program(program);
+  if (!p) {
+    write_err(err_buf, err_buf_len, "invalid program handle");
+    return 1;
+  }
+  std::lock_guard<std::mutex> lock(p->mu);
+  if (!p->gates.empty()) {
+    write_err(err_buf, err_buf_len, "set the split-precision mode before adding gates");
+    return 1;
+  }
+  p->split = enable != 0;
+  clear_err(err_buf, err_buf_len);
+  return 0;
 }
 
 uint32_t cast_b200_program_num_gates(const void *program) {

@@ -507,6 +507,7 @@ bool launch_gate(const GateData &g, void *sv, uint32_t n, cudaStream_t stream, s
     err = "statevector pointer must not be null";
     return false;
   }
+  if (g.d_tc) return launch_gate_tensor(g, sv, n, stream, err);
   Targets t;
   for (uint32_t b = 0; b < kMaxGateQubits; ++b) {
     const uint32_t q = b < g.k ? g.qubits[b] : 0;

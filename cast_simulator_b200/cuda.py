@@ -106,10 +106,17 @@ class CudaStatevector:
     def nbytes(self) -> int:
         return self._len * self._prec.scalar_bytes()
 
-    def zero(self) -> None:
+    def zero(self, stream=None) -> None:
+        """Reset to |0...0>: host-synchronous (cast_cuda_sv_zero) without a
+        stream, ordered on `stream` (a Stream or a raw handle) with one."""
         eb = L.errbuf()
-        L.check(L.lib().cast_cuda_sv_zero(self._dptr, self._len, int(self._prec), eb, L.ERR_LEN), eb,
-                "sv zero")
+        if stream is None:
+            L.check(L.lib().cast_cuda_sv_zero(self._dptr, self._len, int(self._prec), eb, L.ERR_LEN),
+                    eb, "sv zero")
+            return
+        h = getattr(stream, "handle", stream)
+        L.check(L.lib().cast_b200_sv_zero_async(self._dptr, self._len, int(self._prec), h, eb,
+                                                L.ERR_LEN), eb, "sv zero async")
 
     def upload(self, amps) -> None:
         a = np.ascontiguousarray(np.asarray(amps, dtype=np.complex128))

@@ -1,0 +1,302 @@
+"""Continuous-batching request loop for circuit simulation on one GPU.
+
+The reference runs one circuit at a time through ``Simulator::simulate`` /
+``sample_trajectory`` (src/simulator/mod.rs:523-547, trajectory.rs:104-130);
+this engine keeps many requests in flight:
+
+  * requests (a circuit, a precision, optionally a trajectory count) queue in
+    arrival order;
+  * a dispatcher admits the head of the queue as soon as a slot is free and the
+    device-memory budget covers its footprint (16 * 2^n bytes for complex128,
+    8 * 2^n for complex64, the trajectory workspace for noisy requests);
+    admission never reorders requests;
+  * each admitted request runs on its own CUDA stream in a worker thread: its
+    gates are fused by the native planner and uploaded as a gate program that is
+    launched on that stream (noisy requests run the persistent trajectory
+    kernel from a CUDA graph); work of different requests overlaps on the device;
+  * when a request finishes, its <Z_q> vector is read back (FP64 device
+    reduction), its memory returns to the budget and the next requests are
+    admitted - the batch composition changes continuously.
+
+Statevectors are recycled through a per-(qubits, precision) free list, so
+steady-state admission does not call cudaMalloc.
+"""
+from __future__ import annotations
+
+import collections
+import math
+import threading
+import time
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+from .cuda import CudaPrecision, CudaStatevector, cuda_free_memory_bytes
+from .fusion import FusionConfig, optimize_native
+from .simulator import GateProgram, Stream, qubit_populations
+from .trajectory import TrajectoryProgram
+from .types import QuantumCircuit
+
+
+@dataclass
+class Request:
+    circuit: QuantumCircuit
+    precision: CudaPrecision = CudaPrecision.F64
+    n_traj: int = 0  # 0: pure state-vector simulation
+    seed: int = 0
+    arrival: float = 0.0  # seconds after the stream starts (run_stream)
+    rid: int = -1
+
+
+@dataclass
+class Result:
+    rid: int
+    z: np.ndarray  # <Z_q> for every qubit (trajectory mean for noisy requests)
+    arrival: float
+    admitted: float
+    finished: float
+    n_qubits: int
+    precision: CudaPrecision
+    n_traj: int
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def request_bytes(req: Request, sm_count: int = 148) -> int:
+    n = req.circuit.n_qubits()
+    if req.n_traj:
+        return (8 << n) * min(req.n_traj, sm_count) + 8 * req.n_traj * (n + 1)
+    return (16 if req.precision == CudaPrecision.F64 else 8) << n
+
+
+class _SvPool:
+    """Free lists of device statevectors keyed by (qubits, precision)."""
+
+    def __init__(self):
+        self._free: dict = collections.defaultdict(list)
+        self._lock = threading.Lock()
+
+    def get(self, n: int, prec: CudaPrecision) -> CudaStatevector:
+        with self._lock:
+            lst = self._free[(n, prec)]
+            if lst:
+                return lst.pop()
+        return CudaStatevector(n, prec)
+
+    def put(self, sv: CudaStatevector) -> None:
+        with self._lock:
+            self._free[(sv.n_qubits(), sv.precision())].append(sv)
+
+    def drop_all(self) -> int:
+        with self._lock:
+            n = sum(len(v) for v in self._free.values())
+            self._free.clear()
+        return n
+
+    def cached_bytes(self) -> int:
+        with self._lock:
+            return sum(sv.nbytes() for v in self._free.values() for sv in v)
+
+
+class ServingEngine:
+    def __init__(self, max_slots: int = 8, mem_budget_bytes: int | None = None, fusion_k: int = 4,
+                 traj_fusion_k: int = 3, use_graph: bool = False):
+        if mem_budget_bytes is None:
+            free, _ = cuda_free_memory_bytes()
+            mem_budget_bytes = int(free * 0.8)
+        self.max_slots = max_slots
+        self.budget = mem_budget_bytes
+        self.fusion_k = fusion_k
+        self.traj_fusion_k = traj_fusion_k
+        self.use_graph = use_graph
+        self._pool = _SvPool()
+        self._pending: collections.deque = collections.deque()
+        self._cv = threading.Condition()
+        self._in_use = 0
+        self._active = 0
+        self._stop = False
+        self._t0 = time.perf_counter()
+        self._work: collections.deque = collections.deque()
+        self._work_cv = threading.Condition()
+        self._workers = [threading.Thread(target=self._worker, daemon=True) for _ in range(max_slots)]
+        self._dispatcher = threading.Thread(target=self._dispatch, daemon=True)
+        for t in self._workers:
+            t.start()
+        self._dispatcher.start()
+        self.max_concurrent = 0
+
+    # -- public API
+    def now(self) -> float:
+        return time.perf_counter() - self._t0
+
+    def submit(self, req: Request) -> Future:
+        need = request_bytes(req)
+        if need > self.budget:
+            raise ValueError(f"request needs {need} bytes, above the device-memory budget {self.budget}")
+        fut: Future = Future()
+        with self._cv:
+            self._pending.append((req, fut, self.now()))
+            self._cv.notify_all()
+        return fut
+
+    def run_stream(self, requests: list[Request]) -> list[Result]:
+        """Submit requests at their arrival offsets (real time) and wait for all."""
+        base = self.now()
+        futs = []
+        for r in sorted(requests, key=lambda x: x.arrival):
+            delay = base + r.arrival - self.now()
+            if delay > 0:
+                time.sleep(delay)
+            futs.append(self.submit(r))
+        return [f.result() for f in futs]
+
+    def shutdown(self) -> None:
+        with self._cv:
+            self._stop = True
+            self._cv.notify_all()
+        with self._work_cv:
+            self._work_cv.notify_all()
+        self._dispatcher.join(timeout=30)
+        for t in self._workers:
+            t.join(timeout=30)
+        self._pool.drop_all()
+
+    # -- internals
+    def _dispatch(self) -> None:
+        while True:
+            with self._cv:
+                while not self._stop and not self._can_admit_head():
+                    self._cv.wait(timeout=0.05)
+                if self._stop:
+                    return
+                req, fut, t_arr = self._pending.popleft()
+                need = request_bytes(req)
+                self._in_use += need
+                self._active += 1
+                self.max_concurrent = max(self.max_concurrent, self._active)
+            with self._work_cv:
+                self._work.append((req, fut, t_arr, need, self.now()))
+                self._work_cv.notify()
+
+    def _can_admit_head(self) -> bool:
+        if not self._pending or self._active >= self.max_slots:
+            return False
+        need = request_bytes(self._pending[0][0])
+        if self._in_use + need > self.budget:
+            return False
+        if self._in_use + need + self._pool.cached_bytes() > self.budget:
+            self._pool.drop_all()  # cached statevectors go back to the device first
+        return True
+
+    def _worker(self) -> None:
+        stream = Stream()
+        while True:
+            with self._work_cv:
+                while not self._work and not self._stop:
+                    self._work_cv.wait(timeout=0.1)
+                if self._stop and not self._work:
+                    return
+                req, fut, t_arr, need, t_adm = self._work.popleft()
+            try:
+                z = self._execute(req, stream)
+                res = Result(req.rid, z, t_arr, t_adm, self.now(), req.circuit.n_qubits(),
+                             req.precision, req.n_traj)
+                fut.set_result(res)
+            except Exception as e:  # the request fails, the engine keeps serving
+                fut.set_exception(e)
+            finally:
+                with self._cv:
+                    self._in_use -= need
+                    self._active -= 1
+                    self._cv.notify_all()
+
+    def _execute(self, req: Request, stream: Stream) -> np.ndarray:
+        n = req.circuit.n_qubits()
+        if req.n_traj:
+            prog = TrajectoryProgram(req.circuit, self.traj_fusion_k)
+            z, _ = prog.run(req.n_traj, req.seed, stream, True)
+            return z.mean(axis=0)
+        fused = optimize_native(n, req.circuit.gates(), FusionConfig.size_only(self.fusion_k))
+        tol = 1e-12 if req.precision == CudaPrecision.F64 else 1e-6
+        prog = GateProgram(req.precision, n, tol, tol)
+        eb = L.errbuf()
+        L.check(L.lib().cast_b200_program_add_fused(prog.handle, fused.handle, eb, L.ERR_LEN), eb,
+                "program_add_fused")
+        sv = self._pool.get(n, req.precision)
+        try:
+            sv.zero(stream)
+            prog.run(sv, stream, self.use_graph)
+            p1, nrm = qubit_populations(sv, stream)
+            return (nrm - 2.0 * p1) / nrm
+        finally:
+            self._pool.put(sv)
+
+
+# ── workload generation and the sequential plain-path baseline ──────────────
+
+
+def make_stream(n_requests: int, rate_hz: float, seed: int, n_range=(10, 28), depth_range=(5, 40),
+                noisy_frac: float = 0.2, n_traj: int = 256, noisy_max_qubits: int = 16,
+                depolarizing: float = 1e-3) -> list[Request]:
+    """Poisson arrivals of random brickwork circuits: qubits and depth uniform in
+    the given ranges, half complex64 / half complex128, a fraction noisy
+    (depolarizing p after every gate, n_traj trajectories, at most
+    noisy_max_qubits qubits)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n_requests):
+        t += rng.exponential(1.0 / rate_hz)
+        noisy = rng.random() < noisy_frac
+        n = int(rng.integers(n_range[0], (noisy_max_qubits if noisy else n_range[1]) + 1))
+        d = int(rng.integers(depth_range[0], depth_range[1] + 1))
+        prec = CudaPrecision.F32 if (noisy or rng.random() < 0.5) else CudaPrecision.F64
+        circ = QuantumCircuit.brickwork(n, d, int(rng.integers(1 << 31)),
+                                        depolarizing=depolarizing if noisy else 0.0)
+        out.append(Request(circ, prec, n_traj if noisy else 0, int(rng.integers(1 << 31)), t, i))
+    return out
+
+
+def plain_service_time(req: Request) -> float:
+    """Run one request alone on the plain per-gate path through the drop-in C ABI
+    (compile_gate_ptx -> cubin_load -> kernel_launch for every unfused gate, the
+    reference's execution of an unfused circuit; noisy requests run host-driven
+    trajectories one by one) and return its wall time."""
+    from .cuda import CudaKernelGenSpec, CudaKernelManager
+    from .trajectory import run_plain
+
+    t0 = time.perf_counter()
+    n = req.circuit.n_qubits()
+    if req.n_traj:
+        run_plain(req.circuit, req.n_traj, req.seed)
+        return time.perf_counter() - t0
+    spec = CudaKernelGenSpec.f64() if req.precision == CudaPrecision.F64 else CudaKernelGenSpec.f32()
+    mgr = CudaKernelManager(spec, timing=False)
+    sv = CudaStatevector(n, req.precision)
+    sv.zero()
+    for g in req.circuit.gates():
+        mgr.apply(mgr.generate(g), sv)
+    mgr.sync()
+    qubit_populations(sv)
+    return time.perf_counter() - t0
+
+
+def sequential_latencies(arrivals, service_times) -> np.ndarray:
+    """Latencies of a single FIFO server that runs one request at a time."""
+    free_at = 0.0
+    out = []
+    for a, s in zip(arrivals, service_times):
+        start = max(a, free_at)
+        free_at = start + s
+        out.append(free_at - a)
+    return np.array(out)
+
+
+def latency_summary(lat) -> dict:
+    lat = np.asarray(lat)
+    return {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "mean_ms": float(lat.mean() * 1e3), "n": int(lat.size)}

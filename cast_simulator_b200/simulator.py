@@ -27,11 +27,15 @@ class Representation(enum.Enum):
 
 
 class Stream:
-    """An owned CUDA stream (cast_cuda_stream_create)."""
+    """An owned CUDA stream.  Non-blocking by default (it does not synchronise
+    with the legacy default stream, so a graph capture on it cannot be
+    invalidated by other threads' stream-0 work); ``blocking=True`` gives the
+    reference's CU_STREAM_DEFAULT kind (cast_cuda_stream_create)."""
 
-    def __init__(self):
+    def __init__(self, blocking: bool = False):
         eb = L.errbuf()
-        self.handle = L.check_ptr(L.lib().cast_cuda_stream_create(eb, L.ERR_LEN), eb, "stream")
+        fn = L.lib().cast_cuda_stream_create if blocking else L.lib().cast_b200_stream_create_nonblocking
+        self.handle = L.check_ptr(fn(eb, L.ERR_LEN), eb, "stream")
 
     def sync(self):
         eb = L.errbuf()
@@ -80,11 +84,15 @@ class Event:
 class GateProgram:
     """Ordered gates for one statevector size, uploaded once (cast_b200_program_*)."""
 
-    def __init__(self, precision: CudaPrecision, n_qubits: int, ztol: float, otol: float):
+    def __init__(self, precision: CudaPrecision, n_qubits: int, ztol: float, otol: float,
+                 split_precision: bool = False):
         eb = L.errbuf()
         self.handle = L.check_ptr(
             L.lib().cast_b200_program_create(int(precision), n_qubits, ztol, otol, eb, L.ERR_LEN), eb,
             "program_create")
+        if split_precision:
+            L.check(L.lib().cast_b200_program_set_split_precision(self.handle, 1, eb, L.ERR_LEN), eb,
+                    "set_split_precision")
         self.n_qubits = n_qubits
         self.precision = CudaPrecision(precision)
         self.gate_sizes: list[int] = []
@@ -234,9 +242,13 @@ class RunTiming:
 class Simulator:
     """Simulator<Cuda> (mod.rs:446-547)."""
 
-    def __init__(self, spec: CudaKernelGenSpec | None = None, use_graph: bool = True):
+    def __init__(self, spec: CudaKernelGenSpec | None = None, use_graph: bool = True,
+                 split_precision: bool = False):
+        """split_precision: complex64 gates with 4..6 qubits run on the tensor
+        cores in split BF16 (about 1e-5 relative error per fused pass)."""
         self.spec = spec or CudaKernelGenSpec.f64()
         self.use_graph = use_graph
+        self.split_precision = split_precision
         self._stream = None
 
     @classmethod
@@ -254,7 +266,8 @@ class Simulator:
         return self._stream
 
     def compile_batch(self, gates, n_sv: int) -> GateProgram:
-        prog = GateProgram(self.spec.precision, n_sv, self.spec.ztol, self.spec.otol)
+        prog = GateProgram(self.spec.precision, n_sv, self.spec.ztol, self.spec.otol,
+                           self.split_precision and self.spec.precision == CudaPrecision.F32)
         for i, g in enumerate(gates):
             try:
                 prog.add(g.matrix(), g.qubits())
@@ -269,7 +282,7 @@ class Simulator:
         prog = self.compile_batch(gates, n_sv)
         sv = CudaStatevector(n_sv, self.spec.precision)
         if initial is None:
-            sv.zero()
+            sv.zero(self.stream)
         else:
             sv.upload(initial)
         prog.run(sv, self.stream, self.use_graph)
@@ -290,7 +303,7 @@ class Simulator:
         e0, e1 = Event(), Event()
 
         def one():
-            sv.zero()
+            sv.zero(st)
             e0.record(st)
             prog.run(sv, st, self.use_graph)
             e1.record(st)

@@ -27,6 +27,17 @@ extern "C" {
  * (src/cpp/cuda/cuda_exec.cpp:50). */
 int cast_b200_set_device(int device, char *err_buf, size_t err_buf_len);
 
+/* -- Stream-ordered helpers ------------------------------------------------------
+ * A stream that does not synchronise with the legacy default stream (so work
+ * that other threads put on stream 0 cannot invalidate a graph capture on it),
+ * and a reset to |0...0> ordered on `stream` (cudaMemsetAsync plus one element
+ * written by a kernel; no host copy).  The reference's cast_cuda_stream_create
+ * and cast_cuda_sv_zero (src/cpp/cuda/cuda_exec.cpp:268-279, 452-479) are the
+ * blocking / host-synchronous forms. */
+void *cast_b200_stream_create_nonblocking(char *err_buf, size_t err_buf_len);
+int cast_b200_sv_zero_async(uint64_t dptr, size_t n_elements, uint8_t precision, void *stream,
+                            char *err_buf, size_t err_buf_len);
+
 /* -- Kernel path control ------------------------------------------------------
  * 0 = automatic (default), 1 = register kernel only, 2 = shared-memory tile
  * kernel wherever it applies.  For measurement and tests; returns the previous
@@ -55,6 +66,12 @@ void *cast_b200_program_create(uint8_t precision, uint32_t sv_n_qubits, double z
 int cast_b200_program_add_gate(void *program, const cast_complex64_t *matrix,
                                const uint32_t *qubits, uint32_t n_gate_qubits, char *err_buf,
                                size_t err_buf_len);
+/* Opt-in tensor-core path for complex64 programs: gates with 4..6 qubits added
+ * afterwards run as split-BF16 tensor-core GEMMs ([[A,-B],[B,A]] applied to
+ * 64-group tiles, hi/lo operand split, three products, FP32 accumulation;
+ * ~1e-5 relative error per pass).  Must be set before the first gate. */
+int cast_b200_program_set_split_precision(void *program, int enable, char *err_buf,
+                                          size_t err_buf_len);
 uint32_t cast_b200_program_num_gates(const void *program);
 int cast_b200_program_run(void *program, uint64_t sv_dptr, void *stream, int use_graph,
                           char *err_buf, size_t err_buf_len);

@@ -1,0 +1,86 @@
+"""Split-BF16 tensor-core path (complex64, fused gates with 4..6 qubits).
+
+Stated bound, per fused pass: every amplitude within 1e-4 of the largest
+reference amplitude (relative product error ~2^-16), a direction error
+1 - |<ref|psi>| / ||psi|| <= 1e-8 and a norm drift |1 - ||psi||| <= 1e-6 (the
+tensor cores' FP32 accumulation does not round to nearest, so the norm shrinks
+slightly).  A whole fused circuit, renormalised at the end, stays within
+1 - |<ref|psi>| <= 1e-6 of the FP64 oracle."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mods(cblib):
+    from cast_simulator_b200 import cuda, fusion, simulator, types
+
+    return cuda, fusion, simulator, types
+
+
+def haar(rng, d):
+    z = rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))
+    q, r = np.linalg.qr(z)
+    return q * (np.diag(r) / np.abs(np.diag(r)))
+
+
+@pytest.mark.parametrize("k", [4, 5, 6])
+def test_single_gate_within_bound(mods, oracle, k):
+    cu, F, S, T = mods
+    rng = np.random.default_rng(40 + k)
+    n = 16
+    for q in [tuple(range(n - k, n)), tuple(range(k)), tuple(sorted([0, 3] + list(range(n - k + 2, n))))]:
+        m = haar(rng, 1 << k)
+        init = oracle.random_state(n, k)
+        ref = init.copy()
+        oracle.apply_gate(ref, m, q)
+        prog = S.GateProgram(cu.CudaPrecision.F32, n, 1e-6, 1e-6, split_precision=True)
+        prog.add(m, q)
+        sv = cu.CudaStatevector(n, cu.CudaPrecision.F32)
+        sv.upload(init)
+        st = S.Stream()
+        prog.run(sv, st, use_graph=False)
+        st.sync()
+        got = sv.download()
+        rep = oracle.fidelity_report(ref, got)
+        nrm = float(np.linalg.norm(got))
+        direction = 1.0 - abs(oracle.inner(ref, got)) / nrm
+        print(f"k={k} q={q} max_err={rep['max_abs_err']:.3e} 1-|ov|={rep['one_minus_abs_overlap']:.3e} "
+              f"direction={direction:.3e} norm_drift={1 - nrm:.3e}")
+        assert rep["max_abs_err"] <= 1e-4 * np.max(np.abs(ref)), (q, rep)
+        assert direction <= 1e-8, (q, direction)
+        assert abs(1.0 - nrm) <= 1e-6, (q, nrm)
+
+
+@pytest.mark.parametrize("k", [5, 6])
+def test_fused_circuit_fidelity(mods, oracle, k):
+    cu, F, S, T = mods
+    n = 20
+    circ = T.QuantumCircuit.brickwork(n, 12, 77)
+    ref = oracle.simulate(n, [(g.matrix(), g.qubits()) for g in circ.gates()])
+    fused = F.optimize_native(n, circ.gates(), F.FusionConfig.size_only(k)).gates()
+    assert max(g.n_qubits() for g in fused) == k
+    sim = S.Simulator(cu.CudaKernelGenSpec.f32(), split_precision=True)
+    state = sim.simulate(F.CircuitGraph.from_gates(n, fused))
+    raw = state.download_amplitudes()
+    state.sv.normalize()
+    got = state.download_amplitudes()
+    rep = oracle.fidelity_report(ref, got)
+    print(f"k={k} circuit: 1-|ov| renormalised={rep['one_minus_abs_overlap']:.3e} "
+          f"raw={oracle.fidelity_report(ref, raw)['one_minus_abs_overlap']:.3e}")
+    assert rep["one_minus_abs_overlap"] <= 1e-6, rep
+    plain = S.Simulator(cu.CudaKernelGenSpec.f32()).simulate(F.CircuitGraph.from_gates(n, fused))
+    rep_plain = oracle.fidelity_report(ref, plain.download_amplitudes())
+    assert rep_plain["one_minus_abs_overlap"] <= 1e-6
+
+
+def test_split_mode_must_precede_gates(mods):
+    cu, F, S, T = mods
+    prog = S.GateProgram(cu.CudaPrecision.F32, 8, 1e-6, 1e-6)
+    prog.add(np.eye(2), (0,))
+    from cast_simulator_b200 import _lib as L
+
+    eb = L.errbuf()
+    assert L.lib().cast_b200_program_set_split_precision(prog.handle, 1, eb, L.ERR_LEN) == 1
+    assert b"before adding gates" in eb.value
