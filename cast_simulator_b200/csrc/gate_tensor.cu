@@ -14,12 +14,15 @@
 //
 // Kernel: persistent CTAs of 8 warps; each warp keeps its 16-row slices of
 // A_hi / A_lo as mma.sync A fragments in registers (packed on the host in
-// fragment order) for the whole launch.  Per tile of 64 groups the CTA loads the
-// 64 x 2^k amplitudes with coalesced 64-bit loads (consecutive groups are
-// consecutive amplitudes when the targets are high), splits them into BF16
-// hi/lo columns in shared memory (rows padded by 16 bytes: conflict-free
-// fragment loads), issues m16n8k16 BF16 MMAs, stages the FP32 result through
-// the same shared memory and stores it back coalesced.
+// fragment order) for the whole launch.  Tiles of 64 groups (64 x 2^k
+// amplitudes) are fetched with cp.async into a double buffer one tile ahead
+// (consecutive groups are consecutive amplitudes when the targets are high, so
+// the copies coalesce), split into BF16 hi/lo in shared memory in the loaded,
+// member-major orientation (rows padded by 16 bytes), turned into B fragments
+// by ldmatrix.trans and multiplied with m16n8k16 BF16 MMAs; the FP32 result is
+// staged through the same shared memory and stored back coalesced (stores
+// straight from the accumulator fragments scatter over 8 member rows per
+// instruction and measured slower).
 #include "internal.hpp"
 
 #include <cuda_bf16.h>
@@ -41,12 +44,31 @@ template <int K> struct TcCfg {
   static constexpr int WN = 8 / MT;           // warps sharing one m-tile
   static constexpr int NF = (kTcG / 8) / WN;  // n8 fragments per warp
   static constexpr int KS = R / 16;           // k16 steps
-  static constexpr int SK = R + 8;            // bf16 elements per X row (one row per group)
-  static constexpr int SG = kTcG + 4;         // floats per Y row (one row per real output)
-  static constexpr size_t XBYTES = 2ull * kTcG * SK * sizeof(__nv_bfloat16);
+  static constexpr int SN = kTcG + 8;         // bf16 elements per X row (one row per real input)
+  static constexpr int AMPS = kTcG * D;        // amplitudes per tile
+  static constexpr int PER = AMPS / kTcThreads;  // per thread
+  static constexpr size_t STAGE = 2ull * AMPS * sizeof(float2);  // double-buffered raw tiles
+  static constexpr int SG = kTcG + 4;         // floats per staged result row
+  static constexpr size_t XBYTES = 2ull * R * SN * sizeof(__nv_bfloat16);
   static constexpr size_t YBYTES = (size_t)R * SG * sizeof(float);
-  static constexpr size_t SMEM = XBYTES > YBYTES ? XBYTES : YBYTES;
+  static constexpr size_t SMEM = STAGE + (XBYTES > YBYTES ? XBYTES : YBYTES);
 };
+
+__device__ __forceinline__ void cp_async8(void *smem_dst, const void *gmem_src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+// Four transposed 8x8 b16 tiles: lanes 8j..8j+7 give the row addresses of tile j.
+__device__ __forceinline__ void ldsm_x4_trans(uint32_t (&r)[4], const void *row_addr) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(row_addr);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
+}
 
 struct TcTargets {
   uint64_t lo_mask[kMaxGateQubits];
@@ -78,15 +100,19 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], 
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// The raw tile of the next iteration is fetched with cp.async into the other
+// half of a double buffer while this iteration splits, multiplies and stores.
 template <int K>
 __global__ void __launch_bounds__(kTcThreads, 2)
     k_gate_tc(float2 *__restrict__ psi, uint64_t n_groups, TcTargets t,
               const uint32_t *__restrict__ afrag) {
   using C = TcCfg<K>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __nv_bfloat16 *Xhi = reinterpret_cast<__nv_bfloat16 *>(smem_raw);
-  __nv_bfloat16 *Xlo = Xhi + kTcG * C::SK;
-  float *Ys = reinterpret_cast<float *>(smem_raw);  // aliases X once the MMAs are done
+  float2 *stage = reinterpret_cast<float2 *>(smem_raw);  // [2][D][kTcG]
+  unsigned char *xy = smem_raw + C::STAGE;
+  __nv_bfloat16 *Xhi = reinterpret_cast<__nv_bfloat16 *>(xy);
+  __nv_bfloat16 *Xlo = Xhi + C::R * C::SN;
+  float *Ys = reinterpret_cast<float *>(xy);  // aliases X once the MMAs are done
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int mt = warp % C::MT, wn = warp / C::MT;
   uint32_t ah[C::KS][4], al[C::KS][4];
@@ -100,57 +126,90 @@ __global__ void __launch_bounds__(kTcThreads, 2)
       al[ks][i] = fl[idx];
     }
   const uint64_t n_tiles = (n_groups + kTcG - 1) / kTcG;
-  for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+  auto issue = [&](uint64_t tile, int buf) {
     const uint64_t g0 = tile * kTcG;
-    for (int i = threadIdx.x; i < kTcG * C::D; i += kTcThreads) {
+    float2 *dst = stage + buf * C::AMPS;
+#pragma unroll
+    for (int j = 0; j < C::PER; ++j) {
+      const int i = threadIdx.x + j * kTcThreads;
       const int gg = i % kTcG, a = i / kTcG;
       const uint64_t g = g0 + gg;
-      float2 v = make_float2(0.f, 0.f);
-      if (g < n_groups) v = psi[tc_base<K>(g, t) + tc_off<K>(a, t)];
-      const __nv_bfloat16 hr = __float2bfloat16_rn(v.x), hi = __float2bfloat16_rn(v.y);
-      Xhi[gg * C::SK + a] = hr;
-      Xhi[gg * C::SK + C::D + a] = hi;
-      Xlo[gg * C::SK + a] = __float2bfloat16_rn(v.x - __bfloat162float(hr));
-      Xlo[gg * C::SK + C::D + a] = __float2bfloat16_rn(v.y - __bfloat162float(hi));
+      if (g < n_groups) cp_async8(dst + i, psi + tc_base<K>(g, t) + tc_off<K>(a, t));
+      else dst[i] = make_float2(0.f, 0.f);
+    }
+    cp_async_commit();
+  };
+  uint64_t tile = blockIdx.x;
+  int buf = 0;
+  if (tile < n_tiles) issue(tile, 0);
+  for (; tile < n_tiles; tile += gridDim.x, buf ^= 1) {
+    const uint64_t next = tile + gridDim.x;
+    if (next < n_tiles) issue(next, buf ^ 1);
+    else cp_async_commit();  // an empty group keeps wait_group<1> meaning "tile landed"
+    cp_async_wait<1>();
+    __syncthreads();
+    // split: member-major X[k][group]; each thread converts two adjacent groups
+    // of one member (a 16-byte read, 32-bit stores, both conflict-free)
+    const float2 *cur = stage + buf * C::AMPS;
+#pragma unroll
+    for (int j = 0; j < C::PER / 2; ++j) {
+      const int i = threadIdx.x + j * kTcThreads;
+      const int gg = 2 * (i % (kTcG / 2)), a = i / (kTcG / 2);
+      const float4 v = *reinterpret_cast<const float4 *>(cur + a * kTcG + gg);
+      const __nv_bfloat162 hr = __floats2bfloat162_rn(v.x, v.z);
+      const __nv_bfloat162 hi = __floats2bfloat162_rn(v.y, v.w);
+      const __nv_bfloat162 lr = __floats2bfloat162_rn(v.x - __low2float(hr), v.z - __high2float(hr));
+      const __nv_bfloat162 li = __floats2bfloat162_rn(v.y - __low2float(hi), v.w - __high2float(hi));
+      *reinterpret_cast<__nv_bfloat162 *>(&Xhi[a * C::SN + gg]) = hr;
+      *reinterpret_cast<__nv_bfloat162 *>(&Xhi[(C::D + a) * C::SN + gg]) = hi;
+      *reinterpret_cast<__nv_bfloat162 *>(&Xlo[a * C::SN + gg]) = lr;
+      *reinterpret_cast<__nv_bfloat162 *>(&Xlo[(C::D + a) * C::SN + gg]) = li;
     }
     __syncthreads();
     float acc[C::NF][4];
 #pragma unroll
     for (int nf = 0; nf < C::NF; ++nf) acc[nf][0] = acc[nf][1] = acc[nf][2] = acc[nf][3] = 0.f;
+    const int lrow = (lane & 7) + ((lane >> 3) & 1) * 8;  // k row within the k16 step
+    const int lcol = (lane >> 4) * 8;                     // n offset: second fragment of the pair
 #pragma unroll
     for (int ks = 0; ks < C::KS; ++ks) {
-      const int kb = ks * 16 + 2 * (lane & 3);
 #pragma unroll
-      for (int nf = 0; nf < C::NF; ++nf) {
-        const int n = (wn * C::NF + nf) * 8 + (lane >> 2);
-        const uint32_t bh0 = *reinterpret_cast<const uint32_t *>(&Xhi[n * C::SK + kb]);
-        const uint32_t bh1 = *reinterpret_cast<const uint32_t *>(&Xhi[n * C::SK + kb + 8]);
-        const uint32_t bl0 = *reinterpret_cast<const uint32_t *>(&Xlo[n * C::SK + kb]);
-        const uint32_t bl1 = *reinterpret_cast<const uint32_t *>(&Xlo[n * C::SK + kb + 8]);
-        mma_bf16(acc[nf], al[ks], bh0, bh1);
-        mma_bf16(acc[nf], ah[ks], bl0, bl1);
-        mma_bf16(acc[nf], ah[ks], bh0, bh1);
+      for (int nf = 0; nf < C::NF; nf += 2) {
+        const int off = (ks * 16 + lrow) * C::SN + (wn * C::NF + nf) * 8 + lcol;
+        uint32_t bh[4], bl[4];
+        ldsm_x4_trans(bh, &Xhi[off]);
+        ldsm_x4_trans(bl, &Xlo[off]);
+        mma_bf16(acc[nf], al[ks], bh[0], bh[1]);
+        mma_bf16(acc[nf], ah[ks], bl[0], bl[1]);
+        mma_bf16(acc[nf], ah[ks], bh[0], bh[1]);
+        mma_bf16(acc[nf + 1], al[ks], bh[2], bh[3]);
+        mma_bf16(acc[nf + 1], ah[ks], bl[2], bl[3]);
+        mma_bf16(acc[nf + 1], ah[ks], bh[2], bh[3]);
       }
     }
-    __syncthreads();
+    __syncthreads();  // X is free: the result tile is staged in its place
+    // m-tile mt holds Re (rows 0-7) and Im (rows 8-15) of members 8mt..8mt+7
 #pragma unroll
     for (int nf = 0; nf < C::NF; ++nf) {
       const int r0 = mt * 16 + (lane >> 2), c0 = (wn * C::NF + nf) * 8 + 2 * (lane & 3);
-      Ys[r0 * C::SG + c0] = acc[nf][0];
-      Ys[r0 * C::SG + c0 + 1] = acc[nf][1];
-      Ys[(r0 + 8) * C::SG + c0] = acc[nf][2];
-      Ys[(r0 + 8) * C::SG + c0 + 1] = acc[nf][3];
+      *reinterpret_cast<float2 *>(&Ys[r0 * C::SG + c0]) = make_float2(acc[nf][0], acc[nf][1]);
+      *reinterpret_cast<float2 *>(&Ys[(r0 + 8) * C::SG + c0]) = make_float2(acc[nf][2], acc[nf][3]);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kTcG * C::D; i += kTcThreads) {
+    const uint64_t g0 = tile * kTcG;
+#pragma unroll
+    for (int j = 0; j < C::PER; ++j) {
+      const int i = threadIdx.x + j * kTcThreads;
       const int gg = i % kTcG, a = i / kTcG;
+      const int row = (a >> 3) * 16 + (a & 7);
       const uint64_t g = g0 + gg;
       if (g < n_groups)
         psi[tc_base<K>(g, t) + tc_off<K>(a, t)] =
-            make_float2(Ys[a * C::SG + gg], Ys[(C::D + a) * C::SG + gg]);
+            make_float2(Ys[row * C::SG + gg], Ys[(row + 8) * C::SG + gg]);
     }
     __syncthreads();
   }
+  cp_async_wait<0>();
 }
 
 uint16_t bf16_bits_rn(float f) {
@@ -176,6 +235,9 @@ bool launch_tc_k(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::s
   std::call_once(once, [] {
     attr_rc = cudaFuncSetAttribute(k_gate_tc<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)C::SMEM);
+    if (attr_rc == cudaSuccess)
+      attr_rc = cudaFuncSetAttribute(k_gate_tc<K>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     cudaSharedmemCarveoutMaxShared);
     int b = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_gate_tc<K>, kTcThreads, C::SMEM) ==
             cudaSuccess &&
@@ -204,23 +266,28 @@ bool tensor_path_supported(const GateData &g) {
   return g.precision == 0 && g.k >= 4 && g.k <= 6;
 }
 
-// Packs [[A, -B], [B, A]] into mma.sync m16n8k16 A fragments (row-major 16x16
-// per fragment; a0..a3 = rows gid / gid+8, columns 2t..2t+1 / 2t+8..2t+9), hi
-// fragments first, then lo, and uploads them.
+// Packs [[A, -B], [B, A]] (rows permuted as below) into mma.sync m16n8k16 A
+// fragments (row-major 16x16 per fragment; a0..a3 = rows gid / gid+8, columns
+// 2t..2t+1 / 2t+8..2t+9), hi fragments first, then lo, and uploads them.
 bool prepare_tensor_gate(GateData &g, std::string &err) {
   if (!tensor_path_supported(g)) {
     err = "the tensor-core path takes complex64 gates with 4..6 qubits";
     return false;
   }
   const int D = 1 << g.k, R = 2 * D, MT = R / 16, KS = R / 16;
+  // Rows are ordered per m16 tile: tile mt = Re rows of members 8mt..8mt+7, then
+  // their Im rows; columns are [Re x ; Im x].
   std::vector<double> Mr((size_t)R * R);
-  for (int r = 0; r < D; ++r)
-    for (int c = 0; c < D; ++c) {
-      const double a = g.m64[2 * (r * D + c)], b = g.m64[2 * (r * D + c) + 1];
-      Mr[(size_t)r * R + c] = a;
-      Mr[(size_t)r * R + D + c] = -b;
-      Mr[(size_t)(D + r) * R + c] = b;
-      Mr[(size_t)(D + r) * R + D + c] = a;
+  for (int mt = 0; mt < MT; ++mt)
+    for (int j = 0; j < 16; ++j) {
+      const int r = mt * 8 + (j & 7);  // member
+      const bool im = j >= 8;
+      double *row = &Mr[(size_t)(mt * 16 + j) * R];
+      for (int c = 0; c < D; ++c) {
+        const double a = g.m64[2 * (r * D + c)], b = g.m64[2 * (r * D + c) + 1];
+        row[c] = im ? b : a;       // x_re coefficient
+        row[D + c] = im ? a : -b;  // x_im coefficient
+      }
     }
   std::vector<uint16_t> hi((size_t)R * R), lo((size_t)R * R);
   for (size_t i = 0; i < Mr.size(); ++i) {
