@@ -37,6 +37,12 @@ def device_sm() -> tuple[int, int]:
     return ma.value, mi.value
 
 
+def set_device(device: int) -> None:
+    """Make ``device`` current for this host thread (cudaSetDevice)."""
+    eb = L.errbuf()
+    L.check(L.lib().cast_b200_set_device(int(device), eb, L.ERR_LEN), eb, "set_device")
+
+
 def cuda_free_memory_bytes() -> tuple[int, int]:
     """(free, total) device memory in bytes (mod.rs:62-73)."""
     eb = L.errbuf()
