@@ -235,6 +235,20 @@ int cast_b200_program_set_split_precision(void *program, int enable, char *err_b
   return 0;
 }
 
+int cast_b200_tensor_status(uint32_t *out_bits, char *err_buf, size_t err_buf_len) {
+  if (!out_bits) {
+    write_err(err_buf, err_buf_len, "out_bits is null");
+    return 1;
+  }
+  std::string err;
+  if (!cb2::tensor_error_status(out_bits, err)) {
+    write_err(err_buf, err_buf_len, err);
+    return 1;
+  }
+  clear_err(err_buf, err_buf_len);
+  return 0;
+}
+
 uint32_t cast_b200_program_num_gates(const void *program) {
   const Program *p = static_cast<const Program *>(program);
   return p && p->magic == kProgramMagic ? (uint32_t)p->gates.size() : 0;

@@ -1,28 +1,40 @@
-// Tensor-core gate application for complex64 statevectors, k = 4, 5, 6.
+// Tensor-core gate application for complex64 statevectors, k = 5, 6, on the
+// fifth-generation tensor cores (tcgen05.mma, accumulators in tensor memory).
 //
-// A fused k-qubit gate M = A + iB (2^k x 2^k) applied to G gather groups is the
-// real GEMM
-//     [Yr]   [A  -B] [Xr]
-//     [Yi] = [B   A] [Xi]        (R x R) x (R x G),  R = 2^(k+1),
-// with one column per group (X rows = real parts then imaginary parts of the
-// group's 2^k members).  It runs on the tensor cores in split BF16: every FP32
-// operand v is written as hi + lo with hi = bf16(v), lo = bf16(v - hi), and
-// Y = A_lo X_hi + A_hi X_lo + A_hi X_hi with FP32 accumulation (the lo*lo term,
-// below 2^-16 of the product, is dropped).  Relative error per product is about
-// 2^-16, so a fused pass changes an amplitude by ~1e-5 of the norm of its group
-// - the bound the tests state.
+// A fused k-qubit gate M = A + iB (D x D, D = 2^k) applied to the gather groups
+// of a statevector is a real GEMM with R = 2D reals per group.  It is issued
+// transposed, one tile of 128 groups at a time:
 //
-// Kernel: persistent CTAs of 8 warps; each warp keeps its 16-row slices of
-// A_hi / A_lo as mma.sync A fragments in registers (packed on the host in
-// fragment order) for the whole launch.  Tiles of 64 groups (64 x 2^k
-// amplitudes) are fetched with cp.async into a double buffer one tile ahead
-// (consecutive groups are consecutive amplitudes when the targets are high, so
-// the copies coalesce), split into BF16 hi/lo in shared memory in the loaded,
-// member-major orientation (rows padded by 16 bytes), turned into B fragments
-// by ldmatrix.trans and multiplied with m16n8k16 BF16 MMAs; the FP32 result is
-// staged through the same shared memory and stored back coalesced (stores
-// straight from the accumulator fragments scatter over 8 member rows per
-// instruction and measured slower).
+//     Y^T (128 x R)  =  X^T (128 x R) . Mr^T,     Mr[2r+c'][2m+c] = the real
+//     2x2 block [[A, -B], [B, A]] of M[r][m] (c, c' = 0 real, 1 imaginary),
+//
+// so the tile's groups are the MMA's M = 128 rows (one tensor-memory lane per
+// group), the gate is the resident N x K = R x R operand, and the k16 loop runs
+// over the group's members (Re, Im interleaved, exactly as the amplitudes lie in
+// memory).  Every FP32 operand v is split into BF16 hi + lo (hi = bf16(v),
+// lo = bf16(v - hi)) and Y = X_lo M_hi + X_hi M_lo + X_hi M_hi is accumulated in
+// FP32 in tensor memory (the lo*lo term, below 2^-16 of the product, is
+// dropped): about 2^-16 relative error per product, ~1e-5 of the group norm per
+// fused pass.
+//
+// One persistent CTA per SM, warp-specialised:
+//   warps 0-3   epilogue: tensor memory -> registers (tcgen05.ld 32x32b, lane =
+//               group) -> coalesced 8-byte stores, 32 consecutive groups of one
+//               member per warp instruction;
+//   warps 4-19  loaders: 8-byte global loads of 4 members per (group, chunk),
+//               split into BF16 hi/lo in registers, 16-byte shared stores in the
+//               UMMA K-major layout with the 128-byte swizzle (8 rows x 128 B
+//               atoms, the 16-byte chunk index XORed with the row: conflict-free
+//               for these stores and for the tensor core's operand reads);
+//   warp 20     allocates tensor memory and issues the MMAs (one thread).
+// The loader warps form 2^(7-k) groups; group j fills operand stage j with every
+// (2^(7-k))-th tile, so 128 KB of loads per SM are in flight for every k (one
+// tile's worth per group; a single group would leave the loads latency-bound).
+// Shared memory holds the gate (hi and lo) for the whole launch plus the stages;
+// tensor memory holds two accumulators so the epilogue of one tile overlaps the
+// MMAs of the next.  Every wait on an mbarrier is bounded:
+// on expiry the CTA records an error code (read back by tensor_error_status),
+// drains its outstanding MMAs, frees its tensor memory and exits.
 #include "internal.hpp"
 
 #include <cuda_bf16.h>
@@ -34,41 +46,51 @@ namespace cb2 {
 
 namespace {
 
-constexpr int kTcThreads = 256;
-constexpr int kTcG = 64;  // groups per tile
+constexpr int kTileGroups = 128;                   // MMA M: one TMEM lane per group
+constexpr int kEpiWarps = 4;                       // warps 0-3 (TMEM sub-partitions 0-3)
+constexpr int kLoadWarps = 16;                     // warps 4-19
+constexpr int kMmaWarp = kEpiWarps + kLoadWarps;   // warp 20
+constexpr int kUmThreads = (kMmaWarp + 1) * 32;    // 672
+constexpr int kLoadThreads = kLoadWarps * 32;
+constexpr int kLoadItems = 8;                      // 16-byte chunks per loader thread per tile
+constexpr uint32_t kSuspendNs = 20000;             // hardware suspend hint per try_wait poll
+constexpr uint32_t kSpinLimit = 1u << 16;          // polls before a wait gives up (<= ~1.3 s)
 
-template <int K> struct TcCfg {
+// error bits recorded in g_umma_error
+constexpr uint32_t kErrLoaderWait = 1, kErrMmaFullWait = 2, kErrMmaAccWait = 4,
+                   kErrEpilogueWait = 8, kErrDrainWait = 16;
+
+__device__ uint32_t g_umma_error;
+
+template <int K> struct UmCfg {
   static constexpr int D = 1 << K;
-  static constexpr int R = 2 * D;             // real rows / columns of the GEMM
-  static constexpr int MT = R / 16;           // m16 tiles
-  static constexpr int WN = 8 / MT;           // warps sharing one m-tile
-  static constexpr int NF = (kTcG / 8) / WN;  // n8 fragments per warp
-  static constexpr int KS = R / 16;           // k16 steps
-  static constexpr int SN = kTcG + 8;         // bf16 elements per X row (one row per real input)
-  static constexpr int AMPS = kTcG * D;        // amplitudes per tile
-  static constexpr int PER = AMPS / kTcThreads;  // per thread
-  static constexpr size_t STAGE = 2ull * AMPS * sizeof(float2);  // double-buffered raw tiles
-  static constexpr int SG = kTcG + 4;         // floats per staged result row
-  static constexpr size_t XBYTES = 2ull * R * SN * sizeof(__nv_bfloat16);
-  static constexpr size_t YBYTES = (size_t)R * SG * sizeof(float);
-  static constexpr size_t SMEM = STAGE + (XBYTES > YBYTES ? XBYTES : YBYTES);
+  static constexpr int R = 2 * D;                          // reals per group: MMA N and K extent
+  static constexpr int CH = D / 4;                         // 16-byte chunks (4 members) per group
+  static constexpr int LG = kLoadThreads * kLoadItems / (kTileGroups * CH);  // loader groups
+  static constexpr int GS = kLoadThreads / LG;             // threads per loader group
+  static constexpr uint32_t ATOM_X = kTileGroups * 128;    // one 64-wide K block of X (all rows)
+  static constexpr uint32_t ATOM_G = R * 128;              // one 64-wide K block of Mr
+  static constexpr uint32_t XBYTES = kTileGroups * R * 2;  // one BF16 operand tile (hi or lo)
+  static constexpr uint32_t GBYTES = R * R * 2;            // one BF16 gate (hi or lo)
+  static constexpr uint32_t STAGE = 2 * XBYTES;
+  static constexpr int S = LG;                             // operand stages: one per loader group
+  static constexpr int KS = R / 16;                        // k16 steps
+  static constexpr uint32_t TCOLS = 2 * R;                 // two FP32 accumulators of N = R columns
+  static constexpr uint32_t NBARS = 2 * S + 5;             // full, empty, accfull x2, accempty x2, drain
+  static constexpr uint32_t OFF_BARS = 2 * GBYTES + S * STAGE;
+  static constexpr uint32_t OFF_MOFF = OFF_BARS + NBARS * 8;         // member offsets (u64 x D)
+  static constexpr uint32_t OFF_MISC = OFF_MOFF + D * 8;             // tmem slot, abort flag
+  static constexpr uint32_t SMEM = OFF_MISC + 16 + 1024;              // + 1024-byte alignment slack
+  // kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both K-major,
+  // N = R, M = 128.
+  static constexpr uint32_t IDESC =
+      (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(R >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  static_assert(LG * GS == kLoadThreads && GS * kLoadItems == kTileGroups * CH, "loader mapping");
+  static_assert(GS % 32 == 0 && (GS % kTileGroups == 0 || kTileGroups % GS == 0), "loader groups");
+  static_assert(K >= 5 && R % 64 == 0 && R <= 256, "N, and K blocks of one 128-byte swizzle atom");
+  static_assert(TCOLS >= 32 && (TCOLS & (TCOLS - 1)) == 0 && TCOLS <= 512, "TMEM columns");
+  static_assert(SMEM <= 227 * 1024, "shared memory");
 };
-
-__device__ __forceinline__ void cp_async8(void *smem_dst, const void *gmem_src) {
-  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-// Four transposed 8x8 b16 tiles: lanes 8j..8j+7 give the row addresses of tile j.
-__device__ __forceinline__ void ldsm_x4_trans(uint32_t (&r)[4], const void *row_addr) {
-  const uint32_t a = (uint32_t)__cvta_generic_to_shared(row_addr);
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-               : "r"(a));
-}
 
 struct TcTargets {
   uint64_t lo_mask[kMaxGateQubits];
@@ -91,125 +113,286 @@ __device__ __forceinline__ uint64_t tc_off(int a, const TcTargets &t) {
   return o;
 }
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
-                                         uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-      "{%8,%9}, {%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// The raw tile of the next iteration is fetched with cp.async into the other
-// half of a double buffer while this iteration splits, multiplies and stores.
-template <int K>
-__global__ void __launch_bounds__(kTcThreads, 2)
-    k_gate_tc(float2 *__restrict__ psi, uint64_t n_groups, TcTargets t,
-              const uint32_t *__restrict__ afrag) {
-  using C = TcCfg<K>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2 *stage = reinterpret_cast<float2 *>(smem_raw);  // [2][D][kTcG]
-  unsigned char *xy = smem_raw + C::STAGE;
-  __nv_bfloat16 *Xhi = reinterpret_cast<__nv_bfloat16 *>(xy);
-  __nv_bfloat16 *Xlo = Xhi + C::R * C::SN;
-  float *Ys = reinterpret_cast<float *>(xy);  // aliases X once the MMAs are done
+__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t a) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(a) : "memory");
+}
+// One poll: the thread is suspended in hardware until the phase completes or
+// kSuspendNs elapse, so waiting warps take no issue slots from working ones.
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(a), "r"(parity), "r"(kSuspendNs)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the phase of parity `parity`.  Returns false when another
+// role has aborted or the poll limit expired (then the abort flag and `code`
+// are recorded).
+__device__ __noinline__ bool mbar_wait(uint32_t a, uint32_t parity, volatile uint32_t *abort_flag,
+                                       uint32_t code) {
+  for (uint32_t i = 0; i < kSpinLimit; ++i) {
+    if (mbar_try(a, parity)) return true;
+    if ((i & 15) == 15 && *abort_flag) return false;
+  }
+  *abort_flag = 1;
+  atomicOr(&g_umma_error, code);
+  return false;
+}
+// Warp-uniform form: lane 0 waits, the outcome is broadcast.
+__device__ __forceinline__ bool mbar_wait_warp(uint32_t a, uint32_t parity,
+                                               volatile uint32_t *abort_flag, uint32_t code) {
+  int ok = 0;
+  if ((threadIdx.x & 31) == 0) ok = mbar_wait(a, parity, abort_flag, code) ? 1 : 0;
+  return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tc_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                   mbar)
+               : "memory");
+}
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
+                                       uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+// 32 lanes x 32 consecutive FP32 columns; the wait is in the same asm block so
+// no use of the registers can be scheduled before the data has landed.
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+      "%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared-memory matrix descriptor, K-major with the 128-byte swizzle: rows of
+// 128 bytes (64 BF16 along K), 8-row atoms 1024 bytes apart (SBO), leading
+// offset unused (1), version 1 (bits 46-47), layout type 2 (bits 61-63).  The
+// start address steps by 32 bytes per k16 inside an atom.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         (1ull << 46) | (2ull << 61);
+}
+
+__device__ __forceinline__ uint32_t bf162_bits(__nv_bfloat162 v) {
+  return *reinterpret_cast<uint32_t *>(&v);
+}
+
+// Off: type of the member offsets (uint32_t while every amplitude index fits,
+// which makes each load/store address one wide multiply-add).
+template <int K, typename Off>
+__global__ void __launch_bounds__(kUmThreads, 1)
+    k_gate_umma(float2 *__restrict__ psi, uint64_t n_groups, TcTargets t,
+                const uint4 *__restrict__ gate) {
+  using C = UmCfg<K>;
+  extern __shared__ __align__(1024) unsigned char smem_dyn[];
+  unsigned char *sm = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~static_cast<uintptr_t>(1023));
+  const uint32_t s_gate = smem_u32(sm);               // hi at +0, lo at +GBYTES
+  const uint32_t s_stage = s_gate + 2 * C::GBYTES;     // stage i: hi at +i*STAGE, lo at +XBYTES
+  const uint32_t s_bar = s_gate + C::OFF_BARS;
+  auto full_bar = [&](int s) { return s_bar + 8u * s; };
+  auto empty_bar = [&](int s) { return s_bar + 8u * (C::S + s); };
+  auto accfull_bar = [&](int b) { return s_bar + 8u * (2 * C::S + b); };
+  auto accempty_bar = [&](int b) { return s_bar + 8u * (2 * C::S + 2 + b); };
+  const uint32_t drain_bar = s_bar + 8u * (2 * C::S + 4);
+  Off *moff = reinterpret_cast<Off *>(sm + C::OFF_MOFF);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sm + C::OFF_MISC);
+  volatile uint32_t *abort_flag = tmem_slot + 1;
+
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int mt = warp % C::MT, wn = warp / C::MT;
-  uint32_t ah[C::KS][4], al[C::KS][4];
-  const uint32_t *fh = afrag, *fl = afrag + (size_t)C::MT * C::KS * 128;
-#pragma unroll
-  for (int ks = 0; ks < C::KS; ++ks)
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const size_t idx = (((size_t)mt * C::KS + ks) * 32 + lane) * 4 + i;
-      ah[ks][i] = fh[idx];
-      al[ks][i] = fl[idx];
+  const uint64_t n_tiles = (n_groups + kTileGroups - 1) / kTileGroups;
+
+  // gate (packed on the host in the operand layout) and member offsets
+  {
+    uint4 *dst = reinterpret_cast<uint4 *>(sm);
+    for (uint32_t i = threadIdx.x; i < 2 * C::GBYTES / 16; i += kUmThreads) dst[i] = gate[i];
+    for (int m = threadIdx.x; m < C::D; m += kUmThreads) moff[m] = (Off)tc_off<K>(m, t);
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < C::S; ++s) {
+      mbar_init(full_bar(s), C::GS);
+      mbar_init(empty_bar(s), 1);
     }
-  const uint64_t n_tiles = (n_groups + kTcG - 1) / kTcG;
-  auto issue = [&](uint64_t tile, int buf) {
-    const uint64_t g0 = tile * kTcG;
-    float2 *dst = stage + buf * C::AMPS;
-#pragma unroll
-    for (int j = 0; j < C::PER; ++j) {
-      const int i = threadIdx.x + j * kTcThreads;
-      const int gg = i % kTcG, a = i / kTcG;
-      const uint64_t g = g0 + gg;
-      if (g < n_groups) cp_async8(dst + i, psi + tc_base<K>(g, t) + tc_off<K>(a, t));
-      else dst[i] = make_float2(0.f, 0.f);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accfull_bar(b), 1);
+      mbar_init(accempty_bar(b), kEpiWarps * 32);
     }
-    cp_async_commit();
-  };
-  uint64_t tile = blockIdx.x;
-  int buf = 0;
-  if (tile < n_tiles) issue(tile, 0);
-  for (; tile < n_tiles; tile += gridDim.x, buf ^= 1) {
-    const uint64_t next = tile + gridDim.x;
-    if (next < n_tiles) issue(next, buf ^ 1);
-    else cp_async_commit();  // an empty group keeps wait_group<1> meaning "tile landed"
-    cp_async_wait<1>();
-    __syncthreads();
-    // split: member-major X[k][group]; each thread converts two adjacent groups
-    // of one member (a 16-byte read, 32-bit stores, both conflict-free)
-    const float2 *cur = stage + buf * C::AMPS;
+    mbar_init(drain_bar, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  fence_async_smem();  // the gate's generic stores become visible to the tensor core
+  if (warp == kMmaWarp) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(C::TCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == kMmaWarp) {
+    // ---- MMA issuer ----------------------------------------------------------
+    uint32_t it = 0;
+    bool issued = false;
+    for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++it) {
+      const uint32_t s = it % C::S, u = it / C::S, b = it & 1, v = it >> 1;
+      if (!mbar_wait_warp(full_bar(s), u & 1, abort_flag, kErrMmaFullWait)) break;
+      if (!mbar_wait_warp(accempty_bar(b), (v & 1) ^ 1, abort_flag, kErrMmaAccWait)) break;
+      tc_fence_after();
+      if (lane == 0) {
+        const uint32_t xh = s_stage + s * C::STAGE, xl = xh + C::XBYTES;
+        const uint32_t gh = s_gate, gl = s_gate + C::GBYTES;
+        const uint32_t d = tmem + b * C::R;
 #pragma unroll
-    for (int j = 0; j < C::PER / 2; ++j) {
-      const int i = threadIdx.x + j * kTcThreads;
-      const int gg = 2 * (i % (kTcG / 2)), a = i / (kTcG / 2);
-      const float4 v = *reinterpret_cast<const float4 *>(cur + a * kTcG + gg);
-      const __nv_bfloat162 hr = __floats2bfloat162_rn(v.x, v.z);
-      const __nv_bfloat162 hi = __floats2bfloat162_rn(v.y, v.w);
-      const __nv_bfloat162 lr = __floats2bfloat162_rn(v.x - __low2float(hr), v.z - __high2float(hr));
-      const __nv_bfloat162 li = __floats2bfloat162_rn(v.y - __low2float(hi), v.w - __high2float(hi));
-      *reinterpret_cast<__nv_bfloat162 *>(&Xhi[a * C::SN + gg]) = hr;
-      *reinterpret_cast<__nv_bfloat162 *>(&Xhi[(C::D + a) * C::SN + gg]) = hi;
-      *reinterpret_cast<__nv_bfloat162 *>(&Xlo[a * C::SN + gg]) = lr;
-      *reinterpret_cast<__nv_bfloat162 *>(&Xlo[(C::D + a) * C::SN + gg]) = li;
+        for (int ks = 0; ks < C::KS; ++ks) {
+          const uint32_t ox = (ks / 4) * C::ATOM_X + (ks % 4) * 32;
+          const uint32_t og = (ks / 4) * C::ATOM_G + (ks % 4) * 32;
+          const uint64_t a_hi = umma_desc_sw128(xh + ox), a_lo = umma_desc_sw128(xl + ox);
+          const uint64_t b_hi = umma_desc_sw128(gh + og), b_lo = umma_desc_sw128(gl + og);
+          tc_mma(d, a_lo, b_hi, C::IDESC, ks > 0 ? 1u : 0u);
+          tc_mma(d, a_hi, b_lo, C::IDESC, 1u);
+          tc_mma(d, a_hi, b_hi, C::IDESC, 1u);
+        }
+        tc_commit(empty_bar(s));
+        tc_commit(accfull_bar(b));
+      }
+      __syncwarp();
+      issued = true;
     }
-    __syncthreads();
-    float acc[C::NF][4];
+    // every MMA of this CTA has completed before tensor memory is released
+    if (issued) {
+      if (lane == 0) tc_commit(drain_bar);
+      __syncwarp();
+      volatile uint32_t never = 0;
+      mbar_wait_warp(drain_bar, 0, &never, kErrDrainWait);
+    }
+  } else if (warp >= kEpiWarps) {
+    // ---- loaders: HBM -> split BF16 -> operand stage --------------------------
+    // group lg owns stage lg and the CTA's tiles it = lg, lg + LG, ...; item i of
+    // a tile (i = lt' + GS * j) is chunk i / 128 of group i % 128, so a warp
+    // covers 32 consecutive groups of one chunk.
+    const int lt = threadIdx.x - kEpiWarps * 32;
+    const int lg = lt / C::GS, lp = lt % C::GS;
+    // group bases split as pdep(tile * 128) | pdep(gg): the second part is fixed
+    // for the launch (one value, or two when a loader group is 64 threads wide)
+    constexpr int NGB = C::GS >= kTileGroups ? 1 : kTileGroups / C::GS;
+    uint64_t gb[NGB];
 #pragma unroll
-    for (int nf = 0; nf < C::NF; ++nf) acc[nf][0] = acc[nf][1] = acc[nf][2] = acc[nf][3] = 0.f;
-    const int lrow = (lane & 7) + ((lane >> 3) & 1) * 8;  // k row within the k16 step
-    const int lcol = (lane >> 4) * 8;                     // n offset: second fragment of the pair
+    for (int i = 0; i < NGB; ++i) gb[i] = tc_base<K>((uint64_t)((lp + C::GS * i) % kTileGroups), t);
+    unsigned char *xh = sm + 2 * C::GBYTES + lg * C::STAGE, *xl = xh + C::XBYTES;
+    for (uint32_t it = lg;; it += C::LG) {
+      const uint64_t tile = blockIdx.x + (uint64_t)it * gridDim.x;
+      if (tile >= n_tiles) break;
+      const uint32_t u = it / C::LG;
+      const float2 *tp = psi + tc_base<K>(tile * kTileGroups, t);
+      const bool full = (tile + 1) * kTileGroups <= n_groups;
+      float2 v[kLoadItems][4];
 #pragma unroll
-    for (int ks = 0; ks < C::KS; ++ks) {
+      for (int j = 0; j < kLoadItems; ++j) {
+        const int item = lp + C::GS * j, gg = item % kTileGroups, c = item / kTileGroups;
+        const float2 *p = tp + gb[j % NGB];
+        if (full || tile * kTileGroups + gg < n_groups) {
 #pragma unroll
-      for (int nf = 0; nf < C::NF; nf += 2) {
-        const int off = (ks * 16 + lrow) * C::SN + (wn * C::NF + nf) * 8 + lcol;
-        uint32_t bh[4], bl[4];
-        ldsm_x4_trans(bh, &Xhi[off]);
-        ldsm_x4_trans(bl, &Xlo[off]);
-        mma_bf16(acc[nf], al[ks], bh[0], bh[1]);
-        mma_bf16(acc[nf], ah[ks], bl[0], bl[1]);
-        mma_bf16(acc[nf], ah[ks], bh[0], bh[1]);
-        mma_bf16(acc[nf + 1], al[ks], bh[2], bh[3]);
-        mma_bf16(acc[nf + 1], ah[ks], bl[2], bl[3]);
-        mma_bf16(acc[nf + 1], ah[ks], bh[2], bh[3]);
+          for (int q = 0; q < 4; ++q) v[j][q] = p[moff[4 * c + q]];
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) v[j][q] = make_float2(0.f, 0.f);
+        }
+      }
+      if (!mbar_wait_warp(empty_bar(lg), (u & 1) ^ 1, abort_flag, kErrLoaderWait)) break;
+#pragma unroll
+      for (int j = 0; j < kLoadItems; ++j) {
+        const int item = lp + C::GS * j, gg = item % kTileGroups, c = item / kTileGroups;
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const __nv_bfloat162 hv = __floats2bfloat162_rn(v[j][q].x, v[j][q].y);
+          const uint32_t hb = bf162_bits(hv);
+          const __nv_bfloat162 lv = __floats2bfloat162_rn(v[j][q].x - __uint_as_float(hb << 16),
+                                                          v[j][q].y - __uint_as_float(hb & 0xFFFF0000u));
+          h[q] = hb;
+          l[q] = bf162_bits(lv);
+        }
+        const uint32_t off = (uint32_t)(c / 8) * C::ATOM_X + (uint32_t)gg * 128 +
+                             ((uint32_t)((c % 8) ^ (gg & 7)) << 4);
+        *reinterpret_cast<uint4 *>(xh + off) = make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4 *>(xl + off) = make_uint4(l[0], l[1], l[2], l[3]);
+      }
+      fence_async_smem();
+      mbar_arrive(full_bar(lg));
+    }
+  } else {
+    // ---- epilogue: TMEM -> registers -> HBM -----------------------------------
+    const int gg = warp * 32 + lane;
+    const uint64_t gb = tc_base<K>((uint64_t)gg, t);
+    uint32_t it = 0;
+    for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++it) {
+      const uint32_t b = it & 1, v = it >> 1;
+      if (!mbar_wait_warp(accfull_bar(b), v & 1, abort_flag, kErrEpilogueWait)) break;
+      tc_fence_after();
+      const bool live = tile * kTileGroups + gg < n_groups;
+      float2 *p = psi + tc_base<K>(tile * kTileGroups, t) + gb;
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + b * C::R;
+#pragma unroll
+      for (int cc = 0; cc < C::R / 32; ++cc) {
+        float r[32];
+        tc_ld32(taddr + cc * 32, r);
+        if (cc == C::R / 32 - 1) {
+          tc_fence_before();
+          mbar_arrive(accempty_bar(b));
+        }
+        if (live) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) p[moff[cc * 16 + j]] = make_float2(r[2 * j], r[2 * j + 1]);
+        }
       }
     }
-    __syncthreads();  // X is free: the result tile is staged in its place
-    // m-tile mt holds Re (rows 0-7) and Im (rows 8-15) of members 8mt..8mt+7
-#pragma unroll
-    for (int nf = 0; nf < C::NF; ++nf) {
-      const int r0 = mt * 16 + (lane >> 2), c0 = (wn * C::NF + nf) * 8 + 2 * (lane & 3);
-      *reinterpret_cast<float2 *>(&Ys[r0 * C::SG + c0]) = make_float2(acc[nf][0], acc[nf][1]);
-      *reinterpret_cast<float2 *>(&Ys[(r0 + 8) * C::SG + c0]) = make_float2(acc[nf][2], acc[nf][3]);
-    }
-    __syncthreads();
-    const uint64_t g0 = tile * kTcG;
-#pragma unroll
-    for (int j = 0; j < C::PER; ++j) {
-      const int i = threadIdx.x + j * kTcThreads;
-      const int gg = i % kTcG, a = i / kTcG;
-      const int row = (a >> 3) * 16 + (a & 7);
-      const uint64_t g = g0 + gg;
-      if (g < n_groups)
-        psi[tc_base<K>(g, t) + tc_off<K>(a, t)] =
-            make_float2(Ys[row * C::SG + gg], Ys[(row + 8) * C::SG + gg]);
-    }
-    __syncthreads();
   }
-  cp_async_wait<0>();
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kMmaWarp) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
+                 "r"(C::TCOLS)
+                 : "memory");
+  }
 }
 
 uint16_t bf16_bits_rn(float f) {
@@ -226,23 +409,21 @@ float bf16_value(uint16_t b) {
   return f;
 }
 
-template <int K>
-bool launch_tc_k(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::string &err) {
-  using C = TcCfg<K>;
+template <int K, typename Off>
+bool launch_um_k(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::string &err) {
+  using C = UmCfg<K>;
   static std::once_flag once;
   static cudaError_t attr_rc = cudaSuccess;
   static int blocks_per_sm = 1;
   std::call_once(once, [] {
-    attr_rc = cudaFuncSetAttribute(k_gate_tc<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    attr_rc = cudaFuncSetAttribute(k_gate_umma<K, Off>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)C::SMEM);
-    if (attr_rc == cudaSuccess)
-      attr_rc = cudaFuncSetAttribute(k_gate_tc<K>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                     cudaSharedmemCarveoutMaxShared);
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_gate_tc<K>, kTcThreads, C::SMEM) ==
+    if (attr_rc == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_gate_umma<K, Off>, kUmThreads, C::SMEM) ==
             cudaSuccess &&
         b > 0)
-      blocks_per_sm = b;
+      blocks_per_sm = std::min(b, (int)(512 / C::TCOLS));
   });
   if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(tensor gate kernel)", err)) return false;
   TcTargets t;
@@ -252,83 +433,75 @@ bool launch_tc_k(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::s
     t.stride[b] = 1ull << q;
   }
   const uint64_t n_groups = 1ull << (n - K);
-  const uint64_t n_tiles = (n_groups + kTcG - 1) / kTcG;
-  const unsigned grid =
-      (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(n_tiles, (uint64_t)blocks_per_sm * sm_count()));
-  k_gate_tc<K><<<grid, kTcThreads, C::SMEM, s>>>(static_cast<float2 *>(sv), n_groups, t,
-                                                  static_cast<const uint32_t *>(g.d_tc));
+  const uint64_t n_tiles = (n_groups + kTileGroups - 1) / kTileGroups;
+  const unsigned grid = (unsigned)std::max<uint64_t>(
+      1, std::min<uint64_t>(n_tiles, (uint64_t)blocks_per_sm * sm_count()));
+  k_gate_umma<K, Off><<<grid, kUmThreads, C::SMEM, s>>>(static_cast<float2 *>(sv), n_groups, t,
+                                                    static_cast<const uint4 *>(g.d_tc));
   return cuda_ok(cudaGetLastError(), "tensor gate kernel launch", err);
 }
 
 }  // namespace
 
 bool tensor_path_supported(const GateData &g) {
-  return g.precision == 0 && g.k >= 4 && g.k <= 6;
+  return g.precision == 0 && g.k >= 5 && g.k <= 6;
 }
 
-// Packs [[A, -B], [B, A]] (rows permuted as below) into mma.sync m16n8k16 A
-// fragments (row-major 16x16 per fragment; a0..a3 = rows gid / gid+8, columns
-// 2t..2t+1 / 2t+8..2t+9), hi fragments first, then lo, and uploads them.
+// Packs Mr (R x R, Mr[2r+c'][2m+c] as in the header) as the MMA's K-major
+// operand with the 128-byte swizzle: element (row, col) at byte
+// (col / 64) * R * 128 + row * 128 + (((col % 64) / 8 ^ row % 8) * 16) + (col % 8) * 2;
+// hi block first, then lo.
 bool prepare_tensor_gate(GateData &g, std::string &err) {
   if (!tensor_path_supported(g)) {
-    err = "the tensor-core path takes complex64 gates with 4..6 qubits";
+    err = "the tensor-core path takes complex64 gates with 5 or 6 qubits";
     return false;
   }
-  const int D = 1 << g.k, R = 2 * D, MT = R / 16, KS = R / 16;
-  // Rows are ordered per m16 tile: tile mt = Re rows of members 8mt..8mt+7, then
-  // their Im rows; columns are [Re x ; Im x].
-  std::vector<double> Mr((size_t)R * R);
-  for (int mt = 0; mt < MT; ++mt)
-    for (int j = 0; j < 16; ++j) {
-      const int r = mt * 8 + (j & 7);  // member
-      const bool im = j >= 8;
-      double *row = &Mr[(size_t)(mt * 16 + j) * R];
-      for (int c = 0; c < D; ++c) {
-        const double a = g.m64[2 * (r * D + c)], b = g.m64[2 * (r * D + c) + 1];
-        row[c] = im ? b : a;       // x_re coefficient
-        row[D + c] = im ? a : -b;  // x_im coefficient
-      }
+  const int D = 1 << g.k, R = 2 * D;
+  const size_t per = (size_t)R * R;
+  std::vector<uint16_t> packed(2 * per);
+  for (int row = 0; row < R; ++row)
+    for (int col = 0; col < R; ++col) {
+      const int r = row >> 1, m = col >> 1;
+      const double a = g.m64[2 * ((size_t)r * D + m)], b = g.m64[2 * ((size_t)r * D + m) + 1];
+      const bool out_im = row & 1, in_im = col & 1;
+      const double v = out_im ? (in_im ? a : b) : (in_im ? -b : a);
+      const uint16_t hi = bf16_bits_rn((float)v);
+      const uint16_t lo = bf16_bits_rn((float)(v - (double)bf16_value(hi)));
+      const size_t byte = (size_t)(col / 64) * R * 128 + (size_t)row * 128 +
+                          ((size_t)(((col % 64) / 8) ^ (row % 8)) << 4) + (col % 8) * 2;
+      packed[byte / 2] = hi;
+      packed[per + byte / 2] = lo;
     }
-  std::vector<uint16_t> hi((size_t)R * R), lo((size_t)R * R);
-  for (size_t i = 0; i < Mr.size(); ++i) {
-    hi[i] = bf16_bits_rn((float)Mr[i]);
-    lo[i] = bf16_bits_rn((float)(Mr[i] - (double)bf16_value(hi[i])));
-  }
-  const size_t per = (size_t)MT * KS * 128;  // uint32 per operand
-  std::vector<uint32_t> frag(2 * per);
-  auto at = [&](const std::vector<uint16_t> &m, int r, int c) -> uint32_t { return m[(size_t)r * R + c]; };
-  for (int mt = 0; mt < MT; ++mt)
-    for (int ks = 0; ks < KS; ++ks)
-      for (int lane = 0; lane < 32; ++lane) {
-        const int gid = lane >> 2, tq = lane & 3;
-        const int r0 = mt * 16 + gid, c0 = ks * 16 + 2 * tq;
-        for (int which = 0; which < 2; ++which) {
-          const std::vector<uint16_t> &m = which ? lo : hi;
-          uint32_t *dst = frag.data() + which * per + (((size_t)mt * KS + ks) * 32 + lane) * 4;
-          dst[0] = at(m, r0, c0) | (at(m, r0, c0 + 1) << 16);
-          dst[1] = at(m, r0 + 8, c0) | (at(m, r0 + 8, c0 + 1) << 16);
-          dst[2] = at(m, r0, c0 + 8) | (at(m, r0, c0 + 9) << 16);
-          dst[3] = at(m, r0 + 8, c0 + 8) | (at(m, r0 + 8, c0 + 9) << 16);
-        }
-      }
   if (g.d_tc) cudaFree(g.d_tc);
   g.d_tc = nullptr;
-  if (!cuda_ok(cudaMalloc(&g.d_tc, frag.size() * 4), "cudaMalloc (tensor gate fragments)", err))
+  if (!cuda_ok(cudaMalloc(&g.d_tc, packed.size() * 2), "cudaMalloc (tensor gate operand)", err))
     return false;
-  return cuda_ok(cudaMemcpy(g.d_tc, frag.data(), frag.size() * 4, cudaMemcpyHostToDevice),
-                 "cudaMemcpy (tensor gate fragments)", err);
+  return cuda_ok(cudaMemcpy(g.d_tc, packed.data(), packed.size() * 2, cudaMemcpyHostToDevice),
+                 "cudaMemcpy (tensor gate operand)", err);
 }
 
 bool launch_gate_tensor(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::string &err) {
   if (!g.d_tc || !tensor_path_supported(g)) {
-    err = "gate has no tensor-core fragments";
+    err = "gate has no tensor-core operand";
     return false;
   }
+  // member offsets are below 2^n amplitudes: 32-bit while n <= 32
+  const bool narrow = n <= 32;
   switch (g.k) {
-  case 4: return launch_tc_k<4>(g, sv, n, s, err);
-  case 5: return launch_tc_k<5>(g, sv, n, s, err);
-  default: return launch_tc_k<6>(g, sv, n, s, err);
+  case 5: return narrow ? launch_um_k<5, uint32_t>(g, sv, n, s, err) : launch_um_k<5, uint64_t>(g, sv, n, s, err);
+  default: return narrow ? launch_um_k<6, uint32_t>(g, sv, n, s, err) : launch_um_k<6, uint64_t>(g, sv, n, s, err);
   }
 }
 
+// Reads and clears the tensor kernel's error word (a bit per wait that expired).
+bool tensor_error_status(uint32_t *out, std::string &err) {
+  uint32_t zero = 0;
+  if (!cuda_ok(cudaMemcpyFromSymbol(out, g_umma_error, sizeof(uint32_t)),
+               "cudaMemcpyFromSymbol (tensor error word)", err))
+    return false;
+  return cuda_ok(cudaMemcpyToSymbol(g_umma_error, &zero, sizeof(uint32_t)),
+                 "cudaMemcpyToSymbol (tensor error word)", err);
+}
+
 }  // namespace cb2
+

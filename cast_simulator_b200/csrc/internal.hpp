@@ -22,7 +22,7 @@ struct GateData {
   std::vector<double> m64;
   std::vector<float> m32;
   void *d_mat = nullptr;  // device copy in the gate's precision (owned by the holder)
-  void *d_tc = nullptr;   // split-BF16 tensor-core fragments (owned by the holder), if any
+  void *d_tc = nullptr;   // split-BF16 tensor-core gate operand (owned by the holder), if any
 };
 
 // Error helper: fills `err` and returns false on a CUDA failure.
@@ -53,12 +53,14 @@ bool launch_gate(const GateData &g, void *sv, uint32_t n, cudaStream_t stream, s
 // 1/2^k and fills g.m64 / g.m32 (src/cpp/cuda/cuda_gen.cpp:84-103).
 void snap_matrix(GateData &g, const double *interleaved, double ztol, double otol);
 
-// Tensor-core path (gate_tensor.cu): complex64 gates with 4..6 qubits in split
+// Tensor-core path (gate_tensor.cu): complex64 gates with 5 or 6 qubits in split
 // BF16.  prepare_tensor_gate uploads g.d_tc; launch_gate runs the tensor kernel
 // for gates that have it.
 bool tensor_path_supported(const GateData &g);
 bool prepare_tensor_gate(GateData &g, std::string &err);
 bool launch_gate_tensor(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::string &err);
+// Reads and clears the tensor kernel's error word (nonzero: a bounded wait expired).
+bool tensor_error_status(uint32_t *out, std::string &err);
 
 // Device helpers shared between translation units.
 int sm_count();

@@ -66,12 +66,17 @@ void *cast_b200_program_create(uint8_t precision, uint32_t sv_n_qubits, double z
 int cast_b200_program_add_gate(void *program, const cast_complex64_t *matrix,
                                const uint32_t *qubits, uint32_t n_gate_qubits, char *err_buf,
                                size_t err_buf_len);
-/* Opt-in tensor-core path for complex64 programs: gates with 4..6 qubits added
- * afterwards run as split-BF16 tensor-core GEMMs ([[A,-B],[B,A]] applied to
- * 64-group tiles, hi/lo operand split, three products, FP32 accumulation;
- * ~1e-5 relative error per pass).  Must be set before the first gate. */
+/* Opt-in tensor-core path for complex64 programs: gates with 5 or 6 qubits added
+ * afterwards run as split-BF16 tcgen05 GEMMs ([[A,-B],[B,A]] applied to
+ * 128-group tiles, hi/lo operand split, three products, FP32 accumulation in
+ * tensor memory; ~1e-5 relative error per pass).  Must be set before the first
+ * gate. */
 int cast_b200_program_set_split_precision(void *program, int enable, char *err_buf,
                                           size_t err_buf_len);
+/* Reads and clears the tensor-core kernel's error word: 0 when every bounded
+ * wait of every launch since the last call completed, else a bit per wait kind
+ * that expired (the affected tiles were left unwritten).  Synchronous. */
+int cast_b200_tensor_status(uint32_t *out_bits, char *err_buf, size_t err_buf_len);
 uint32_t cast_b200_program_num_gates(const void *program);
 int cast_b200_program_run(void *program, uint64_t sv_dptr, void *stream, int use_graph,
                           char *err_buf, size_t err_buf_len);
