@@ -62,7 +62,7 @@ constexpr uint32_t kErrLoaderWait = 1, kErrMmaFullWait = 2, kErrMmaAccWait = 4,
 
 __device__ uint32_t g_umma_error;
 
-template <int K> struct UmCfg {
+template <int K, bool kStage> struct UmCfg {
   static constexpr int D = 1 << K;
   static constexpr int R = 2 * D;                          // reals per group: MMA N and K extent
   static constexpr int CH = D / 4;                         // 16-byte chunks (4 members) per group
@@ -79,8 +79,12 @@ template <int K> struct UmCfg {
   static constexpr uint32_t NBARS = 2 * S + 5;             // full, empty, accfull x2, accempty x2, drain
   static constexpr uint32_t OFF_BARS = 2 * GBYTES + S * STAGE;
   static constexpr uint32_t OFF_MOFF = OFF_BARS + NBARS * 8;         // member offsets (u64 x D)
-  static constexpr uint32_t OFF_MISC = OFF_MOFF + D * 8;             // tmem slot, abort flag
-  static constexpr uint32_t SMEM = OFF_MISC + 16 + 1024;              // + 1024-byte alignment slack
+  static constexpr uint32_t OFF_GBASE = OFF_MOFF + D * 8;            // group bases (u64 x 128)
+  static constexpr uint32_t OFF_MISC = OFF_GBASE + kTileGroups * 8;   // tmem slot, abort flag
+  static constexpr uint32_t STG_ROW = 144;                            // one group's 128-byte chunk + pad
+  static constexpr uint32_t OFF_STG = (OFF_MISC + 16 + 15) & ~15u;    // epilogue staging, low targets
+  static constexpr uint32_t SMEM =
+      OFF_STG + (kStage ? kEpiWarps * 32 * STG_ROW : 0) + 1024;  // + alignment slack
   // kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both K-major,
   // N = R, M = 128.
   static constexpr uint32_t IDESC =
@@ -90,6 +94,7 @@ template <int K> struct UmCfg {
   static_assert(K >= 5 && R % 64 == 0 && R <= 256, "N, and K blocks of one 128-byte swizzle atom");
   static_assert(TCOLS >= 32 && (TCOLS & (TCOLS - 1)) == 0 && TCOLS <= 512, "TMEM columns");
   static_assert(SMEM <= 227 * 1024, "shared memory");
+  static_assert(OFF_STG % 16 == 0 && STG_ROW % 16 == 0 && OFF_GBASE % 8 == 0, "alignment");
 };
 
 struct TcTargets {
@@ -212,11 +217,17 @@ __device__ __forceinline__ uint32_t bf162_bits(__nv_bfloat162 v) {
 
 // Off: type of the member offsets (uint32_t while every amplitude index fits,
 // which makes each load/store address one wide multiply-add).
-template <int K, typename Off>
+// kStage: qubit 0 is a target (members 2i, 2i+1 adjacent), so the epilogue
+// stages each group's 128-byte chunk through shared memory and writes member
+// pairs; the staging area exists only in this instance, since shared memory is
+// carved from the same array as the L1 that holds the loads in flight.
+// quad (runtime): qubits 0 and 1 are both targets, a chunk's 4 members are 32
+// contiguous bytes and the loaders read them as two 16-byte vectors.
+template <int K, typename Off, bool kStage>
 __global__ void __launch_bounds__(kUmThreads, 1)
     k_gate_umma(float2 *__restrict__ psi, uint64_t n_groups, TcTargets t,
-                const uint4 *__restrict__ gate) {
-  using C = UmCfg<K>;
+                const uint4 *__restrict__ gate, int quad) {
+  using C = UmCfg<K, kStage>;
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char *sm = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~static_cast<uintptr_t>(1023));
@@ -229,6 +240,7 @@ __global__ void __launch_bounds__(kUmThreads, 1)
   auto accempty_bar = [&](int b) { return s_bar + 8u * (2 * C::S + 2 + b); };
   const uint32_t drain_bar = s_bar + 8u * (2 * C::S + 4);
   Off *moff = reinterpret_cast<Off *>(sm + C::OFF_MOFF);
+  uint64_t *gbase = reinterpret_cast<uint64_t *>(sm + C::OFF_GBASE);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sm + C::OFF_MISC);
   volatile uint32_t *abort_flag = tmem_slot + 1;
 
@@ -240,6 +252,7 @@ __global__ void __launch_bounds__(kUmThreads, 1)
     uint4 *dst = reinterpret_cast<uint4 *>(sm);
     for (uint32_t i = threadIdx.x; i < 2 * C::GBYTES / 16; i += kUmThreads) dst[i] = gate[i];
     for (int m = threadIdx.x; m < C::D; m += kUmThreads) moff[m] = (Off)tc_off<K>(m, t);
+    for (int g = threadIdx.x; g < kTileGroups; g += kUmThreads) gbase[g] = tc_base<K>((uint64_t)g, t);
   }
   if (threadIdx.x == 0) {
     for (int s = 0; s < C::S; ++s) {
@@ -329,8 +342,17 @@ __global__ void __launch_bounds__(kUmThreads, 1)
         const int item = lp + C::GS * j, gg = item % kTileGroups, c = item / kTileGroups;
         const float2 *p = tp + gb[j % NGB];
         if (full || tile * kTileGroups + gg < n_groups) {
+          if (kStage && quad) {
+            const float4 a = *reinterpret_cast<const float4 *>(p + moff[4 * c]);
+            const float4 b = *reinterpret_cast<const float4 *>(p + moff[4 * c] + 2);
+            v[j][0] = make_float2(a.x, a.y);
+            v[j][1] = make_float2(a.z, a.w);
+            v[j][2] = make_float2(b.x, b.y);
+            v[j][3] = make_float2(b.z, b.w);
+          } else {
 #pragma unroll
-          for (int q = 0; q < 4; ++q) v[j][q] = p[moff[4 * c + q]];
+            for (int q = 0; q < 4; ++q) v[j][q] = p[moff[4 * c + q]];
+          }
         } else {
 #pragma unroll
           for (int q = 0; q < 4; ++q) v[j][q] = make_float2(0.f, 0.f);
@@ -362,13 +384,15 @@ __global__ void __launch_bounds__(kUmThreads, 1)
     // ---- epilogue: TMEM -> registers -> HBM -----------------------------------
     const int gg = warp * 32 + lane;
     const uint64_t gb = tc_base<K>((uint64_t)gg, t);
+    unsigned char *stg = sm + C::OFF_STG + warp * 32 * C::STG_ROW;
     uint32_t it = 0;
     for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++it) {
       const uint32_t b = it & 1, v = it >> 1;
       if (!mbar_wait_warp(accfull_bar(b), v & 1, abort_flag, kErrEpilogueWait)) break;
       tc_fence_after();
       const bool live = tile * kTileGroups + gg < n_groups;
-      float2 *p = psi + tc_base<K>(tile * kTileGroups, t) + gb;
+      float2 *const tb = psi + tc_base<K>(tile * kTileGroups, t);
+      float2 *p = tb + gb;
       const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + b * C::R;
 #pragma unroll
       for (int cc = 0; cc < C::R / 32; ++cc) {
@@ -378,9 +402,29 @@ __global__ void __launch_bounds__(kUmThreads, 1)
           tc_fence_before();
           mbar_arrive(accempty_bar(b));
         }
-        if (live) {
+        if constexpr (!kStage) {
+          if (live) {
 #pragma unroll
-          for (int j = 0; j < 16; ++j) p[moff[cc * 16 + j]] = make_float2(r[2 * j], r[2 * j + 1]);
+            for (int j = 0; j < 16; ++j) p[moff[cc * 16 + j]] = make_float2(r[2 * j], r[2 * j + 1]);
+          }
+        } else {
+          // a group's 16 members of this chunk go to its staging row; then the
+          // warp writes member pairs (16 bytes), 4 groups x 8 pairs per instruction
+          unsigned char *row = stg + lane * C::STG_ROW;
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            *reinterpret_cast<float4 *>(row + 16 * j) =
+                make_float4(r[4 * j], r[4 * j + 1], r[4 * j + 2], r[4 * j + 3]);
+          __syncwarp();
+          const int pj = lane & 7;
+#pragma unroll
+          for (int rd = 0; rd < 8; ++rd) {
+            const int gi = rd * 4 + (lane >> 3), g2 = warp * 32 + gi;
+            const float4 val = *reinterpret_cast<const float4 *>(stg + gi * C::STG_ROW + 16 * pj);
+            if (tile * kTileGroups + g2 < n_groups)
+              *reinterpret_cast<float4 *>(tb + gbase[g2] + moff[cc * 16 + 2 * pj]) = val;
+          }
+          __syncwarp();
         }
       }
     }
@@ -409,18 +453,18 @@ float bf16_value(uint16_t b) {
   return f;
 }
 
-template <int K, typename Off>
+template <int K, typename Off, bool kStage>
 bool launch_um_k(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::string &err) {
-  using C = UmCfg<K>;
+  using C = UmCfg<K, kStage>;
   static std::once_flag once;
   static cudaError_t attr_rc = cudaSuccess;
   static int blocks_per_sm = 1;
   std::call_once(once, [] {
-    attr_rc = cudaFuncSetAttribute(k_gate_umma<K, Off>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    attr_rc = cudaFuncSetAttribute(k_gate_umma<K, Off, kStage>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)C::SMEM);
     int b = 0;
     if (attr_rc == cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_gate_umma<K, Off>, kUmThreads, C::SMEM) ==
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_gate_umma<K, Off, kStage>, kUmThreads, C::SMEM) ==
             cudaSuccess &&
         b > 0)
       blocks_per_sm = std::min(b, (int)(512 / C::TCOLS));
@@ -436,8 +480,9 @@ bool launch_um_k(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::s
   const uint64_t n_tiles = (n_groups + kTileGroups - 1) / kTileGroups;
   const unsigned grid = (unsigned)std::max<uint64_t>(
       1, std::min<uint64_t>(n_tiles, (uint64_t)blocks_per_sm * sm_count()));
-  k_gate_umma<K, Off><<<grid, kUmThreads, C::SMEM, s>>>(static_cast<float2 *>(sv), n_groups, t,
-                                                    static_cast<const uint4 *>(g.d_tc));
+  const int quad = kStage && g.qubits[1] == 1;
+  k_gate_umma<K, Off, kStage><<<grid, kUmThreads, C::SMEM, s>>>(
+      static_cast<float2 *>(sv), n_groups, t, static_cast<const uint4 *>(g.d_tc), quad);
   return cuda_ok(cudaGetLastError(), "tensor gate kernel launch", err);
 }
 
@@ -486,11 +531,17 @@ bool launch_gate_tensor(const GateData &g, void *sv, uint32_t n, cudaStream_t s,
     return false;
   }
   // member offsets are below 2^n amplitudes: 32-bit while n <= 32
-  const bool narrow = n <= 32;
-  switch (g.k) {
-  case 5: return narrow ? launch_um_k<5, uint32_t>(g, sv, n, s, err) : launch_um_k<5, uint64_t>(g, sv, n, s, err);
-  default: return narrow ? launch_um_k<6, uint32_t>(g, sv, n, s, err) : launch_um_k<6, uint64_t>(g, sv, n, s, err);
+  const bool narrow = n <= 32, stage = g.qubits[0] == 0;
+  if (g.k == 5) {
+    if (narrow) return stage ? launch_um_k<5, uint32_t, true>(g, sv, n, s, err)
+                             : launch_um_k<5, uint32_t, false>(g, sv, n, s, err);
+    return stage ? launch_um_k<5, uint64_t, true>(g, sv, n, s, err)
+                 : launch_um_k<5, uint64_t, false>(g, sv, n, s, err);
   }
+  if (narrow) return stage ? launch_um_k<6, uint32_t, true>(g, sv, n, s, err)
+                           : launch_um_k<6, uint32_t, false>(g, sv, n, s, err);
+  return stage ? launch_um_k<6, uint64_t, true>(g, sv, n, s, err)
+               : launch_um_k<6, uint64_t, false>(g, sv, n, s, err);
 }
 
 // Reads and clears the tensor kernel's error word (a bit per wait that expired).
