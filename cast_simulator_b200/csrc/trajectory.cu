@@ -5,7 +5,7 @@
 // p_i and launches one kernel per gate per member, syncing with the host at
 // every noisy gate) with quantum-jump trajectories sampled on the device:
 //
-//  * one CTA (512 threads) owns one trajectory at a time; its 2^n complex64
+//  * one CTA (1024 threads) owns one trajectory at a time; its 2^n complex64
 //    statevector lives in a per-CTA slice of a workspace in global memory
 //    (148 CTAs x 512 KiB = 74 MiB at 16 qubits, resident in the 126 MB L2);
 //    the CTA loops over trajectories blockIdx.x, blockIdx.x + gridDim.x, ...
