@@ -186,6 +186,106 @@ def run_reference(args):
     return 0
 
 
+def _random_state(n: int, seed: int) -> np.ndarray:
+    """Seeded i.i.d. Gaussian real/imaginary parts, normalised (complex128)."""
+    rng = np.random.default_rng(seed)
+    v = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    return v / np.linalg.norm(v)
+
+
+def _run_fused(n: int, gates, precision, split: bool = False, initial=None, reps: int = 3):
+    """Device time (median of reps, CUDA events) of a fused gate list as one
+    gate program, and the final statevector object."""
+    from cast_simulator_b200 import cuda as cu
+    from cast_simulator_b200.simulator import Event, GateProgram, Stream
+
+    prog = GateProgram(precision, n, 1e-12 if precision == cu.CudaPrecision.F64 else 1e-6,
+                       1e-12 if precision == cu.CudaPrecision.F64 else 1e-6, split)
+    for g in gates:
+        prog.add(g.matrix(), g.qubits())
+    sv = cu.CudaStatevector(n, precision)
+    st = Stream()
+    e0, e1 = Event(), Event()
+    ts = []
+    for _ in range(reps):
+        if initial is None:
+            sv.zero(st)
+        else:
+            sv.upload(initial)
+        e0.record(st)
+        prog.run(sv, st, use_graph=True)
+        e1.record(st)
+        e1.sync()
+        ts.append(e1.elapsed_s(e0))
+    return float(np.median(ts)), sv
+
+
+def qft_leg(n: int = 22, seed: int = 7):
+    """Plain method, small configuration: QFT-CX on a seeded random complex128
+    state with the default fusion (size-only, k <= 6), against the same circuit
+    unfused (fusion invariance; the oracle comparison is tests/test_gpu_configs.py)."""
+    from cast_simulator_b200 import cuda as cu
+    from cast_simulator_b200.fusion import FusionConfig, optimize_native
+    from cast_simulator_b200.types import QuantumCircuit
+
+    circ = QuantumCircuit.qft_cx(n)
+    init = _random_state(n, seed)
+    fused = optimize_native(n, circ.gates(), FusionConfig.default()).gates()
+    t, sv = _run_fused(n, fused, cu.CudaPrecision.F64, initial=init)
+    got = sv.download()
+    _, sv_u = _run_fused(n, circ.gates(), cu.CudaPrecision.F64, initial=init, reps=1)
+    ref = sv_u.download()
+    passes = len(fused)
+    return {"workload": f"qft-cx-{n}q-c128-default-fusion", "unfused_gates": len(circ),
+            "fused_gates": passes, "ms": t * 1e3,
+            "hbm_gbs": passes * 2 * (1 << n) * 16 / t / 1e9,
+            "gates_amps_per_s": len(circ) * (1 << n) / t,
+            "max_abs_diff_vs_unfused": float(np.max(np.abs(got - ref)))}
+
+
+def largest_leg(depth: int = 10, n64: int = 34, n128: int = 33, n_prefix: int = 28):
+    """Largest single-GPU fit: 34-qubit complex64 and 33-qubit complex128 (128 GiB
+    each), brickwork (depth 10) and QFT-CX; plain CUDA-core path at k = 4 vs the
+    split-BF16 tensor path at k = 5, 6 for complex64.  Fidelity on a 28-qubit
+    prefix of the same constructions against the complex128 plain path."""
+    from cast_simulator_b200 import cuda as cu
+    from cast_simulator_b200.fusion import FusionConfig, optimize_native
+    from cast_simulator_b200.types import QuantumCircuit
+
+    out = {"runs": []}
+    for n, prec, label in ((n64, cu.CudaPrecision.F32, "c64"), (n128, cu.CudaPrecision.F64, "c128")):
+        amp = 8 if label == "c64" else 16
+        for name, circ in (("brickwork", QuantumCircuit.brickwork(n, depth, 2024)),
+                           ("qft-cx", QuantumCircuit.qft_cx(n))):
+            variants = [(4, False)] + ([(5, True), (6, True)] if label == "c64" else [])
+            for k, split in variants:
+                fused = optimize_native(n, circ.gates(), FusionConfig.size_only(k)).gates()
+                t, sv = _run_fused(n, fused, prec, split, reps=2)
+                del sv
+                out["runs"].append({"workload": f"{name}-{n}q-{label}", "fusion_k": k,
+                                    "tensor_cores": split, "fused_gates": len(fused),
+                                    "ms": t * 1e3,
+                                    "hbm_gbs": len(fused) * 2 * (1 << n) * amp / t / 1e9})
+    fid = {}
+    for name, circ in (("brickwork", QuantumCircuit.brickwork(n_prefix, depth, 2024)),
+                       ("qft-cx", QuantumCircuit.qft_cx(n_prefix))):
+        g4 = optimize_native(n_prefix, circ.gates(), FusionConfig.size_only(4)).gates()
+        _, ref_sv = _run_fused(n_prefix, g4, cu.CudaPrecision.F64, reps=1)
+        ref = ref_sv.download()
+        del ref_sv
+        for k, split in ((4, False), (6, True)):
+            gk = optimize_native(n_prefix, circ.gates(), FusionConfig.size_only(k)).gates()
+            _, sv = _run_fused(n_prefix, gk, cu.CudaPrecision.F32, split, reps=1)
+            psi = sv.download()
+            del sv
+            nrm = float(np.linalg.norm(psi))
+            fid[f"{name}-k{k}{'-tensor' if split else ''}"] = {
+                "one_minus_abs_overlap_renormalised": float(1 - abs(np.vdot(ref, psi / nrm))),
+                "max_abs_err": float(np.max(np.abs(ref - psi)))}
+    out["fidelity_28q_prefix_vs_c128"] = fid
+    return out
+
+
 def trajectory_leg(n: int = 16, depth: int = 30, n_traj: int = 4096, k: int = 3):
     """Noisy-trajectory configuration: brickwork depth 30 with depolarizing 1e-3
     after every gate and amplitude damping 5e-4 per qubit per layer; 4096
@@ -341,6 +441,8 @@ def main(argv=None):
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip trajectory and serving legs")
     ap.add_argument("--serve-requests", type=int, default=60)
+    ap.add_argument("--largest", action="store_true",
+                    help="add the 34q complex64 / 33q complex128 largest-fit leg (minutes)")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
@@ -478,9 +580,12 @@ def main(argv=None):
             "value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
             "sample": f"{passes} fused-gate passes of the {n_cpu}-qubit brickwork (k={args.k}) in {el:.1f} s"}
     if rank == 0 and not args.no_extras:
+        line["qft"] = qft_leg()
         line["tensor_path"] = tensor_leg(n, args.depth)
         line["trajectories"] = trajectory_leg()
         line["serving"] = serving_leg(args.serve_requests)
+    if rank == 0 and args.largest:
+        line["largest_fit"] = largest_leg()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg:

@@ -1,0 +1,253 @@
+"""Autotuner: device timings of fused-gate passes, the roofline fit of the
+reference's hardware profiler refitted to include the tensor pipe, and the
+choice of fusion width (and tensor-core use) for a circuit.
+
+The reference's profiler (src/profile.rs:229-352, fit at :137-183 and
+:361-410) sweeps gates across arithmetic intensities, fits a two-segment
+roofline GFLOP/s = min(bw_slope * AI, peak) and hands the crossover
+AI = peak / bw_slope to the hardware-adaptive cost model
+(src/cost_model.rs:120-275).  Here:
+
+  * ``measure_profile`` sweeps dense k-qubit gates (AI = 2^(k+1) scalars per
+    amplitude, the same AI definition, gate.rs:261-272) on the CUDA-core path
+    and fits the roofline the same way (slope = median of GFLOP/s / AI over the
+    lower half of the sweep, peak = the largest GFLOP/s);
+  * for complex64 it also times the split-BF16 tensor-core path on k = 5, 6 and
+    records its effective ceiling as ``tensor_gflops_s`` with
+    ``tensor_min_k = 5``, so ``HardwareProfile.crossover_for(k)`` gives the
+    tensor-pipe crossover for wide gates;
+  * ``choose_fusion`` fuses the circuit at every width k with the native
+    planner and predicts its time from the measured per-pass times (scaled by
+    2^(n - n_profile), the passes being memory-bound), then returns the width
+    and engine with the least predicted time.
+
+Command line:
+
+    python -m cast_simulator_b200.autotune gate --k 6 --n 26 --mode tc [--low]
+    python -m cast_simulator_b200.autotune profile --n 26 --precision f32 [--out prof.json]
+    python -m cast_simulator_b200.autotune choose --n 30 --depth 20 --precision f32
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .fusion import FusionConfig, HardwareProfile, optimize_native
+
+MODES = ("f64", "f32", "tc")  # CUDA-core FP64 / FP32, split-BF16 tensor cores (complex64)
+TENSOR_KS = (5, 6)
+
+
+def haar(k: int, rng: np.random.Generator) -> np.ndarray:
+    d = 1 << k
+    z = rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))
+    q, r = np.linalg.qr(z)
+    return q * (np.diag(r) / np.abs(np.diag(r)))
+
+
+def dense_ai(k: int) -> float:
+    """Arithmetic intensity of a dense k-qubit gate: scalar nonzeros / 2^k."""
+    return 2.0 * (1 << k)
+
+
+def time_gate(n: int, k: int, mode: str, low: bool = False, reps: int = 5, seed: int = 1) -> float:
+    """Seconds for one in-place application of a Haar-random k-qubit gate to a
+    2^n statevector (best of ``reps`` after one warm-up), timed with CUDA events
+    on the launching stream.  Targets are the top k qubits, or the bottom k when
+    ``low``."""
+    from .cuda import CudaPrecision, CudaStatevector
+    from .simulator import Event, GateProgram, Stream
+
+    if mode not in MODES:
+        raise ValueError(f"mode must be one of {MODES}")
+    prec = CudaPrecision.F64 if mode == "f64" else CudaPrecision.F32
+    q = tuple(range(k)) if low else tuple(range(n - k, n))
+    prog = GateProgram(prec, n, 1e-12, 1e-12, split_precision=(mode == "tc"))
+    prog.add(haar(k, np.random.default_rng(seed)), q)
+    sv = CudaStatevector(n, prec)
+    sv.zero()
+    st = Stream()
+    e0, e1 = Event(), Event()
+    best = math.inf
+    for i in range(reps + 1):
+        e0.record(st)
+        prog.run(sv, st, use_graph=False)
+        e1.record(st)
+        e1.sync()
+        if i:
+            best = min(best, e1.elapsed_s(e0))
+    return best
+
+
+@dataclass
+class Probe:
+    k: int
+    mode: str
+    ai: float
+    seconds: float
+    gflops_s: float
+    gib_s: float
+
+
+def probe(n: int, k: int, mode: str, reps: int = 3) -> Probe:
+    t = time_gate(n, k, mode, reps=reps)
+    scalar = 8 if mode == "f64" else 4
+    sv_bytes = (1 << n) * 2 * scalar
+    ai = dense_ai(k)
+    return Probe(k, mode, ai, t, ai * (1 << n) * 2.0 / t / 1e9, 2.0 * sv_bytes / t / (1 << 30))
+
+
+def fit_roofline(probes: list[Probe]) -> tuple[float, float, float]:
+    """(bw_slope, peak_gflops, crossover_ai) as profile.rs:137-162: the slope
+    is the median GFLOP/s / AI over the lower half of the sweep (sorted by AI),
+    the peak the largest observed GFLOP/s."""
+    if not probes:
+        raise ValueError("fit_roofline needs at least one probe")
+    sweep = sorted(probes, key=lambda p: p.ai)
+    lower = sweep[: (len(sweep) + 1) // 2]
+    ratios = sorted(p.gflops_s / p.ai for p in lower)
+    slope = ratios[len(ratios) // 2]
+    peak = max(p.gflops_s for p in sweep)
+    return slope, peak, (peak / slope if slope > 0 else math.inf)
+
+
+def roofline_r2(probes: list[Probe], slope: float, peak: float) -> float:
+    """Coefficient of determination of min(slope * AI, peak) (profile.rs:164-183)."""
+    g = np.array([p.gflops_s for p in probes])
+    pred = np.array([min(slope * p.ai, peak) for p in probes])
+    ss_tot = float(((g - g.mean()) ** 2).sum())
+    return 1.0 if ss_tot < 1e-30 else 1.0 - float(((g - pred) ** 2).sum()) / ss_tot
+
+
+def profile_from_probes(probes: list[Probe], precision: str, n: int,
+                        tensor: list[Probe] | None = None) -> HardwareProfile:
+    """HardwareProfile from a CUDA-core sweep (and, for complex64, the tensor
+    probes): peak bandwidth and GFLOP/s are the largest observed, the slope and
+    crossover come from ``fit_roofline``; the tensor ceiling is the largest
+    effective GFLOP/s of the tensor probes."""
+    slope, peak, xo = fit_roofline(probes)
+    prof = HardwareProfile(
+        peak_bw_gib_s=max(p.gib_s for p in probes), peak_gflops_s=peak, bw_slope=slope,
+        crossover_ai=xo,
+        config={"device": "cuda", "precision": precision, "n_qubits": n,
+                "r2": roofline_r2(probes, slope, peak)},
+        raw=[p.__dict__ for p in probes + (tensor or [])])
+    if tensor:
+        prof.tensor_gflops_s = max(p.gflops_s for p in tensor)
+        prof.tensor_min_k = min(p.k for p in tensor)
+    return prof
+
+
+def measure_profile(n: int = 26, precision: str = "f32", ks=range(1, 8), reps: int = 3) -> HardwareProfile:
+    """Sweep dense gates k = 1..7 on the CUDA-core path (and k = 5, 6 on the
+    tensor cores for complex64) and fit the profile."""
+    probes = [probe(n, k, precision, reps) for k in ks]
+    tensor = [probe(n, k, "tc", reps) for k in TENSOR_KS] if precision == "f32" else None
+    return profile_from_probes(probes, precision, n, tensor)
+
+
+@dataclass
+class PassTable:
+    """Measured seconds per pass, keyed by (k, mode), at ``n_qubits``."""
+
+    n_qubits: int
+    seconds: dict = field(default_factory=dict)
+
+    def predict(self, k: int, mode: str, n: int) -> float:
+        key = (k, mode)
+        if key not in self.seconds:
+            raise KeyError(f"no measured pass time for k={k} mode={mode}")
+        return self.seconds[key] * 2.0 ** (n - self.n_qubits)
+
+
+def measure_pass_table(n: int, precision: str, ks=range(1, 8), tensor: bool = True,
+                       reps: int = 3) -> PassTable:
+    tab = PassTable(n)
+    for k in ks:
+        tab.seconds[(k, precision)] = time_gate(n, k, precision, reps=reps)
+    if tensor and precision == "f32":
+        for k in TENSOR_KS:
+            tab.seconds[(k, "tc")] = time_gate(n, k, "tc", reps=reps)
+    return tab
+
+
+def engine_for(k: int, precision: str, split: bool) -> str:
+    """The kernel family a fused k-qubit gate runs on in a program."""
+    return "tc" if split and precision == "f32" and k in TENSOR_KS else precision
+
+
+@dataclass
+class Choice:
+    fusion_k: int
+    split_precision: bool
+    predicted_s: float
+    candidates: list
+
+
+def choose_fusion(n: int, gates, precision: str, table: PassTable, ks=range(2, 7),
+                  allow_tensor: bool = True) -> Choice:
+    """Fuse ``gates`` at each width in ``ks`` (size-only cost, the reference's
+    default) and predict the circuit time from ``table``; returns the width and
+    engine (CUDA cores, or tensor cores for 5- and 6-qubit gates) with the least
+    predicted time."""
+    cands = []
+    splits = (False, True) if (allow_tensor and precision == "f32") else (False,)
+    for k in ks:
+        fused = optimize_native(n, gates, FusionConfig.size_only(k)).gates()
+        for split in splits:
+            t = sum(table.predict(g.n_qubits(), engine_for(g.n_qubits(), precision, split), n)
+                    for g in fused)
+            cands.append({"fusion_k": k, "split_precision": split, "fused_gates": len(fused),
+                          "predicted_s": t})
+    best = min(cands, key=lambda c: c["predicted_s"])
+    return Choice(best["fusion_k"], best["split_precision"], best["predicted_s"], cands)
+
+
+def _main(argv=None) -> None:
+    ap = argparse.ArgumentParser(prog="python -m cast_simulator_b200.autotune")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    g = sub.add_parser("gate", help="time one Haar-random gate application")
+    g.add_argument("--k", type=int, required=True)
+    g.add_argument("--n", type=int, default=26)
+    g.add_argument("--mode", choices=MODES, default="f32")
+    g.add_argument("--low", action="store_true", help="targets are qubits 0..k-1")
+    g.add_argument("--reps", type=int, default=5)
+    p = sub.add_parser("profile", help="roofline profile with the tensor-pipe crossover")
+    p.add_argument("--n", type=int, default=26)
+    p.add_argument("--precision", choices=("f64", "f32"), default="f32")
+    p.add_argument("--out")
+    c = sub.add_parser("choose", help="fusion width / engine for a brickwork circuit")
+    c.add_argument("--n", type=int, default=30)
+    c.add_argument("--depth", type=int, default=20)
+    c.add_argument("--precision", choices=("f64", "f32"), default="f32")
+    c.add_argument("--profile-n", type=int, default=26)
+    a = ap.parse_args(argv)
+    if a.cmd == "gate":
+        t = time_gate(a.n, a.k, a.mode, a.low, a.reps)
+        b = 2 * (1 << a.n) * (16 if a.mode == "f64" else 8)
+        print(json.dumps({"k": a.k, "n": a.n, "mode": a.mode, "low_targets": a.low,
+                          "ms": t * 1e3, "gb_s": b / t / 1e9}))
+    elif a.cmd == "profile":
+        prof = measure_profile(a.n, a.precision)
+        if a.out:
+            prof.save(a.out)
+        d = dict(prof.__dict__)
+        d.pop("raw")
+        d["crossover_tensor_ai"] = prof.crossover_for(prof.tensor_min_k) if prof.tensor_min_k else None
+        print(json.dumps(d))
+    else:
+        from .types import QuantumCircuit
+
+        circ = QuantumCircuit.brickwork(a.n, a.depth, 2024)
+        tab = measure_pass_table(a.profile_n, a.precision)
+        ch = choose_fusion(a.n, circ.gates(), a.precision, tab)
+        print(json.dumps({"fusion_k": ch.fusion_k, "split_precision": ch.split_precision,
+                          "predicted_ms": ch.predicted_s * 1e3, "candidates": ch.candidates}))
+
+
+if __name__ == "__main__":
+    _main()

@@ -186,7 +186,7 @@ class NoiseModel:
 
 
 class QuantumGate:
-    __slots__ = ("_m", "_q", "_noise", "_name", "_prov")
+    __slots__ = ("_m", "_q", "_noise", "_name", "_prov", "_op")
 
     def __init__(self, matrix, qubits, noise: NoiseModel | None = None, name: str = ""):
         m = np.ascontiguousarray(np.asarray(matrix, dtype=np.complex128))
@@ -195,12 +195,14 @@ class QuantumGate:
         self._noise = noise
         self._name = name
         self._prov = None
+        self._op = None
 
     def with_provenance(self, index: int) -> "QuantumGate":
         """Copy tagged with a source index; matmul concatenates the tags in
         application order, so a fused gate knows which gates it contains."""
         g = QuantumGate.__new__(QuantumGate)
         g._m, g._q, g._noise, g._name, g._prov = self._m, self._q, self._noise, self._name, [index]
+        g._op = self._op
         return g
 
     def provenance(self):
@@ -213,35 +215,47 @@ class QuantumGate:
         return cls(np.asarray(data, dtype=np.float64).reshape(d, d).astype(np.complex128), qubits)
 
     @classmethod
-    def x(cls, q): return cls(mat_x(), [q], name="x")
+    def _named(cls, mat, qubits, name, params=()):
+        """A named standard gate that remembers its OpenQASM form (name, angles,
+        operands in the order given), so a circuit of them can be written back."""
+        g = cls(mat, qubits, name=name)
+        g._op = (name, tuple(float(p) for p in params), tuple(int(q) for q in qubits))
+        return g
+
     @classmethod
-    def y(cls, q): return cls(mat_y(), [q], name="y")
+    def x(cls, q): return cls._named(mat_x(), [q], "x")
     @classmethod
-    def z(cls, q): return cls(mat_z(), [q], name="z")
+    def y(cls, q): return cls._named(mat_y(), [q], "y")
     @classmethod
-    def h(cls, q): return cls(mat_h(), [q], name="h")
+    def z(cls, q): return cls._named(mat_z(), [q], "z")
     @classmethod
-    def s(cls, q): return cls(mat_s(), [q], name="s")
+    def h(cls, q): return cls._named(mat_h(), [q], "h")
     @classmethod
-    def t(cls, q): return cls(mat_t(), [q], name="t")
+    def s(cls, q): return cls._named(mat_s(), [q], "s")
     @classmethod
-    def rx(cls, th, q): return cls(mat_rx(th), [q], name="rx")
+    def t(cls, q): return cls._named(mat_t(), [q], "t")
     @classmethod
-    def ry(cls, th, q): return cls(mat_ry(th), [q], name="ry")
+    def rx(cls, th, q): return cls._named(mat_rx(th), [q], "rx", (th,))
     @classmethod
-    def rz(cls, th, q): return cls(mat_rz(th), [q], name="rz")
+    def ry(cls, th, q): return cls._named(mat_ry(th), [q], "ry", (th,))
     @classmethod
-    def u3(cls, th, ph, la, q): return cls(mat_u3(th, ph, la), [q], name="u3")
+    def rz(cls, th, q): return cls._named(mat_rz(th), [q], "rz", (th,))
     @classmethod
-    def cx(cls, c, t): return cls(mat_cx(), [c, t], name="cx")
+    def u3(cls, th, ph, la, q): return cls._named(mat_u3(th, ph, la), [q], "u3", (th, ph, la))
     @classmethod
-    def cz(cls, c, t): return cls(mat_cz(), [c, t], name="cz")
+    def cx(cls, c, t): return cls._named(mat_cx(), [c, t], "cx")
     @classmethod
-    def cp(cls, th, c, t): return cls(mat_cp(th), [c, t], name="cp")
+    def cz(cls, c, t): return cls._named(mat_cz(), [c, t], "cz")
     @classmethod
-    def swap(cls, a, b): return cls(mat_swap(), [a, b], name="swap")
+    def cp(cls, th, c, t): return cls._named(mat_cp(th), [c, t], "cp", (th,))
     @classmethod
-    def ccx(cls, a, b, t): return cls(mat_ccx(), [a, b, t], name="ccx")
+    def swap(cls, a, b): return cls._named(mat_swap(), [a, b], "swap")
+    @classmethod
+    def ccx(cls, a, b, t): return cls._named(mat_ccx(), [a, b, t], "ccx")
+
+    def op(self):
+        """(name, angles, operands) of a named standard gate, else None."""
+        return self._op
 
     @classmethod
     def random_unitary(cls, qubits, rng: np.random.Generator):
@@ -271,6 +285,7 @@ class QuantumGate:
             br.append((float(p), v @ self._m))
         g = QuantumGate.__new__(QuantumGate)
         g._m, g._q, g._noise, g._name, g._prov = self._m, self._q, NoiseModel(br), self._name, None
+        g._op = None
         return g
 
     def with_kraus(self, kraus_ops) -> "QuantumGate":
@@ -282,6 +297,7 @@ class QuantumGate:
         br = [(1.0 / m, math.sqrt(m) * np.asarray(k, dtype=np.complex128)) for k in kraus_ops]
         g = QuantumGate.__new__(QuantumGate)
         g._m, g._q, g._noise, g._name, g._prov = self._m, self._q, NoiseModel(br), self._name, None
+        g._op = None
         return g
 
     def with_depolarizing(self, p: float) -> "QuantumGate":
@@ -366,6 +382,7 @@ class QuantumGate:
         g = QuantumGate.__new__(QuantumGate)
         g._m, g._q, g._noise, g._name = np.ascontiguousarray(fused), uq, noise, "fused"
         g._prov = (other._prov + self._prov) if (self._prov is not None and other._prov is not None) else None
+        g._op = None
         return g
 
     def to_density_matrix_gate(self, n_total: int) -> "QuantumGate":
