@@ -21,18 +21,19 @@
 //   warps 0-3   epilogue: tensor memory -> registers (tcgen05.ld 32x32b, lane =
 //               group) -> coalesced 8-byte stores, 32 consecutive groups of one
 //               member per warp instruction;
-//   warps 4-19  loaders: 8-byte global loads of 4 members per (group, chunk),
+//   warps 4-15  loaders: 8-byte global loads of 4 members per (group, chunk),
 //               split into BF16 hi/lo in registers, 16-byte shared stores in the
 //               UMMA K-major layout with the 128-byte swizzle (8 rows x 128 B
 //               atoms, the 16-byte chunk index XORed with the row: conflict-free
 //               for these stores and for the tensor core's operand reads);
-//   warp 20     allocates tensor memory and issues the MMAs (one thread).
-// The loader warps form 2^(7-k) groups; group j fills operand stage j with every
-// (2^(7-k))-th tile, so 128 KB of loads per SM are in flight for every k (one
-// tile's worth per group; a single group would leave the loads latency-bound).
-// Shared memory holds the gate (hi and lo) for the whole launch plus the stages;
-// tensor memory holds two accumulators so the epilogue of one tile overlaps the
-// MMAs of the next.  Every wait on an mbarrier is bounded:
+//   warp 16     allocates tensor memory and issues the MMAs (one thread).
+// An operand stage holds one 64-real K atom (32 members) of a tile's 128 groups,
+// hi and lo (32 KB); a tile takes 2^k / 32 consecutive stages.  The loader warps
+// form 3 groups of 128 threads, group j owning stage j, so three stages of loads
+// (96 KB) are in flight per SM.  Shared memory is kept small on purpose: it is
+// carved from the same array as the L1 that holds those loads in flight (k = 6:
+// 64 KB gate + 96 KB stages).  Tensor memory holds two accumulators so the
+// epilogue of one tile overlaps the MMAs of the next.  Every wait on an mbarrier is bounded:
 // on expiry the CTA records an error code (read back by tensor_error_status),
 // drains its outstanding MMAs, frees its tensor memory and exits.
 #include "internal.hpp"
@@ -48,11 +49,13 @@ namespace {
 
 constexpr int kTileGroups = 128;                   // MMA M: one TMEM lane per group
 constexpr int kEpiWarps = 4;                       // warps 0-3 (TMEM sub-partitions 0-3)
-constexpr int kLoadWarps = 16;                     // warps 4-19
-constexpr int kMmaWarp = kEpiWarps + kLoadWarps;   // warp 20
-constexpr int kUmThreads = (kMmaWarp + 1) * 32;    // 672
+constexpr int kLoadWarps = 12;                     // warps 4-15
+constexpr int kMmaWarp = kEpiWarps + kLoadWarps;   // warp 16
+constexpr int kUmThreads = (kMmaWarp + 1) * 32;    // 544
 constexpr int kLoadThreads = kLoadWarps * 32;
-constexpr int kLoadItems = 8;                      // 16-byte chunks per loader thread per tile
+constexpr int kStages = 3;                          // operand stages = loader groups
+constexpr int kStageMembers = 32;                   // members per stage: one 64-real K atom
+constexpr int kLoadItems = kStageMembers / 4;       // 4-member chunks per loader thread per stage
 constexpr uint32_t kSuspendNs = 20000;             // hardware suspend hint per try_wait poll
 constexpr uint32_t kSpinLimit = 1u << 16;          // polls before a wait gives up (<= ~1.3 s)
 
@@ -66,15 +69,14 @@ template <int K, bool kStage> struct UmCfg {
   static constexpr int D = 1 << K;
   static constexpr int R = 2 * D;                          // reals per group: MMA N and K extent
   static constexpr int CH = D / 4;                         // 16-byte chunks (4 members) per group
-  static constexpr int LG = kLoadThreads * kLoadItems / (kTileGroups * CH);  // loader groups
-  static constexpr int GS = kLoadThreads / LG;             // threads per loader group
-  static constexpr uint32_t ATOM_X = kTileGroups * 128;    // one 64-wide K block of X (all rows)
+  static constexpr int KH = D / kStageMembers;             // stages (K atoms) per tile
+  static constexpr int LG = kStages;                       // loader groups: one per stage
+  static constexpr int GS = kLoadThreads / LG;             // threads per loader group: one per group row
   static constexpr uint32_t ATOM_G = R * 128;              // one 64-wide K block of Mr
-  static constexpr uint32_t XBYTES = kTileGroups * R * 2;  // one BF16 operand tile (hi or lo)
+  static constexpr uint32_t XBYTES = kTileGroups * 128;    // one K atom of X for the tile (hi or lo)
   static constexpr uint32_t GBYTES = R * R * 2;            // one BF16 gate (hi or lo)
   static constexpr uint32_t STAGE = 2 * XBYTES;
-  static constexpr int S = LG;                             // operand stages: one per loader group
-  static constexpr int KS = R / 16;                        // k16 steps
+  static constexpr int S = kStages;
   static constexpr uint32_t TCOLS = 2 * R;                 // two FP32 accumulators of N = R columns
   static constexpr uint32_t NBARS = 2 * S + 5;             // full, empty, accfull x2, accempty x2, drain
   static constexpr uint32_t OFF_BARS = 2 * GBYTES + S * STAGE;
@@ -89,8 +91,8 @@ template <int K, bool kStage> struct UmCfg {
   // N = R, M = 128.
   static constexpr uint32_t IDESC =
       (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(R >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-  static_assert(LG * GS == kLoadThreads && GS * kLoadItems == kTileGroups * CH, "loader mapping");
-  static_assert(GS % 32 == 0 && (GS % kTileGroups == 0 || kTileGroups % GS == 0), "loader groups");
+  static_assert(LG * GS == kLoadThreads && GS == kTileGroups && KH * kStageMembers == D,
+                "one loader thread per group row, whole K atoms per stage");
   static_assert(K >= 5 && R % 64 == 0 && R <= 256, "N, and K blocks of one 128-byte swizzle atom");
   static_assert(TCOLS >= 32 && (TCOLS & (TCOLS - 1)) == 0 && TCOLS <= 512, "TMEM columns");
   static_assert(SMEM <= 227 * 1024, "shared memory");
@@ -282,32 +284,37 @@ __global__ void __launch_bounds__(kUmThreads, 1)
 
   if (warp == kMmaWarp) {
     // ---- MMA issuer ----------------------------------------------------------
+    // tile `it` consumes stages h = it * KH .. it * KH + KH - 1 (one K atom each)
     uint32_t it = 0;
-    bool issued = false;
-    for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++it) {
-      const uint32_t s = it % C::S, u = it / C::S, b = it & 1, v = it >> 1;
-      if (!mbar_wait_warp(full_bar(s), u & 1, abort_flag, kErrMmaFullWait)) break;
-      if (!mbar_wait_warp(accempty_bar(b), (v & 1) ^ 1, abort_flag, kErrMmaAccWait)) break;
-      tc_fence_after();
-      if (lane == 0) {
-        const uint32_t xh = s_stage + s * C::STAGE, xl = xh + C::XBYTES;
-        const uint32_t gh = s_gate, gl = s_gate + C::GBYTES;
-        const uint32_t d = tmem + b * C::R;
-#pragma unroll
-        for (int ks = 0; ks < C::KS; ++ks) {
-          const uint32_t ox = (ks / 4) * C::ATOM_X + (ks % 4) * 32;
-          const uint32_t og = (ks / 4) * C::ATOM_G + (ks % 4) * 32;
-          const uint64_t a_hi = umma_desc_sw128(xh + ox), a_lo = umma_desc_sw128(xl + ox);
-          const uint64_t b_hi = umma_desc_sw128(gh + og), b_lo = umma_desc_sw128(gl + og);
-          tc_mma(d, a_lo, b_hi, C::IDESC, ks > 0 ? 1u : 0u);
-          tc_mma(d, a_hi, b_lo, C::IDESC, 1u);
-          tc_mma(d, a_hi, b_hi, C::IDESC, 1u);
+    bool issued = false, ok = true;
+    for (uint64_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x, ++it) {
+      const uint32_t b = it & 1, v = it >> 1;
+      for (int kp = 0; kp < C::KH; ++kp) {
+        const uint32_t h = it * C::KH + kp, s = h % C::S, u = h / C::S;
+        if (!mbar_wait_warp(full_bar(s), u & 1, abort_flag, kErrMmaFullWait)) { ok = false; break; }
+        if (kp == 0 && !mbar_wait_warp(accempty_bar(b), (v & 1) ^ 1, abort_flag, kErrMmaAccWait)) {
+          ok = false;
+          break;
         }
-        tc_commit(empty_bar(s));
-        tc_commit(accfull_bar(b));
+        tc_fence_after();
+        if (lane == 0) {
+          const uint32_t xh = s_stage + s * C::STAGE, xl = xh + C::XBYTES;
+          const uint32_t gh = s_gate + kp * C::ATOM_G, gl = gh + C::GBYTES;
+          const uint32_t d = tmem + b * C::R;
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks) {
+            const uint64_t a_hi = umma_desc_sw128(xh + ks * 32), a_lo = umma_desc_sw128(xl + ks * 32);
+            const uint64_t b_hi = umma_desc_sw128(gh + ks * 32), b_lo = umma_desc_sw128(gl + ks * 32);
+            tc_mma(d, a_lo, b_hi, C::IDESC, (kp > 0 || ks > 0) ? 1u : 0u);
+            tc_mma(d, a_hi, b_lo, C::IDESC, 1u);
+            tc_mma(d, a_hi, b_hi, C::IDESC, 1u);
+          }
+          tc_commit(empty_bar(s));
+          if (kp == C::KH - 1) tc_commit(accfull_bar(b));
+        }
+        __syncwarp();
+        issued = true;
       }
-      __syncwarp();
-      issued = true;
     }
     // every MMA of this CTA has completed before tensor memory is released
     if (issued) {
@@ -318,30 +325,25 @@ __global__ void __launch_bounds__(kUmThreads, 1)
     }
   } else if (warp >= kEpiWarps) {
     // ---- loaders: HBM -> split BF16 -> operand stage --------------------------
-    // group lg owns stage lg and the CTA's tiles it = lg, lg + LG, ...; item i of
-    // a tile (i = lt' + GS * j) is chunk i / 128 of group i % 128, so a warp
-    // covers 32 consecutive groups of one chunk.
+    // thread (lg, gg) loads group row gg of the stages group lg owns: 32 members
+    // (8 chunks of 4) per stage, so a warp instruction covers 32 consecutive
+    // groups of one member.
     const int lt = threadIdx.x - kEpiWarps * 32;
-    const int lg = lt / C::GS, lp = lt % C::GS;
-    // group bases split as pdep(tile * 128) | pdep(gg): the second part is fixed
-    // for the launch (one value, or two when a loader group is 64 threads wide)
-    constexpr int NGB = C::GS >= kTileGroups ? 1 : kTileGroups / C::GS;
-    uint64_t gb[NGB];
-#pragma unroll
-    for (int i = 0; i < NGB; ++i) gb[i] = tc_base<K>((uint64_t)((lp + C::GS * i) % kTileGroups), t);
+    const int lg = lt / C::GS, gg = lt % C::GS;  // group row gg of every tile
+    const uint64_t gb = tc_base<K>((uint64_t)gg, t);
     unsigned char *xh = sm + 2 * C::GBYTES + lg * C::STAGE, *xl = xh + C::XBYTES;
-    for (uint32_t it = lg;; it += C::LG) {
-      const uint64_t tile = blockIdx.x + (uint64_t)it * gridDim.x;
+    // stage h holds K atom h % KH of tile h / KH; group lg fills stages h = lg, lg + S, ...
+    for (uint32_t h = lg;; h += C::S) {
+      const uint32_t ti = h / C::KH, kp = h % C::KH, u = h / C::S;
+      const uint64_t tile = blockIdx.x + (uint64_t)ti * gridDim.x;
       if (tile >= n_tiles) break;
-      const uint32_t u = it / C::LG;
-      const float2 *tp = psi + tc_base<K>(tile * kTileGroups, t);
-      const bool full = (tile + 1) * kTileGroups <= n_groups;
+      const bool live = tile * kTileGroups + gg < n_groups;
+      const float2 *p = psi + tc_base<K>(tile * kTileGroups, t) + gb;
       float2 v[kLoadItems][4];
 #pragma unroll
       for (int j = 0; j < kLoadItems; ++j) {
-        const int item = lp + C::GS * j, gg = item % kTileGroups, c = item / kTileGroups;
-        const float2 *p = tp + gb[j % NGB];
-        if (full || tile * kTileGroups + gg < n_groups) {
+        const int c = kp * kLoadItems + j;
+        if (live) {
           if (kStage && quad) {
             const float4 a = *reinterpret_cast<const float4 *>(p + moff[4 * c]);
             const float4 b = *reinterpret_cast<const float4 *>(p + moff[4 * c] + 2);
@@ -361,21 +363,19 @@ __global__ void __launch_bounds__(kUmThreads, 1)
       if (!mbar_wait_warp(empty_bar(lg), (u & 1) ^ 1, abort_flag, kErrLoaderWait)) break;
 #pragma unroll
       for (int j = 0; j < kLoadItems; ++j) {
-        const int item = lp + C::GS * j, gg = item % kTileGroups, c = item / kTileGroups;
-        uint32_t h[4], l[4];
+        uint32_t hb4[4], lb4[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const __nv_bfloat162 hv = __floats2bfloat162_rn(v[j][q].x, v[j][q].y);
           const uint32_t hb = bf162_bits(hv);
           const __nv_bfloat162 lv = __floats2bfloat162_rn(v[j][q].x - __uint_as_float(hb << 16),
                                                           v[j][q].y - __uint_as_float(hb & 0xFFFF0000u));
-          h[q] = hb;
-          l[q] = bf162_bits(lv);
+          hb4[q] = hb;
+          lb4[q] = bf162_bits(lv);
         }
-        const uint32_t off = (uint32_t)(c / 8) * C::ATOM_X + (uint32_t)gg * 128 +
-                             ((uint32_t)((c % 8) ^ (gg & 7)) << 4);
-        *reinterpret_cast<uint4 *>(xh + off) = make_uint4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<uint4 *>(xl + off) = make_uint4(l[0], l[1], l[2], l[3]);
+        const uint32_t off = (uint32_t)gg * 128 + ((uint32_t)(j ^ (gg & 7)) << 4);
+        *reinterpret_cast<uint4 *>(xh + off) = make_uint4(hb4[0], hb4[1], hb4[2], hb4[3]);
+        *reinterpret_cast<uint4 *>(xl + off) = make_uint4(lb4[0], lb4[1], lb4[2], lb4[3]);
       }
       fence_async_smem();
       mbar_arrive(full_bar(lg));
