@@ -117,6 +117,7 @@ CAST_B200 = [
     ("cast_b200_program_set_split_precision", C.c_int,
      [C.c_void_p, C.c_int, C.c_char_p, C.c_size_t]),
     ("cast_b200_tensor_status", C.c_int, [C.POINTER(C.c_uint32), C.c_char_p, C.c_size_t]),
+    ("cast_b200_set_tensor_loader", C.c_int, [C.c_int]),
     ("cast_b200_program_num_gates", C.c_uint32, [C.c_void_p]),
     ("cast_b200_program_run", C.c_int,
      [C.c_void_p, C.c_uint64, C.c_void_p, C.c_int, C.c_char_p, C.c_size_t]),

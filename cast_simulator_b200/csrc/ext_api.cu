@@ -235,6 +235,8 @@ int cast_b200_program_set_split_precision(void *program, int enable, char *err_b
   return 0;
 }
 
+int cast_b200_set_tensor_loader(int mode) { return cb2::set_tensor_loader(mode); }
+
 int cast_b200_tensor_status(uint32_t *out_bits, char *err_buf, size_t err_buf_len) {
   if (!out_bits) {
     write_err(err_buf, err_buf_len, "out_bits is null");

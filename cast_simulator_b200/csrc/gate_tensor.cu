@@ -41,6 +41,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 namespace cb2 {
@@ -61,9 +62,13 @@ constexpr uint32_t kSpinLimit = 1u << 16;          // polls before a wait gives 
 
 // error bits recorded in g_umma_error
 constexpr uint32_t kErrLoaderWait = 1, kErrMmaFullWait = 2, kErrMmaAccWait = 4,
-                   kErrEpilogueWait = 8, kErrDrainWait = 16;
+                   kErrEpilogueWait = 8, kErrDrainWait = 16, kErrProducerWait = 32,
+                   kErrConvertWait = 64;
 
 __device__ uint32_t g_umma_error;
+
+std::atomic<int> g_tensor_loader{0};  // 0 auto, 1 register loaders, 2 TMA where eligible
+bool tma_enabled() { return g_tensor_loader.load() != 1; }
 
 template <int K, bool kStage> struct UmCfg {
   static constexpr int D = 1 << K;
@@ -439,6 +444,270 @@ __global__ void __launch_bounds__(kUmThreads, 1)
   }
 }
 
+// ---- TMA-fed variant ----------------------------------------------------------
+// For gates whose lowest target qubit is >= 7 (launched for those only; the kernel
+// itself handles runs of 2^min(q0, 7) amplitudes), the 128 groups of a tile are
+// one contiguous 1 KB run for every member, so the raw
+// FP32 tile is fetched with TMA bulk copies (cp.async.bulk, completion counted
+// on an mbarrier) into a ring of raw slots, one 32-member K atom per slot.  The
+// copies occupy neither L1 nor registers, so the loads in flight are bounded
+// only by the ring (96 KB for k = 6, 128 KB for k = 5).  Warps:
+//   0-7   epilogue: warp w reads TMEM sub-partition w % 4 (32 groups) and half
+//         w / 4 of the accumulator columns, so twice as many warps keep stores in
+//         flight as in k_gate_umma;
+//   8-15  converters: thread (gg, half) splits group row gg, members
+//         16 half .. 16 half + 15 of a raw slot into the swizzled operand stage;
+//   16    producer: lane 0 arms the slot's mbarrier with the slot's bytes, the 32
+//         lanes issue its bulk copies; before exiting it waits (bounded) for the
+//         copies of the last slots it armed;
+//   17    TMEM allocation and MMA issue, as in k_gate_umma.
+constexpr int kTEpiWarps = 8;                         // two per TMEM sub-partition
+constexpr int kTConvWarps = 8;
+constexpr int kTProdWarp = kTEpiWarps + kTConvWarps;  // 16
+constexpr int kTMmaWarp = kTProdWarp + 1;             // 17
+constexpr int kTThreads = (kTMmaWarp + 1) * 32;       // 576
+constexpr int kTConvThreads = kTConvWarps * 32;
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t a, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(a), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t smem_dst, const void *gmem_src, uint32_t bytes,
+                                         uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_dst),
+      "l"(gmem_src), "r"(bytes), "r"(mbar)
+      : "memory");
+}
+
+template <int K> struct UtCfg {
+  static constexpr int D = 1 << K;
+  static constexpr int R = 2 * D;
+  static constexpr int KH = D / kStageMembers;             // K atoms (slots, stages) per tile
+  static constexpr int S = 2;                              // operand stages
+  static constexpr int RS = K == 6 ? 3 : 4;                // raw slots
+  static constexpr uint32_t ATOM_G = R * 128;
+  static constexpr uint32_t XBYTES = kTileGroups * 128;    // one K atom of X (hi or lo)
+  static constexpr uint32_t STAGE = 2 * XBYTES;
+  static constexpr uint32_t RAW = kStageMembers * kTileGroups * 8;  // FP32 amplitudes of one slot
+  static constexpr uint32_t GBYTES = R * R * 2;
+  static constexpr uint32_t TCOLS = 2 * R;
+  static constexpr uint32_t NBARS = 2 * RS + 2 * S + 5;
+  static constexpr uint32_t OFF_OP = 2 * GBYTES;
+  static constexpr uint32_t OFF_RAW = OFF_OP + S * STAGE;
+  static constexpr uint32_t OFF_BARS = OFF_RAW + RS * RAW;
+  static constexpr uint32_t OFF_MOFF = OFF_BARS + NBARS * 8;
+  static constexpr uint32_t OFF_GBASE = OFF_MOFF + D * 8;
+  static constexpr uint32_t OFF_MISC = OFF_GBASE + kTileGroups * 8;
+  static constexpr uint32_t SMEM = OFF_MISC + 16 + 1024;
+  static constexpr uint32_t IDESC =
+      (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(R >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  static_assert(K >= 5 && KH * kStageMembers == D, "whole K atoms");
+  static_assert(SMEM <= 227 * 1024, "shared memory");
+  static_assert(OFF_RAW % 1024 == 0 && OFF_OP % 1024 == 0 && OFF_GBASE % 8 == 0, "alignment");
+};
+
+template <int K, typename Off>
+__global__ void __launch_bounds__(kTThreads, 1)
+    k_gate_umma_tma(float2 *__restrict__ psi, uint64_t n_groups, TcTargets t,
+                    const uint4 *__restrict__ gate, int run_log2) {
+  using C = UtCfg<K>;
+  extern __shared__ __align__(1024) unsigned char smem_dyn[];
+  unsigned char *sm = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~static_cast<uintptr_t>(1023));
+  const uint32_t s_gate = smem_u32(sm);
+  const uint32_t s_bar = s_gate + C::OFF_BARS;
+  auto raw_full = [&](int r) { return s_bar + 8u * r; };
+  auto raw_empty = [&](int r) { return s_bar + 8u * (C::RS + r); };
+  auto op_full = [&](int q) { return s_bar + 8u * (2 * C::RS + q); };
+  auto op_empty = [&](int q) { return s_bar + 8u * (2 * C::RS + C::S + q); };
+  auto accfull_bar = [&](int b) { return s_bar + 8u * (2 * C::RS + 2 * C::S + b); };
+  auto accempty_bar = [&](int b) { return s_bar + 8u * (2 * C::RS + 2 * C::S + 2 + b); };
+  const uint32_t drain_bar = s_bar + 8u * (2 * C::RS + 2 * C::S + 4);
+  Off *moff = reinterpret_cast<Off *>(sm + C::OFF_MOFF);
+  uint64_t *gbase = reinterpret_cast<uint64_t *>(sm + C::OFF_GBASE);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sm + C::OFF_MISC);
+  volatile uint32_t *abort_flag = tmem_slot + 1;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint64_t n_tiles = n_groups / kTileGroups;  // whole tiles only (checked on the host)
+
+  {
+    uint4 *dst = reinterpret_cast<uint4 *>(sm);
+    for (uint32_t i = threadIdx.x; i < 2 * C::GBYTES / 16; i += kTThreads) dst[i] = gate[i];
+    for (int m = threadIdx.x; m < C::D; m += kTThreads) moff[m] = (Off)tc_off<K>(m, t);
+    for (int g = threadIdx.x; g < kTileGroups; g += kTThreads) gbase[g] = tc_base<K>((uint64_t)g, t);
+  }
+  if (threadIdx.x == 0) {
+    for (int r = 0; r < C::RS; ++r) {
+      mbar_init(raw_full(r), 1);
+      mbar_init(raw_empty(r), kTConvThreads);
+    }
+    for (int q = 0; q < C::S; ++q) {
+      mbar_init(op_full(q), kTConvThreads);
+      mbar_init(op_empty(q), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accfull_bar(b), 1);
+      mbar_init(accempty_bar(b), kTEpiWarps * 32);
+    }
+    mbar_init(drain_bar, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  fence_async_smem();
+  if (warp == kTMmaWarp) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(C::TCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == kTMmaWarp) {
+    // ---- MMA issuer: tile `it` consumes operand stages h = it * KH + kp --------
+    uint32_t it = 0;
+    bool issued = false, ok = true;
+    for (uint64_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x, ++it) {
+      const uint32_t b = it & 1, v = it >> 1;
+      for (int kp = 0; kp < C::KH; ++kp) {
+        const uint32_t h = it * C::KH + kp, q = h % C::S, u = h / C::S;
+        if (!mbar_wait_warp(op_full(q), u & 1, abort_flag, kErrMmaFullWait)) { ok = false; break; }
+        if (kp == 0 && !mbar_wait_warp(accempty_bar(b), (v & 1) ^ 1, abort_flag, kErrMmaAccWait)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        if (lane == 0) {
+          const uint32_t xh = s_gate + C::OFF_OP + q * C::STAGE, xl = xh + C::XBYTES;
+          const uint32_t gh = s_gate + kp * C::ATOM_G, gl = gh + C::GBYTES;
+          const uint32_t d = tmem + b * C::R;
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks) {
+            const uint64_t a_hi = umma_desc_sw128(xh + ks * 32), a_lo = umma_desc_sw128(xl + ks * 32);
+            const uint64_t b_hi = umma_desc_sw128(gh + ks * 32), b_lo = umma_desc_sw128(gl + ks * 32);
+            tc_mma(d, a_lo, b_hi, C::IDESC, (kp > 0 || ks > 0) ? 1u : 0u);
+            tc_mma(d, a_hi, b_lo, C::IDESC, 1u);
+            tc_mma(d, a_hi, b_hi, C::IDESC, 1u);
+          }
+          tc_commit(op_empty(q));
+          if (kp == C::KH - 1) tc_commit(accfull_bar(b));
+        }
+        __syncwarp();
+        issued = true;
+      }
+    }
+    if (issued) {
+      if (lane == 0) tc_commit(drain_bar);
+      __syncwarp();
+      volatile uint32_t never = 0;
+      mbar_wait_warp(drain_bar, 0, &never, kErrDrainWait);
+    }
+  } else if (warp == kTProdWarp) {
+    // ---- producer: bulk copies of raw slot h = it * KH + kp --------------------
+    const int run = 1 << run_log2, runs = kTileGroups >> run_log2;
+    const int copies = kStageMembers * runs;
+    uint32_t h = 0;
+    bool ok = true;
+    for (uint64_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
+      const float2 *tp = psi + tc_base<K>(tile * kTileGroups, t);
+      for (int kp = 0; kp < C::KH; ++kp) {
+        const uint32_t r = h % C::RS, u = h / C::RS;
+        if (!mbar_wait_warp(raw_empty(r), (u & 1) ^ 1, abort_flag, kErrProducerWait)) {
+          ok = false;
+          break;
+        }
+        if (lane == 0) mbar_arrive_expect_tx(raw_full(r), C::RAW);
+        __syncwarp();
+        const uint32_t dst0 = s_gate + C::OFF_RAW + r * C::RAW;
+        for (int c = lane; c < copies; c += 32) {
+          const int ml = c / runs, rr = c % runs;
+          bulk_g2s(dst0 + ml * (kTileGroups * 8) + (rr << run_log2) * 8,
+                   tp + gbase[rr << run_log2] + moff[kp * kStageMembers + ml], run * 8, raw_full(r));
+        }
+        ++h;
+      }
+    }
+    // every copy this CTA issued has landed before its shared memory is released
+    volatile uint32_t never = 0;
+    for (uint32_t j = h > (uint32_t)C::RS ? h - C::RS : 0; j < h; ++j)
+      mbar_wait_warp(raw_full(j % C::RS), (j / C::RS) & 1, &never, kErrDrainWait);
+  } else if (warp >= kTEpiWarps) {
+    // ---- converters: raw slot -> split BF16 -> operand stage -------------------
+    const int ct = threadIdx.x - kTEpiWarps * 32;
+    const int gg = ct % kTileGroups, half = ct / kTileGroups;
+    for (uint32_t h = 0;; ++h) {
+      const uint64_t tile = blockIdx.x + (uint64_t)(h / C::KH) * gridDim.x;
+      if (tile >= n_tiles) break;
+      const uint32_t r = h % C::RS, ur = h / C::RS, q = h % C::S, uq = h / C::S;
+      if (!mbar_wait_warp(raw_full(r), ur & 1, abort_flag, kErrConvertWait)) break;
+      if (!mbar_wait_warp(op_empty(q), (uq & 1) ^ 1, abort_flag, kErrConvertWait)) break;
+      const unsigned char *raw = sm + C::OFF_RAW + r * C::RAW + gg * 8;
+      unsigned char *xh = sm + C::OFF_OP + q * C::STAGE, *xl = xh + C::XBYTES;
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        const int chunk = 4 * half + jj;
+        uint32_t hb4[4], lb4[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const float2 v = *reinterpret_cast<const float2 *>(raw + (4 * chunk + m) * (kTileGroups * 8));
+          const __nv_bfloat162 hv = __floats2bfloat162_rn(v.x, v.y);
+          const uint32_t hb = bf162_bits(hv);
+          const __nv_bfloat162 lv = __floats2bfloat162_rn(v.x - __uint_as_float(hb << 16),
+                                                          v.y - __uint_as_float(hb & 0xFFFF0000u));
+          hb4[m] = hb;
+          lb4[m] = bf162_bits(lv);
+        }
+        const uint32_t off = (uint32_t)gg * 128 + ((uint32_t)(chunk ^ (gg & 7)) << 4);
+        *reinterpret_cast<uint4 *>(xh + off) = make_uint4(hb4[0], hb4[1], hb4[2], hb4[3]);
+        *reinterpret_cast<uint4 *>(xl + off) = make_uint4(lb4[0], lb4[1], lb4[2], lb4[3]);
+      }
+      fence_async_smem();
+      mbar_arrive(op_full(q));
+      mbar_arrive(raw_empty(r));
+    }
+  } else {
+    // ---- epilogue: TMEM -> registers -> HBM (qubit 0 is never a target here) ----
+    const int quarter = warp & 3, half = warp >> 2;
+    const int gg = quarter * 32 + lane;
+    const uint64_t gb = gbase[gg];
+    constexpr int CPW = C::R / 64;  // 32-column chunks per epilogue warp
+    uint32_t it = 0;
+    for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++it) {
+      const uint32_t b = it & 1, v = it >> 1;
+      if (!mbar_wait_warp(accfull_bar(b), v & 1, abort_flag, kErrEpilogueWait)) break;
+      tc_fence_after();
+      float2 *p = psi + tc_base<K>(tile * kTileGroups, t) + gb;
+      const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + b * C::R + half * CPW * 32;
+#pragma unroll
+      for (int ci = 0; ci < CPW; ++ci) {
+        const int cc = half * CPW + ci;
+        float rr[32];
+        tc_ld32(taddr + ci * 32, rr);
+        if (ci == CPW - 1) {
+          tc_fence_before();
+          mbar_arrive(accempty_bar(b));
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) p[moff[cc * 16 + j]] = make_float2(rr[2 * j], rr[2 * j + 1]);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kTMmaWarp) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
+                 "r"(C::TCOLS)
+                 : "memory");
+  }
+}
+
 uint16_t bf16_bits_rn(float f) {
   uint32_t u;
   std::memcpy(&u, &f, 4);
@@ -484,6 +753,30 @@ bool launch_um_k(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::s
   k_gate_umma<K, Off, kStage><<<grid, kUmThreads, C::SMEM, s>>>(
       static_cast<float2 *>(sv), n_groups, t, static_cast<const uint4 *>(g.d_tc), quad);
   return cuda_ok(cudaGetLastError(), "tensor gate kernel launch", err);
+}
+
+template <int K, typename Off>
+bool launch_ut_k(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::string &err) {
+  using C = UtCfg<K>;
+  static std::once_flag once;
+  static cudaError_t attr_rc = cudaSuccess;
+  std::call_once(once, [] {
+    attr_rc = cudaFuncSetAttribute(k_gate_umma_tma<K, Off>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)C::SMEM);
+  });
+  if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(tensor gate kernel, TMA)", err)) return false;
+  TcTargets t;
+  for (uint32_t b = 0; b < kMaxGateQubits; ++b) {
+    const uint32_t q = b < g.k ? g.qubits[b] : 0;
+    t.lo_mask[b] = (1ull << q) - 1;
+    t.stride[b] = 1ull << q;
+  }
+  const uint64_t n_tiles = (1ull << (n - K)) / kTileGroups;
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(n_tiles, (uint64_t)sm_count()));
+  const int run_log2 = (int)std::min<uint32_t>(g.qubits[0], 7);
+  k_gate_umma_tma<K, Off><<<grid, kTThreads, C::SMEM, s>>>(
+      static_cast<float2 *>(sv), 1ull << (n - K), t, static_cast<const uint4 *>(g.d_tc), run_log2);
+  return cuda_ok(cudaGetLastError(), "tensor gate kernel launch (TMA)", err);
 }
 
 }  // namespace
@@ -532,6 +825,13 @@ bool launch_gate_tensor(const GateData &g, void *sv, uint32_t n, cudaStream_t s,
   }
   // member offsets are below 2^n amplitudes: 32-bit while n <= 32
   const bool narrow = n <= 32, stage = g.qubits[0] == 0;
+  // lowest target >= 7 and whole tiles: every member's 128 groups are one 1 KB
+  // run, fetched with one TMA bulk copy (shorter runs measured slower with TMA
+  // than with register loads: 256-byte copies ran at 2.0 TB/s for k = 6)
+  // (k = 6 only: for k = 5 the register loaders measured faster, 4.08 vs 4.40 ms
+  // at 30 qubits)
+  if (g.k == 6 && g.qubits[0] >= 7 && n >= g.k + 7 && tma_enabled())
+    return narrow ? launch_ut_k<6, uint32_t>(g, sv, n, s, err) : launch_ut_k<6, uint64_t>(g, sv, n, s, err);
   if (g.k == 5) {
     if (narrow) return stage ? launch_um_k<5, uint32_t, true>(g, sv, n, s, err)
                              : launch_um_k<5, uint32_t, false>(g, sv, n, s, err);
@@ -543,6 +843,8 @@ bool launch_gate_tensor(const GateData &g, void *sv, uint32_t n, cudaStream_t s,
   return stage ? launch_um_k<6, uint64_t, true>(g, sv, n, s, err)
                : launch_um_k<6, uint64_t, false>(g, sv, n, s, err);
 }
+
+int set_tensor_loader(int mode) { return g_tensor_loader.exchange(mode); }
 
 // Reads and clears the tensor kernel's error word (a bit per wait that expired).
 bool tensor_error_status(uint32_t *out, std::string &err) {

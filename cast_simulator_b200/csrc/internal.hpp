@@ -61,6 +61,9 @@ bool prepare_tensor_gate(GateData &g, std::string &err);
 bool launch_gate_tensor(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::string &err);
 // Reads and clears the tensor kernel's error word (nonzero: a bounded wait expired).
 bool tensor_error_status(uint32_t *out, std::string &err);
+// Tensor-kernel loader: 0 auto (TMA bulk copies where the lowest target is >= 7),
+// 1 register loads always, 2 same as auto; returns the previous mode.
+int set_tensor_loader(int mode);
 
 // Device helpers shared between translation units.
 int sm_count();

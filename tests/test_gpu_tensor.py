@@ -36,15 +36,31 @@ def _cases(rng, k):
            (n, tuple(sorted([0, 3] + list(range(n - k + 2, n))))),
            (n, tuple(sorted(rng.choice(n, size=k, replace=False).tolist())))]
     out += [(k + 3, tuple(range(1, k + 1))), (k, tuple(range(k)))]
+    # lowest target 5, 7 and 9: register loads, then the TMA-fed kernel (1 KB runs)
+    out += [(n, tuple([5] + list(range(n - k + 1, n)))), (n, tuple(range(7, 7 + k))),
+            (n, tuple(range(9, 9 + k)))]
     return out
 
 
+@pytest.mark.parametrize("loader", [0, 1])
 @pytest.mark.parametrize("k", [5, 6])
-def test_single_gate_within_bound(mods, oracle, k):
+def test_single_gate_within_bound(mods, oracle, k, loader):
+    """loader 0: TMA bulk copies where eligible (lowest target >= 7, whole
+    tiles), register loads otherwise; loader 1: register loads everywhere."""
     cu, F, S, T = mods
+    from cast_simulator_b200 import _lib as L
+
     rng = np.random.default_rng(40 + k)
     S.tensor_status()  # clear the error word
-    for n, q in _cases(rng, k):
+    old = L.lib().cast_b200_set_tensor_loader(loader)
+    try:
+        _check_cases(cu, S, oracle, k, _cases(rng, k), rng)
+    finally:
+        L.lib().cast_b200_set_tensor_loader(old)
+
+
+def _check_cases(cu, S, oracle, k, cases, rng):
+    for n, q in cases:
         m = haar(rng, 1 << k)
         init = oracle.random_state(n, k)
         ref = init.copy()
