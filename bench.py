@@ -309,8 +309,12 @@ def trajectory_leg(n: int = 16, depth: int = 30, n_traj: int = 4096, k: int = 3)
     t0 = time.perf_counter()
     run_plain(circ, n_plain, 5)
     tp = (time.perf_counter() - t0) / n_plain
+    # every fused block is one pass over the trajectory's 2^n complex64 amplitudes
+    # (read + write); the passes run out of L2, so this is an equivalent rate
+    equiv = n_traj * prog.stats.n_blocks * 2 * (1 << n) * 8 / t / 1e9
     return {"config": f"brickwork-{n}q-d{depth}, depolarizing 1e-3, damping 5e-4, c64, k={k}",
             "n_traj": n_traj, "seconds": t, "traj_per_s": n_traj / t,
+            "pass_equivalent_gbs": equiv,
             "plain_traj_per_s": 1.0 / tp, "speedup_vs_plain": (n_traj / t) * tp,
             "blocks": prog.stats.n_blocks, "error_sites": prog.stats.n_errors,
             "z_mean_first4": [float(x) for x in z.mean(axis=0)[:4]]}

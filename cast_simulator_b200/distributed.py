@@ -1,0 +1,189 @@
+"""Statevector sharded over G = 2^g ranks (one process per GPU) with qubit-swap
+exchanges.
+
+The reference runs one statevector on one device; this is the multi-GPU form of
+the same gate-application path:
+
+  * **Layout.** There are n logical qubits and L = n - g local physical
+    positions per rank. Rank r holds the 2^L amplitudes whose top g physical
+    qubits equal the bits of r. ``perm[logical] = physical`` records which
+    logical qubit currently sits at which physical position; it starts as the
+    identity.
+  * **Local gates.** A gate whose physical targets are all below L runs on every
+    rank's shard locally, through the device kernel (C ABI) on GPU ranks.
+  * **Global targets.** Before a gate touches a global position P = L + b, that
+    position is swapped with a local position p the gate does not use (the
+    highest such). Rank r and its partner r ^ 2^b exchange the half of their
+    shards whose local bit p differs from their own bit b: a pairwise send/recv
+    of 2^(L-1) amplitudes, with no collective. The two positions then trade
+    logical qubits in ``perm``.
+  * **Reading out.** ``gather`` assembles the logical-order state on rank 0.
+    ``expectation_z`` all-reduces per-position populations (FP64) and maps them
+    back to logical qubits.
+
+Communication is ``torch.distributed``: NCCL on GPUs, gloo on CPU.
+"""
+from __future__ import annotations
+
+import math
+from typing import Callable
+
+import numpy as np
+
+LocalApply = Callable[[object, np.ndarray, tuple], None]
+
+
+def swap_plan(targets_phys: tuple, n_local: int, in_use: set | None = None) -> list[tuple[int, int]]:
+    """(global position, local position) swaps that make every physical target
+    local.
+
+    Each global target is paired with the highest local position that is neither
+    a target of this gate nor already chosen."""
+    in_use = set(in_use or ()) | {q for q in targets_phys if q < n_local}
+    plan = []
+    for q in sorted(q for q in targets_phys if q >= n_local):
+        p = next((c for c in range(n_local - 1, -1, -1) if c not in in_use), None)
+        if p is None:
+            raise ValueError("gate is wider than the local qubits of a shard")
+        in_use.add(p)
+        plan.append((q, p))
+    return plan
+
+
+def permute_bits(index: np.ndarray, perm: list[int]) -> np.ndarray:
+    """Physical index of every logical index: bit perm[i] of the result is bit i
+    of ``index``."""
+    out = np.zeros_like(index)
+    for logical, physical in enumerate(perm):
+        out |= ((index >> logical) & 1) << physical
+    return out
+
+
+class ShardedStatevector:
+    """One rank's shard of a 2^n statevector.
+
+    ``shard`` is a 1-D complex tensor of 2^(n-g) amplitudes (torch; CUDA on GPU
+    ranks, CPU with gloo). ``apply_local(shard, matrix, local_qubits)`` applies
+    a gate to the shard in place. On GPU ranks, ``cuda_apply_local`` runs the
+    device kernels through the C ABI."""
+
+    def __init__(self, n_qubits: int, shard, apply_local: LocalApply, group=None):
+        import torch.distributed as dist
+
+        self.dist = dist
+        self.group = group
+        self.world = dist.get_world_size(group) if dist.is_initialized() else 1
+        self.rank = dist.get_rank(group) if dist.is_initialized() else 0
+        g = int(round(math.log2(self.world)))
+        if 1 << g != self.world:
+            raise ValueError("the number of ranks must be a power of two")
+        self.n, self.g, self.n_local = int(n_qubits), g, int(n_qubits) - g
+        if self.n_local < 1 or shard.numel() != (1 << self.n_local):
+            raise ValueError("shard must hold 2^(n - log2(world)) amplitudes")
+        self.shard = shard
+        self.apply_local = apply_local
+        self.perm = list(range(self.n))  # logical -> physical position
+        self.n_exchanges = 0
+
+    # -- state ------------------------------------------------------------------
+    def set_zero(self) -> None:
+        self.shard.zero_()
+        if self.rank == 0:
+            self.shard[0] = 1.0
+        self.perm = list(range(self.n))
+
+    # -- gates ------------------------------------------------------------------
+    def apply(self, matrix: np.ndarray, qubits) -> None:
+        """Apply a gate given on logical qubits (in the order of the matrix's
+        index bits)."""
+        phys = tuple(self.perm[q] for q in qubits)
+        for gpos, lpos in swap_plan(phys, self.n_local):
+            self._swap(gpos, lpos)
+        phys = tuple(self.perm[q] for q in qubits)
+        self.apply_local(self.shard, np.ascontiguousarray(matrix), phys)
+
+    def _swap(self, gpos: int, lpos: int) -> None:
+        """Exchange global position gpos with local position lpos."""
+        import torch
+
+        b = gpos - self.n_local
+        my_bit = (self.rank >> b) & 1
+        partner = self.rank ^ (1 << b)
+        view = self.shard.view(1 << (self.n_local - lpos - 1), 2, 1 << lpos)
+        send = view[:, 1 - my_bit, :].contiguous()
+        recv = torch.empty_like(send)
+        # real views: not every backend transfers complex tensors
+        ops = [self.dist.P2POp(self.dist.isend, torch.view_as_real(send), partner, self.group),
+               self.dist.P2POp(self.dist.irecv, torch.view_as_real(recv), partner, self.group)]
+        for req in self.dist.batch_isend_irecv(ops):
+            req.wait()
+        view[:, 1 - my_bit, :] = recv
+        la = self.perm.index(gpos)
+        lb = self.perm.index(lpos)
+        self.perm[la], self.perm[lb] = lpos, gpos
+        self.n_exchanges += 1
+
+    # -- read-out -----------------------------------------------------------------
+    def gather(self) -> np.ndarray | None:
+        """The full statevector in logical qubit order on rank 0 (None
+        elsewhere)."""
+        import torch
+
+        parts = [torch.empty_like(self.shard) for _ in range(self.world)] if self.rank == 0 else None
+        if self.world == 1:
+            parts = [self.shard]
+        else:
+            self.dist.gather(torch.view_as_real(self.shard),
+                             [torch.view_as_real(x) for x in parts] if parts else None,
+                             dst=0, group=self.group)
+        if self.rank != 0:
+            return None
+        phys = np.concatenate([p.cpu().numpy() for p in parts])
+        idx = np.arange(1 << self.n, dtype=np.int64)
+        return phys[permute_bits(idx, self.perm)]
+
+    def expectation_z(self) -> np.ndarray:
+        """<Z_q> for every logical qubit, every rank (FP64 all-reduce)."""
+        import torch
+
+        p = (self.shard.abs() ** 2).to(torch.float64)
+        ones = torch.zeros(self.n + 1, dtype=torch.float64, device=p.device)
+        idx = torch.arange(1 << self.n_local, device=p.device)
+        for pos in range(self.n_local):
+            ones[pos] = p[((idx >> pos) & 1) == 1].sum()
+        tot = p.sum()
+        for b in range(self.g):
+            ones[self.n_local + b] = tot if (self.rank >> b) & 1 else 0.0
+        ones[self.n] = tot
+        if self.world > 1:
+            self.dist.all_reduce(ones, group=self.group)
+        ones = ones.cpu().numpy()
+        return np.array([1.0 - 2.0 * ones[self.perm[q]] / ones[self.n] for q in range(self.n)])
+
+
+def cuda_apply_local(precision: int, ztol: float = 1e-12, otol: float = 1e-12) -> LocalApply:
+    """Local applier for GPU ranks: the device gate kernels through
+    ``cast_b200_apply_gate`` on the shard's memory, ordered on torch's current
+    stream."""
+    import ctypes as C
+
+    import torch
+
+    from . import _lib as L
+
+    from .types import _canonicalize
+
+    def apply(shard, matrix, phys_qubits):
+        # the kernels take ascending qubits: permute the matrix's index bits
+        m, srt = _canonicalize(np.asarray(matrix, dtype=np.complex128), list(phys_qubits))
+        qs = np.asarray(srt, dtype=np.uint32)
+        k = len(srt)
+        m = np.ascontiguousarray(m)
+        n_local = int(round(math.log2(shard.numel())))
+        eb = L.errbuf()
+        stream = torch.cuda.current_stream(shard.device).cuda_stream
+        L.check(L.lib().cast_b200_apply_gate(
+            shard.data_ptr(), n_local, precision, m.view(np.float64).ctypes.data_as(C.POINTER(L.Complex64)),
+            qs.ctypes.data_as(L.c_u32p), k, ztol, otol, C.c_void_p(stream), eb, L.ERR_LEN), eb, "apply_gate")
+
+    return apply

@@ -319,3 +319,41 @@ def run_plain(circuit: QuantumCircuit, n_traj: int, seed: int, precision=None) -
         p1, nrm = qubit_populations(sv)
         out[t] = 1.0 - 2.0 * p1 / nrm
     return out
+
+
+def _main(argv=None) -> None:
+    """Time one batch of trajectories of the noisy brickwork construction:
+
+        python -m cast_simulator_b200.trajectory --n 16 --depth 30 --traj 4096
+    """
+    import argparse
+    import json
+    import time
+
+    from .simulator import Stream
+
+    ap = argparse.ArgumentParser(prog="python -m cast_simulator_b200.trajectory")
+    ap.add_argument("--n", type=int, default=16)
+    ap.add_argument("--depth", type=int, default=30)
+    ap.add_argument("--traj", type=int, default=4096)
+    ap.add_argument("--k", type=int, default=3, help="fusion width of the unitary blocks (<= 4)")
+    ap.add_argument("--p", type=float, default=1e-3, help="depolarizing after every gate")
+    ap.add_argument("--gamma", type=float, default=5e-4, help="amplitude damping per qubit per layer")
+    ap.add_argument("--reps", type=int, default=3)
+    a = ap.parse_args(argv)
+    circ = QuantumCircuit.brickwork(a.n, a.depth, 31337, depolarizing=a.p, damping=a.gamma)
+    prog = TrajectoryProgram(circ, a.k)
+    st = Stream()
+    prog.run(a.traj, 1, st)
+    best = float("inf")
+    for r in range(a.reps):
+        t0 = time.perf_counter()
+        prog.run(a.traj, 2 + r, st)
+        best = min(best, time.perf_counter() - t0)
+    print(json.dumps({"n": a.n, "depth": a.depth, "n_traj": a.traj, "seconds": best,
+                      "traj_per_s": a.traj / best, "blocks": prog.stats.n_blocks,
+                      "error_sites": prog.stats.n_errors}))
+
+
+if __name__ == "__main__":
+    _main()
