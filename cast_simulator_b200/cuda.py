@@ -82,6 +82,7 @@ class CudaStatevector:
         self._n = int(n_qubits)
         self._prec = CudaPrecision(precision)
         self._len = 2 << self._n
+        self._release = None
         eb = L.errbuf()
         self._dptr = L.lib().cast_cuda_sv_alloc(self._len, int(self._prec), eb, L.ERR_LEN)
         if not self._dptr:
@@ -90,11 +91,25 @@ class CudaStatevector:
     def __del__(self):
         p = getattr(self, "_dptr", 0)
         if p:
+            release = getattr(self, "_release", None)
             try:
+                if release is not None and release(self._n, self._prec, p, self._len):
+                    self._dptr = 0
+                    return
                 L.lib().cast_cuda_sv_free(p)
             except Exception:
                 pass
             self._dptr = 0
+
+    @classmethod
+    def _adopt(cls, n_qubits: int, precision: CudaPrecision, dptr: int, release=None) -> "CudaStatevector":
+        """Wrap an allocation handed back by a memory pool; ``release(n, prec,
+        dptr, len)`` is offered the allocation when this object dies (returns
+        True to keep it)."""
+        sv = cls.__new__(cls)
+        sv._n, sv._prec, sv._len, sv._dptr = int(n_qubits), CudaPrecision(precision), 2 << int(n_qubits), dptr
+        sv._release = release
+        return sv
 
     def n_qubits(self) -> int:
         return self._n

@@ -252,13 +252,45 @@ class Simulator:
     """Simulator<Cuda> (mod.rs:446-547)."""
 
     def __init__(self, spec: CudaKernelGenSpec | None = None, use_graph: bool = True,
-                 split_precision: bool = False):
+                 split_precision: bool = False, reuse_memory: bool = True):
         """split_precision: complex64 gates with 5 or 6 qubits run on the tensor
-        cores in split BF16 (about 1e-5 relative error per fused pass)."""
+        cores in split BF16 (about 1e-5 relative error per fused pass).
+        reuse_memory: when a returned QuantumState is dropped, its statevector
+        allocation is kept (one per qubit count and precision) for the next
+        ``simulate`` instead of being freed; ``release_memory`` frees them."""
         self.spec = spec or CudaKernelGenSpec.f64()
         self.use_graph = use_graph
         self.split_precision = split_precision
         self._stream = None
+        self.reuse_memory = reuse_memory
+        self._free: dict = {}  # (n, precision) -> (dptr, len)
+
+    def _release(self, n, prec, dptr, length) -> bool:
+        key = (n, int(prec))
+        if not self.reuse_memory or key in self._free:
+            return False
+        self._free[key] = (dptr, length)
+        return True
+
+    def _statevector(self, n: int) -> CudaStatevector:
+        hit = self._free.pop((n, int(self.spec.precision)), None)
+        if hit is not None:
+            return CudaStatevector._adopt(n, self.spec.precision, hit[0], self._release)
+        sv = CudaStatevector(n, self.spec.precision)
+        sv._release = self._release if self.reuse_memory else None
+        return sv
+
+    def release_memory(self) -> None:
+        """Free the statevector allocations kept for reuse."""
+        for dptr, _ in self._free.values():
+            L.lib().cast_cuda_sv_free(dptr)
+        self._free.clear()
+
+    def __del__(self):
+        try:
+            self.release_memory()
+        except Exception:
+            pass
 
     @classmethod
     def f64(cls) -> "Simulator":
@@ -289,7 +321,7 @@ class Simulator:
         n_phys = graph.n_qubits()
         gates, n_sv = prepare_gates(graph, n_phys, repr_)
         prog = self.compile_batch(gates, n_sv)
-        sv = CudaStatevector(n_sv, self.spec.precision)
+        sv = self._statevector(n_sv)
         if initial is None:
             sv.zero(self.stream)
         else:

@@ -181,3 +181,28 @@ def test_expectation_z_and_bench(mods, oracle):
     assert np.max(np.abs(z - z_ref)) < 1e-12
     rt = sim.bench(graph, budget_s=0.05)
     assert rt.exec.n_iters() >= 3 if hasattr(rt.exec, "n_iters") else len(rt.exec.samples_s) >= 3
+
+
+def test_simulate_reuses_statevector_memory(mods, oracle):
+    """A dropped QuantumState hands its allocation back to the Simulator; the
+    next simulate of the same width reuses it (no 2^n-sized cudaMalloc per call)
+    and the results are unaffected."""
+    L, cu, F, S, T = mods
+    n = 14
+    circ = T.QuantumCircuit.brickwork(n, 6, 21)
+    ref = oracle.simulate(n, _oracle_gates(circ))
+    sim = S.Simulator.f64()
+    g = F.CircuitGraph.from_circuit(circ)
+    st = sim.simulate(g)
+    p0 = st.sv.dptr
+    assert np.max(np.abs(st.download_amplitudes() - ref)) < 1e-10
+    del st
+    st2 = sim.simulate(g)
+    assert st2.sv.dptr == p0
+    assert np.max(np.abs(st2.download_amplitudes() - ref)) < 1e-10
+    keep = st2
+    st3 = sim.simulate(g)  # the first is still alive: a fresh allocation
+    assert st3.sv.dptr != keep.sv.dptr
+    del keep, st3
+    sim.release_memory()
+    assert sim._free == {}
