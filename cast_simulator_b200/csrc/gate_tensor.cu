@@ -849,6 +849,8 @@ int set_tensor_loader(int mode) { return g_tensor_loader.exchange(mode); }
 // Reads and clears the tensor kernel's error word (a bit per wait that expired).
 bool tensor_error_status(uint32_t *out, std::string &err) {
   uint32_t zero = 0;
+  // launches on non-blocking streams are not ordered with the legacy stream's copy
+  if (!cuda_ok(cudaDeviceSynchronize(), "cudaDeviceSynchronize (tensor error word)", err)) return false;
   if (!cuda_ok(cudaMemcpyFromSymbol(out, g_umma_error, sizeof(uint32_t)),
                "cudaMemcpyFromSymbol (tensor error word)", err))
     return false;

@@ -75,7 +75,8 @@ int cast_b200_program_set_split_precision(void *program, int enable, char *err_b
                                           size_t err_buf_len);
 /* Reads and clears the tensor-core kernel's error word: 0 when every bounded
  * wait of every launch since the last call completed, else a bit per wait kind
- * that expired (the affected tiles were left unwritten).  Synchronous. */
+ * that expired (the affected tiles were left unwritten).  Synchronizes the
+ * device first, so every launch issued before the call is covered. */
 int cast_b200_tensor_status(uint32_t *out_bits, char *err_buf, size_t err_buf_len);
 /* Selects how the tensor-core kernel loads amplitudes: 0 = automatic (TMA bulk
  * copies for 6-qubit gates whose lowest target qubit is >= 7 when the statevector has
