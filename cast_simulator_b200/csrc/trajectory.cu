@@ -27,6 +27,7 @@
 #include "../../include/cast_b200.h"
 #include "internal.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <exception>
 #include <mutex>
@@ -567,6 +568,59 @@ __global__ void __launch_bounds__(kTThreads, 1)
 
 constexpr uint32_t kTrajMagic = 0xCB2077A1u;
 
+// Access-policy window that keeps the per-CTA trajectory slices persisting in
+// L2 (each pass rereads the slice it just wrote; without it most dirty lines are
+// written back to HBM between passes and some reloads miss L2).  The persisting
+// set-aside is a limit of this process's context; it is raised once, to at most
+// the device's maximum, and never lowered.
+bool l2_window(void *base, size_t bytes, cudaAccessPolicyWindow &w) {
+  static std::mutex mu;
+  static size_t limit_set = 0;
+  int dev = 0, max_persist = 0, max_window = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev) != cudaSuccess ||
+      max_persist <= 0 || max_window <= 0) {
+    cudaGetLastError();
+    return false;
+  }
+  const size_t want = std::min(bytes, (size_t)max_persist);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (limit_set < want) {
+      if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+      }
+      limit_set = want;
+    }
+  }
+  w.base_ptr = base;
+  w.num_bytes = std::min(bytes, (size_t)max_window);
+  w.hitRatio = std::min(1.0f, (float)limit_set / (float)w.num_bytes);
+  w.hitProp = cudaAccessPropertyPersisting;
+  w.missProp = cudaAccessPropertyStreaming;
+  return true;
+}
+
+cudaError_t launch_trajectories(unsigned grid, cudaStream_t s, const cudaAccessPolicyWindow *w,
+                                const TOp *ops, uint32_t n_ops, const float2 *pool, float2 *ws,
+                                uint32_t n, const TRun *run, double *z, uint32_t *sample) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kTThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  if (w) {
+    attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+    attr[0].val.accessPolicyWindow = *w;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+  return cudaLaunchKernelEx(&cfg, k_trajectories, ops, n_ops, pool, ws, n, run, z, sample);
+}
+
 struct TrajProgram {
   uint32_t magic = kTrajMagic;
   uint32_t n = 0;
@@ -850,6 +904,8 @@ int cast_b200_traj_run(void *prog, uint32_t n_traj, uint64_t seed, double *out_z
       return 1;
     }
     const uint32_t n_ops = (uint32_t)p->ops.size();
+    cudaAccessPolicyWindow win = {};
+    const bool win_ok = l2_window(p->d_ws, (sizeof(float2) << p->n) * grid, win);
     if (use_graph && s) {
       if (p->graph && (p->graph_stream != stream || p->graph_grid != grid)) {
         cudaGraphExecDestroy(p->graph);
@@ -862,9 +918,9 @@ int cast_b200_traj_run(void *prog, uint32_t n_traj, uint64_t seed, double *out_z
           cb2::write_err(err_buf, err_buf_len, err);
           return 1;
         }
-        k_trajectories<<<grid, kTThreads, 0, s>>>(p->d_ops, n_ops, p->d_pool, p->d_ws, p->n,
-                                                  p->d_run, p->d_z, p->d_sample);
-        const cudaError_t lrc = cudaGetLastError();
+        const cudaError_t lrc = launch_trajectories(grid, s, win_ok ? &win : nullptr, p->d_ops, n_ops,
+                                                    p->d_pool, p->d_ws, p->n, p->d_run, p->d_z,
+                                                    p->d_sample);
         const cudaError_t erc = cudaStreamEndCapture(s, &gph);
         if (!cuda_ok(lrc, "trajectory kernel capture", err) ||
             !cuda_ok(erc, "cudaStreamEndCapture", err) ||
@@ -882,9 +938,9 @@ int cast_b200_traj_run(void *prog, uint32_t n_traj, uint64_t seed, double *out_z
         return 1;
       }
     } else {
-      k_trajectories<<<grid, kTThreads, 0, s>>>(p->d_ops, n_ops, p->d_pool, p->d_ws, p->n,
-                                                p->d_run, p->d_z, p->d_sample);
-      if (!cuda_ok(cudaGetLastError(), "trajectory kernel launch", err)) {
+      if (!cuda_ok(launch_trajectories(grid, s, win_ok ? &win : nullptr, p->d_ops, n_ops, p->d_pool,
+                                       p->d_ws, p->n, p->d_run, p->d_z, p->d_sample),
+                   "trajectory kernel launch", err)) {
         cb2::write_err(err_buf, err_buf_len, err);
         return 1;
       }
