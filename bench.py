@@ -539,6 +539,12 @@ def main(argv=None):
         zs = state.expectation_z()
         del state
     e2e_t = time.perf_counter() - e0
+    if pg:
+        import torch
+
+        et = torch.tensor([e2e_t], device=f"cuda:{local}", dtype=torch.float64)
+        pg.all_reduce(et, op=pg.ReduceOp.MAX)
+        e2e_t = float(et.item())
     e2e_value = ws * args.steps * len(gates) * bytes_per_pass / e2e_t / 1e9
 
     line = {
@@ -583,12 +589,14 @@ def main(argv=None):
         line["cpu_baseline"] = {
             "value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
             "sample": f"{passes} fused-gate passes of the {n_cpu}-qubit brickwork (k={args.k}) in {el:.1f} s"}
-    if rank == 0 and not args.no_extras:
+    # the extra legs run on one GPU only: under torchrun the other ranks would sit
+    # in the closing barrier for the minutes they take
+    if rank == 0 and ws == 1 and not args.no_extras:
         line["qft"] = qft_leg()
         line["tensor_path"] = tensor_leg(n, args.depth)
         line["trajectories"] = trajectory_leg()
         line["serving"] = serving_leg(args.serve_requests)
-    if rank == 0 and args.largest:
+    if rank == 0 and ws == 1 and args.largest:
         line["largest_fit"] = largest_leg()
     if rank == 0:
         print(json.dumps(line), flush=True)
