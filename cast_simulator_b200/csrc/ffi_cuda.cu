@@ -599,6 +599,10 @@ int cast_cuda_sv_zero(uint64_t dptr, size_t n_elements, uint8_t precision, char 
 int cast_cuda_sv_upload(uint64_t dptr, const double *host_data, size_t n_elements,
                         uint8_t precision, char *err_buf, size_t err_buf_len) {
   std::string err;
+  if (n_elements && (!dptr || !host_data)) {
+    write_err(err_buf, err_buf_len, "sv upload: null device or host pointer");
+    return 1;
+  }
   try {
     if (precision != 0) {
       if (!cuda_ok(cudaMemcpy(reinterpret_cast<void *>(dptr), host_data, n_elements * 8,
@@ -632,6 +636,10 @@ int cast_cuda_sv_upload(uint64_t dptr, const double *host_data, size_t n_element
 int cast_cuda_sv_download(uint64_t dptr, double *host_data, size_t n_elements, uint8_t precision,
                           char *err_buf, size_t err_buf_len) {
   std::string err;
+  if (n_elements && (!dptr || !host_data)) {
+    write_err(err_buf, err_buf_len, "sv download: null device or host pointer");
+    return 1;
+  }
   try {
     if (precision != 0) {
       if (!cuda_ok(cudaMemcpy(host_data, reinterpret_cast<const void *>(dptr), n_elements * 8,
