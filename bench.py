@@ -45,6 +45,16 @@ def measured_peak_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def measured_peak_bf16():
+    """Dense BF16 TFLOP/s (burst) from the driver's measurement, else the pool's
+    earlier measurement."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"])
+    except Exception:
+        return 1590.0
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -391,9 +401,18 @@ def tensor_leg(n: int, depth: int):
             if rep:
                 ts.append(e1.elapsed_s(e0))
         t = float(np.median(ts))
-        out["runs"].append({"fusion_k": k, "tensor_cores": split, "fused_gates": len(gates),
-                            "ms_per_circuit": t * 1e3,
-                            "hbm_gbs": len(gates) * 2 * (1 << n) * 8 / t / 1e9})
+        run = {"fusion_k": k, "tensor_cores": split, "fused_gates": len(gates),
+               "ms_per_circuit": t * 1e3, "hbm_gbs": len(gates) * 2 * (1 << n) * 8 / t / 1e9,
+               "hbm_frac": len(gates) * 2 * (1 << n) * 8 / t / 1e9 / measured_peak_hbm()[0]}
+        if split:
+            # tensor-pipe work of the passes that ran there: 3 split products of the
+            # real (2D x 2D) GEMM per group, D = 2^kg
+            flops = sum(3 * 2 * (2 << g.n_qubits()) ** 2 * (1 << (n - g.n_qubits()))
+                        for g in gates if g.n_qubits() in (5, 6))
+            peak = measured_peak_bf16()
+            run["tensor_tflops"] = flops / t / 1e12
+            run["tensor_frac"] = flops / t / 1e12 / peak if peak else None
+        out["runs"].append(run)
         del sv, prog
     base = out["runs"][0]["ms_per_circuit"]
     for r in out["runs"]:
