@@ -32,23 +32,30 @@ from .fusion import CircuitGraph, FusionConfig, optimize
 from .types import QuantumCircuit, QuantumGate, eye, expand_matrix, mat_x, mat_y, mat_z
 
 _PAULIS = (mat_x(), mat_y(), mat_z())
+_EYE2 = eye(2)
+
+
+def _close2(a: np.ndarray, b: np.ndarray, tol: float = 1e-9) -> bool:
+    """Elementwise |a - b| <= tol for 2x2 matrices, without numpy's per-call
+    overhead (the trajectory builder tests every noise site of a circuit)."""
+    return all(abs(x - y) <= tol for x, y in zip(a.ravel().tolist(), b.ravel().tolist()))
 
 
 def _is_pauli_channel(g: QuantumGate):
     """(p, [matrices]) for depolarizing / bit-flip / phase-flip channels on an
     identity base gate, else None."""
-    if g.is_unitary() or g.n_qubits() != 1 or not np.allclose(g.matrix(), eye(2)):
+    if g.is_unitary() or g.n_qubits() != 1 or not _close2(g.matrix(), _EYE2):
         return None
     br = g.noise_model().branches
-    if not np.allclose(br[0][1], eye(2)):
+    if not _close2(br[0][1], _EYE2):
         return None
     errs = br[1:]
     ps = [p for p, _ in errs]
     mats = [m for _, m in errs]
     for m in mats:
-        if not any(np.allclose(m, P) for P in _PAULIS):
+        if not any(_close2(m, P) for P in _PAULIS):
             return None
-    if len(errs) == 3 and np.allclose(ps, ps[0]):
+    if len(errs) == 3 and max(ps) - min(ps) <= 1e-12 * max(1.0, abs(ps[0])):
         return float(sum(ps)), mats
     if len(errs) == 1:
         return float(ps[0]), mats * 3
@@ -58,7 +65,7 @@ def _is_pauli_channel(g: QuantumGate):
 def _damping_rate(g: QuantumGate):
     """gamma for an amplitude-damping channel in the weighted-Kraus form
     (weights 1/2, operators sqrt(2) K0, sqrt(2) K1), else None."""
-    if g.is_unitary() or g.n_qubits() != 1 or not np.allclose(g.matrix(), eye(2)):
+    if g.is_unitary() or g.n_qubits() != 1 or not _close2(g.matrix(), _EYE2):
         return None
     br = g.noise_model().branches
     if len(br) != 2:
@@ -70,7 +77,7 @@ def _damping_rate(g: QuantumGate):
         return None
     gamma = 1.0 - abs(k0[1, 1]) ** 2
     exp1 = np.array([[0, math.sqrt(gamma)], [0, 0]])
-    if not np.allclose(k1, exp1, atol=1e-12):
+    if not _close2(k1, exp1, 1e-12):
         return None
     return gamma
 
@@ -145,12 +152,18 @@ class TrajectoryProgram:
             prov = block.provenance()
             bq = block.qubits()
             self._add_gate(block.matrix(), bq)
+            if not any(j in markers for j in prov):
+                continue
+            # suffix[pos] = product of the block's gates applied after gate pos
+            suffix = [None] * len(prov)
+            u = eye(1 << len(bq))
+            for pos in range(len(prov) - 1, -1, -1):
+                suffix[pos] = u
+                gi = seg[prov[pos]]
+                u = u @ expand_matrix(gi.matrix(), gi.qubits(), bq)
             for pos, j in enumerate(prov):
                 for q, p, mats in markers.get(j, ()):
-                    u = eye(1 << len(bq))
-                    for i in prov[pos + 1:]:
-                        gi = seg[i]
-                        u = expand_matrix(gi.matrix(), gi.qubits(), bq) @ u
+                    u = suffix[pos]
                     ud = u.conj().T
                     prop = [u @ expand_matrix(P, (q,), bq) @ ud for P in mats]
                     self._add_error(p, prop)
