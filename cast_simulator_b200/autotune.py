@@ -19,13 +19,17 @@ AI = peak / bw_slope to the hardware-adaptive cost model
   * ``choose_fusion`` fuses the circuit at every width k with the native
     planner and predicts its time from the measured per-pass times (scaled by
     2^(n - n_profile), the passes being memory-bound), then returns the width
-    and engine with the least predicted time.
+    and engine with the least predicted time;
+  * ``tune_trajectories`` times the batched-trajectory kernel of a noisy
+    circuit at each fusion width and launch shape (threads per CTA, CTAs in
+    flight) and returns the fastest.
 
 Command line:
 
     python -m cast_simulator_b200.autotune gate --k 6 --n 26 --mode tc [--low]
     python -m cast_simulator_b200.autotune profile --n 26 --precision f32 [--out prof.json]
     python -m cast_simulator_b200.autotune choose --n 30 --depth 20 --precision f32
+    python -m cast_simulator_b200.autotune traj --n 16 --depth 30
 """
 from __future__ import annotations
 
@@ -207,6 +211,45 @@ def choose_fusion(n: int, gates, precision: str, table: PassTable, ks=range(2, 7
     return Choice(best["fusion_k"], best["split_precision"], best["predicted_s"], cands)
 
 
+@dataclass
+class TrajChoice:
+    fusion_k: int
+    threads: int
+    max_ctas: int
+    traj_per_s: float
+    candidates: list
+
+
+def tune_trajectories(circuit, n_traj: int = 4096, ks=(2, 3, 4), threads=(0, 512, 1024),
+                      ctas=(0,), reps: int = 2, seed: int = 1) -> TrajChoice:
+    """Trajectories per second of ``circuit`` for every fusion width in ``ks``
+    and launch shape in ``threads`` x ``ctas`` (0 = the kernel's own choice by
+    state size), best of ``reps`` graph replays after one warm-up; returns the
+    fastest."""
+    import time
+
+    from .simulator import Stream
+    from .trajectory import TrajectoryProgram
+
+    st = Stream()
+    cands = []
+    for k in ks:
+        prog = TrajectoryProgram(circuit, k)
+        for th in threads:
+            for c in ctas:
+                prog.set_launch(th, c)
+                prog.run(n_traj, seed, st)
+                best = math.inf
+                for r in range(reps):
+                    t0 = time.perf_counter()
+                    prog.run(n_traj, seed + 1 + r, st)
+                    best = min(best, time.perf_counter() - t0)
+                cands.append({"fusion_k": k, "threads": th, "max_ctas": c,
+                              "traj_per_s": n_traj / best})
+    top = max(cands, key=lambda c: c["traj_per_s"])
+    return TrajChoice(top["fusion_k"], top["threads"], top["max_ctas"], top["traj_per_s"], cands)
+
+
 def _main(argv=None) -> None:
     ap = argparse.ArgumentParser(prog="python -m cast_simulator_b200.autotune")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -225,8 +268,21 @@ def _main(argv=None) -> None:
     c.add_argument("--depth", type=int, default=20)
     c.add_argument("--precision", choices=("f64", "f32"), default="f32")
     c.add_argument("--profile-n", type=int, default=26)
+    t = sub.add_parser("traj", help="fusion width / launch shape for noisy brickwork trajectories")
+    t.add_argument("--n", type=int, default=16)
+    t.add_argument("--depth", type=int, default=30)
+    t.add_argument("--traj", type=int, default=4096)
+    t.add_argument("--p", type=float, default=1e-3)
+    t.add_argument("--gamma", type=float, default=5e-4)
     a = ap.parse_args(argv)
-    if a.cmd == "gate":
+    if a.cmd == "traj":
+        from .types import QuantumCircuit
+
+        circ = QuantumCircuit.brickwork(a.n, a.depth, 31337, depolarizing=a.p, damping=a.gamma)
+        ch = tune_trajectories(circ, a.traj)
+        print(json.dumps({"fusion_k": ch.fusion_k, "threads": ch.threads, "max_ctas": ch.max_ctas,
+                          "traj_per_s": ch.traj_per_s, "candidates": ch.candidates}))
+    elif a.cmd == "gate":
         t = time_gate(a.n, a.k, a.mode, a.low, a.reps)
         b = 2 * (1 << a.n) * (16 if a.mode == "f64" else 8)
         print(json.dumps({"k": a.k, "n": a.n, "mode": a.mode, "low_targets": a.low,

@@ -5,10 +5,10 @@
 // p_i and launches one kernel per gate per member, syncing with the host at
 // every noisy gate) with quantum-jump trajectories sampled on the device:
 //
-//  * one CTA (1024 threads) owns one trajectory at a time; its 2^n complex64
-//    statevector lives in a per-CTA slice of a workspace in global memory
-//    (148 CTAs x 512 KiB = 74 MiB at 16 qubits, resident in the 126 MB L2);
-//    the CTA loops over trajectories blockIdx.x, blockIdx.x + gridDim.x, ...
+//  * one CTA (512 or 1024 threads) owns one trajectory at a time; its 2^n
+//    complex64 statevector lives in a per-CTA slice of a workspace in global
+//    memory (148 CTAs x 512 KiB = 74 MiB at 16 qubits, resident in the 126 MB
+//    L2); the CTA loops over trajectories blockIdx.x, blockIdx.x + gridDim.x, ...
 //  * GATE ops are fused unitary blocks (k <= 4) applied in place;
 //  * ERR ops are state-independent Pauli errors (depolarizing): a Philox draw
 //    decides; when one fires, the Pauli propagated to the end of its fused
@@ -37,10 +37,9 @@ namespace {
 
 using cb2::cuda_ok;
 
-constexpr int kTThreads = 1024;
-constexpr uint32_t kTLogThreads = 10;
+// A CTA has 512 or 1024 threads (the kernel is instantiated for both).
+constexpr int kTMinThreads = 512, kTMaxThreads = 1024;
 constexpr uint32_t kTrajMaxQubits = 22;
-constexpr int kTLoQubits = kTrajMaxQubits - kTLogThreads;  // qubits inside a thread's chunk
 constexpr uint32_t kTrajMaxGate = 4;
 
 enum : uint32_t { T_GATE = 0, T_ERR = 1, T_DAMP = 2, T_CHAN = 3 };
@@ -87,13 +86,24 @@ __device__ __forceinline__ double philox_uniform(uint64_t seed, uint32_t traj, u
 }
 
 struct Shared {
-  double red[3][kTThreads / 32];
+  double red[3][kTMaxThreads / 32];
   double vals[4];
   float dtab[kTrajMaxQubits + 1];  // pending diagonal: scale * s^popc
   double stab[kTrajMaxQubits + 1]; // damping weights (1 - g)^popc for the sums
   uint32_t pmask;
   int pend;
 };
+
+// Two FP32 fused multiply-adds in one instruction (PTX fma.rn.f32x2, sm_100a):
+// (a.x * b.x + c.x, a.y * b.y + c.y), each rounded once as fmaf.
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;"
+      : "=l"(d)
+      : "l"(*reinterpret_cast<const uint64_t *>(&a)), "l"(*reinterpret_cast<const uint64_t *>(&b)),
+        "l"(*reinterpret_cast<const uint64_t *>(&c)));
+  return *reinterpret_cast<const float2 *>(&d);
+}
 
 __device__ __forceinline__ float2 cmul_add(float2 m, float2 x, float2 acc) {
   acc.x = fmaf(m.x, x.x, acc.x);
@@ -103,410 +113,464 @@ __device__ __forceinline__ float2 cmul_add(float2 m, float2 x, float2 acc) {
   return acc;
 }
 
-// Block sum of up to three doubles; every thread gets the results.
-__device__ void block_sum3(Shared &S, double &a, double &b, double &c) {
+// The device side of one trajectory, for CTAs of NT threads.  512-thread CTAs
+// get 128 registers a thread and use packed FMAs for the gates (the passes of
+// small and HBM-sized states are bound by instruction issue); 1024-thread CTAs
+// keep twice the loads in flight, which is what the L2-resident states of 15 to
+// 17 qubits need.
+template <int NT>
+struct Traj {
+  static constexpr int kTThreads = NT;
+  static constexpr uint32_t kTLogThreads = NT == 1024 ? 10 : 9;
+  static constexpr bool kPacked = NT == 512;
+
+  // Block sum of up to three doubles; every thread gets the results.
+  static __device__ void block_sum3(Shared &S, double &a, double &b, double &c) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_down_sync(0xffffffffu, a, o);
-    b += __shfl_down_sync(0xffffffffu, b, o);
-    c += __shfl_down_sync(0xffffffffu, c, o);
-  }
-  const int w = threadIdx.x >> 5;
-  if ((threadIdx.x & 31) == 0) {
-    S.red[0][w] = a;
-    S.red[1][w] = b;
-    S.red[2][w] = c;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double x = 0, y = 0, z = 0;
-    for (int i = 0; i < kTThreads / 32; ++i) {
-      x += S.red[0][i];
-      y += S.red[1][i];
-      z += S.red[2][i];
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+      c += __shfl_down_sync(0xffffffffu, c, o);
     }
-    S.vals[0] = x;
-    S.vals[1] = y;
-    S.vals[2] = z;
-  }
-  __syncthreads();
-  a = S.vals[0];
-  b = S.vals[1];
-  c = S.vals[2];
-  __syncthreads();
-}
-
-__device__ void fill_stab(Shared &S, double g) {
-  if (threadIdx.x == 0) {
-    double f = 1.0;
-    for (uint32_t c = 0; c <= kTrajMaxQubits; ++c) {
-      S.stab[c] = f;
-      f *= 1.0 - g;
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+      S.red[0][w] = a;
+      S.red[1][w] = b;
+      S.red[2][w] = c;
     }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double x = 0, y = 0, z = 0;
+      for (int i = 0; i < kTThreads / 32; ++i) {
+        x += S.red[0][i];
+        y += S.red[1][i];
+        z += S.red[2][i];
+      }
+      S.vals[0] = x;
+      S.vals[1] = y;
+      S.vals[2] = z;
+    }
+    __syncthreads();
+    a = S.vals[0];
+    b = S.vals[1];
+    c = S.vals[2];
+    __syncthreads();
   }
-  __syncthreads();
-}
 
-__device__ __forceinline__ float2 pend_load(const float2 *sv, uint32_t i, const Shared &S) {
-  float2 v = sv[i];
-  if (S.pend) {
-    const float f = S.dtab[__popc(i & S.pmask)];
-    v.x *= f;
-    v.y *= f;
-  }
-  return v;
-}
-
-// Fused-gate pass (k = K).  PEND: the pending diagonal (scale * s^popc(i & pmask))
-// is applied to every loaded amplitude.  With op.stats the pass also sums, over
-// its outputs, t += |o|^2 and d += |o|^2 (1-g)^popc(i & smask) for the damping op
-// that follows.  k = 1 gates take two groups per thread.
-template <int K, bool PEND>
-__device__ __noinline__ void gate_pass(float2 *sv, uint32_t n, const TOp &op, const float2 *M,
-                                       const Shared &S, double &t, double &d) {
-  constexpr int D = 1 << K;
-  constexpr int U = K == 1 ? 2 : 1;
-  uint32_t lo[K];
-#pragma unroll
-  for (int b = 0; b < K; ++b) lo[b] = (1u << op.q[b]) - 1;
-  const uint32_t ng = 1u << (n - K);
-  const bool stats = op.stats != 0;
-  const uint32_t smask = op.smask;
-  const uint32_t pmask = S.pmask;
-  double lt = 0, ld = 0;
-  for (uint32_t g0 = threadIdx.x; g0 < ng; g0 += kTThreads * U) {
-    uint32_t base[U];
-    float2 x[U][D];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const uint32_t g = g0 + u * kTThreads;
-      uint32_t bb = g < ng ? g : 0;
-#pragma unroll
-      for (int b = 0; b < K; ++b) bb = ((bb & ~lo[b]) << 1) | (bb & lo[b]);
-      base[u] = bb;
-#pragma unroll
-      for (int a = 0; a < D; ++a) {
-        uint32_t o = bb;
-#pragma unroll
-        for (int b = 0; b < K; ++b)
-          if ((a >> b) & 1) o += lo[b] + 1;
-        float2 v = make_float2(0.f, 0.f);
-        if (g < ng) v = sv[o];
-        if (PEND) {
-          const float f = S.dtab[__popc(o & pmask)];
-          v.x *= f;
-          v.y *= f;
-        }
-        x[u][a] = v;
+  static __device__ void fill_stab(Shared &S, double g) {
+    if (threadIdx.x == 0) {
+      double f = 1.0;
+      for (uint32_t c = 0; c <= kTrajMaxQubits; ++c) {
+        S.stab[c] = f;
+        f *= 1.0 - g;
       }
     }
-#pragma unroll
-    for (int r = 0; r < D; ++r) {
-      float2 acc[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) acc[u] = make_float2(0.f, 0.f);
-#pragma unroll
-      for (int c = 0; c < D; ++c) {
-        const float2 m = M[r * D + c];
-#pragma unroll
-        for (int u = 0; u < U; ++u) acc[u] = cmul_add(m, x[u][c], acc[u]);
-      }
-      uint32_t roff = 0;
-#pragma unroll
-      for (int b = 0; b < K; ++b)
-        if ((r >> b) & 1) roff += lo[b] + 1;
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (g0 + u * kTThreads < ng) {
-          const uint32_t o = base[u] + roff;
-          sv[o] = acc[u];
-          if (stats) {
-            const double p = (double)acc[u].x * acc[u].x + (double)acc[u].y * acc[u].y;
-            lt += p;
-            ld += p * S.stab[__popc(o & smask)];
-          }
-        }
-      }
-    }
+    __syncthreads();
   }
-  t += lt;
-  d += ld;
-}
 
-__device__ void dispatch_gate(float2 *sv, uint32_t n, const TOp &op, const float2 *M, Shared &S,
-                              double &t, double &d) {
-  if (S.pend) {
-    switch (op.k) {
-    case 1: gate_pass<1, true>(sv, n, op, M, S, t, d); break;
-    case 2: gate_pass<2, true>(sv, n, op, M, S, t, d); break;
-    case 3: gate_pass<3, true>(sv, n, op, M, S, t, d); break;
-    default: gate_pass<4, true>(sv, n, op, M, S, t, d); break;
-    }
-  } else {
-    switch (op.k) {
-    case 1: gate_pass<1, false>(sv, n, op, M, S, t, d); break;
-    case 2: gate_pass<2, false>(sv, n, op, M, S, t, d); break;
-    case 3: gate_pass<3, false>(sv, n, op, M, S, t, d); break;
-    default: gate_pass<4, false>(sv, n, op, M, S, t, d); break;
-    }
-  }
-}
-
-// Stage a 2^k x 2^k matrix into shared memory.
-__device__ void stage_matrix(float2 *Msm, const float2 *pool, uint32_t off, uint32_t entries) {
-  for (uint32_t i = threadIdx.x; i < entries; i += kTThreads) Msm[i] = pool[off + i];
-  __syncthreads();
-}
-
-// Materialise the pending diagonal (and optionally compute sums):
-// t = sum |a|^2, d = sum |a|^2 * w(i) with w = (1-g)^popc(i & mask), j = g * sum_{bit q} |a|^2.
-__device__ __noinline__ void stats_pass(float2 *sv, uint32_t n, Shared &S, uint32_t mask, double g, uint32_t q,
-                           double &t, double &d, double &j) {
-  t = d = j = 0;
-  fill_stab(S, g);
-  const uint32_t N = 1u << n;
-  for (uint32_t i = threadIdx.x; i < N; i += kTThreads) {
+  static __device__ __forceinline__ float2 pend_load(const float2 *sv, uint32_t i, const Shared &S) {
     float2 v = sv[i];
     if (S.pend) {
       const float f = S.dtab[__popc(i & S.pmask)];
       v.x *= f;
       v.y *= f;
-      sv[i] = v;
     }
-    const double p = (double)v.x * v.x + (double)v.y * v.y;
-    t += p;
-    d += p * S.stab[__popc(i & mask)];
-    if ((i >> q) & 1) j += p;
+    return v;
   }
-  __syncthreads();
-  if (threadIdx.x == 0) S.pend = 0;
-  block_sum3(S, t, d, j);
-  j *= g;
-}
 
-__device__ void set_pending(Shared &S, uint32_t mask, double gamma, double scale) {
-  if (threadIdx.x == 0) {
-    S.pend = 1;
-    S.pmask = mask;
-    const double s = sqrt(1.0 - gamma);
-    double f = scale;
-    for (uint32_t c = 0; c <= kTrajMaxQubits; ++c) {
-      S.dtab[c] = (float)f;
-      f *= s;
+  // Fused-gate pass (k = K).  PEND: the pending diagonal (scale * s^popc(i & pmask))
+  // is applied to every loaded amplitude.  With op.stats the pass also sums, over
+  // its outputs, t += |o|^2 and d += |o|^2 (1-g)^popc(i & smask) for the damping op
+  // that follows.
+  //
+  // Packed: M holds each entry as (re, re, im, im); one 16-byte shared load and
+  // two packed FMAs give a += re * x and b += im * x for a complex amplitude x,
+  // and the output is (a.x - b.y, a.y + b.x).  Otherwise M holds complex
+  // entries and each product is four FMAs.  k = 1 gates take two groups a
+  // thread, so every matrix load serves both.
+  template <int K>
+  static constexpr int groups_per_thread() { return K == 1 ? 2 : 1; }
+
+  template <int K, bool PEND>
+  static __device__ __noinline__ void gate_pass(float2 *sv, uint32_t n, const TOp &op, const float4 *M,
+                                         const Shared &S, double &t, double &d) {
+    constexpr int D = 1 << K;
+    constexpr int U = groups_per_thread<K>();
+    uint32_t lo[K];
+#pragma unroll
+    for (int b = 0; b < K; ++b) lo[b] = (1u << op.q[b]) - 1;
+    const uint32_t ng = 1u << (n - K);
+    const bool stats = op.stats != 0;
+    const uint32_t smask = op.smask;
+    const uint32_t pmask = S.pmask;
+    double lt = 0, ld = 0;
+    for (uint32_t g0 = threadIdx.x; g0 < ng; g0 += kTThreads * U) {
+      uint32_t base[U];
+      float2 x[U][D];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const uint32_t g = g0 + u * kTThreads;
+        uint32_t bb = g < ng ? g : 0;
+#pragma unroll
+        for (int b = 0; b < K; ++b) bb = ((bb & ~lo[b]) << 1) | (bb & lo[b]);
+        base[u] = bb;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          uint32_t o = bb;
+#pragma unroll
+          for (int b = 0; b < K; ++b)
+            if ((a >> b) & 1) o += lo[b] + 1;
+          float2 v = make_float2(0.f, 0.f);
+          if (g < ng) v = sv[o];
+          if (PEND) {
+            const float f = S.dtab[__popc(o & pmask)];
+            v.x *= f;
+            v.y *= f;
+          }
+          x[u][a] = v;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < D; ++r) {
+        float2 acc[U];
+        if constexpr (kPacked) {
+          float2 ar[U], ai[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) ar[u] = ai[u] = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int c = 0; c < D; ++c) {
+            const float4 m = M[r * D + c];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              ar[u] = ffma2(make_float2(m.x, m.y), x[u][c], ar[u]);
+              ai[u] = ffma2(make_float2(m.z, m.w), x[u][c], ai[u]);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) acc[u] = make_float2(ar[u].x - ai[u].y, ar[u].y + ai[u].x);
+        } else {
+#pragma unroll
+          for (int u = 0; u < U; ++u) acc[u] = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int c = 0; c < D; ++c) {
+            const float2 m = reinterpret_cast<const float2 *>(M)[r * D + c];
+#pragma unroll
+            for (int u = 0; u < U; ++u) acc[u] = cmul_add(m, x[u][c], acc[u]);
+          }
+        }
+        uint32_t roff = 0;
+#pragma unroll
+        for (int b = 0; b < K; ++b)
+          if ((r >> b) & 1) roff += lo[b] + 1;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (g0 + u * kTThreads < ng) {
+            const uint32_t o = base[u] + roff;
+            sv[o] = acc[u];
+            if (stats) {
+              const double p = (double)acc[u].x * acc[u].x + (double)acc[u].y * acc[u].y;
+              lt += p;
+              ld += p * S.stab[__popc(o & smask)];
+            }
+          }
+        }
+      }
     }
+    t += lt;
+    d += ld;
   }
-  __syncthreads();
-}
 
-// Elementwise single-qubit damping branch on qubit q: jump -> x0 = sqrt(g) x1, x1 = 0;
-// no jump -> x1 *= sqrt(1 - g).
-__device__ __noinline__ void damp_apply(float2 *sv, uint32_t n, uint32_t q, double g, bool jump) {
-  const uint32_t npair = 1u << (n - 1);
-  const uint32_t lo = (1u << q) - 1;
-  const float sj = (float)sqrt(g), sn = (float)sqrt(1.0 - g);
-  for (uint32_t p = threadIdx.x; p < npair; p += kTThreads) {
-    const uint32_t i0 = ((p & ~lo) << 1) | (p & lo), i1 = i0 | (1u << q);
-    const float2 x1 = sv[i1];
-    if (jump) {
-      sv[i0] = make_float2(sj * x1.x, sj * x1.y);
-      sv[i1] = make_float2(0.f, 0.f);
+  static __device__ void dispatch_gate(float2 *sv, uint32_t n, const TOp &op, const float4 *M, Shared &S,
+                                double &t, double &d) {
+    if (S.pend) {
+      switch (op.k) {
+      case 1: gate_pass<1, true>(sv, n, op, M, S, t, d); break;
+      case 2: gate_pass<2, true>(sv, n, op, M, S, t, d); break;
+      case 3: gate_pass<3, true>(sv, n, op, M, S, t, d); break;
+      default: gate_pass<4, true>(sv, n, op, M, S, t, d); break;
+      }
     } else {
-      sv[i1] = make_float2(sn * x1.x, sn * x1.y);
+      switch (op.k) {
+      case 1: gate_pass<1, false>(sv, n, op, M, S, t, d); break;
+      case 2: gate_pass<2, false>(sv, n, op, M, S, t, d); break;
+      case 3: gate_pass<3, false>(sv, n, op, M, S, t, d); break;
+      default: gate_pass<4, false>(sv, n, op, M, S, t, d); break;
+      }
     }
   }
-  __syncthreads();
-}
 
-// General single-qubit channel: p_j = ||K_j psi||^2 (FP64), pick j, apply K_j / sqrt(p_j).
-__device__ __noinline__ void chan_op(float2 *sv, uint32_t n, const TOp &op, const float2 *pool,
-                                     float2 *Msm, Shared &S, uint64_t seed, uint32_t traj,
-                                     uint32_t &ev) {
-  const uint32_t N = 1u << n;
-  stage_matrix(Msm, pool, op.mat, 4 * op.nk);
-  const uint32_t q = op.q[0];
-  const uint32_t lo = (1u << q) - 1;
-  double pj[4] = {0, 0, 0, 0};
-  for (uint32_t p = threadIdx.x; p < N / 2; p += kTThreads) {
-    const uint32_t i0 = ((p & ~lo) << 1) | (p & lo), i1 = i0 | (1u << q);
-    const float2 x0 = pend_load(sv, i0, S), x1 = pend_load(sv, i1, S);
-    for (uint32_t b = 0; b < op.nk; ++b) {
-      const float2 y0 = cmul_add(Msm[4 * b + 1], x1, cmul_add(Msm[4 * b], x0, make_float2(0, 0)));
-      const float2 y1 = cmul_add(Msm[4 * b + 3], x1, cmul_add(Msm[4 * b + 2], x0, make_float2(0, 0)));
-      pj[b] += (double)y0.x * y0.x + (double)y0.y * y0.y + (double)y1.x * y1.x + (double)y1.y * y1.y;
+  // Stage a 2^k x 2^k matrix into shared memory.
+  static __device__ void stage_matrix(float2 *Msm, const float2 *pool, uint32_t off, uint32_t entries) {
+    for (uint32_t i = threadIdx.x; i < entries; i += kTThreads) Msm[i] = pool[off + i];
+    __syncthreads();
+  }
+
+  // Stage a 2^k x 2^k gate matrix into shared memory: (re, re, im, im) entries
+  // for the packed arithmetic, plain complex entries otherwise.
+  static __device__ void stage_gate(float4 *Msm, const float2 *pool, uint32_t off, uint32_t entries) {
+    for (uint32_t i = threadIdx.x; i < entries; i += kTThreads) {
+      const float2 m = pool[off + i];
+      if constexpr (kPacked) Msm[i] = make_float4(m.x, m.x, m.y, m.y);
+      else reinterpret_cast<float2 *>(Msm)[i] = m;
     }
+    __syncthreads();
   }
-  double a = pj[0], b = pj[1], c = pj[2];
-  block_sum3(S, a, b, c);
-  double d3 = pj[3], z0 = 0, z1 = 0;
-  block_sum3(S, d3, z0, z1);
-  const double tot[4] = {a, b, c, d3};
-  double sum = 0;
-  for (uint32_t bb = 0; bb < op.nk; ++bb) sum += tot[bb];
-  const double v = philox_uniform(seed, traj, ev++) * sum;
-  uint32_t pick = op.nk - 1;
-  double acc = 0;
-  for (uint32_t bb = 0; bb < op.nk; ++bb) {
-    acc += tot[bb];
-    if (v < acc) {
-      pick = bb;
-      break;
+
+  // Materialise the pending diagonal (and optionally compute sums):
+  // t = sum |a|^2, d = sum |a|^2 * w(i) with w = (1-g)^popc(i & mask), j = g * sum_{bit q} |a|^2.
+  static __device__ __noinline__ void stats_pass(float2 *sv, uint32_t n, Shared &S, uint32_t mask, double g, uint32_t q,
+                             double &t, double &d, double &j) {
+    t = d = j = 0;
+    fill_stab(S, g);
+    const uint32_t N = 1u << n;
+    for (uint32_t i = threadIdx.x; i < N; i += kTThreads) {
+      float2 v = sv[i];
+      if (S.pend) {
+        const float f = S.dtab[__popc(i & S.pmask)];
+        v.x *= f;
+        v.y *= f;
+        sv[i] = v;
+      }
+      const double p = (double)v.x * v.x + (double)v.y * v.y;
+      t += p;
+      d += p * S.stab[__popc(i & mask)];
+      if ((i >> q) & 1) j += p;
     }
+    __syncthreads();
+    if (threadIdx.x == 0) S.pend = 0;
+    block_sum3(S, t, d, j);
+    j *= g;
   }
-  const float sc = (float)(tot[pick] > 0 ? 1.0 / sqrt(tot[pick]) : 0.0);
-  const float2 *K = Msm + 4 * pick;
-  for (uint32_t p = threadIdx.x; p < N / 2; p += kTThreads) {
-    const uint32_t i0 = ((p & ~lo) << 1) | (p & lo), i1 = i0 | (1u << q);
-    const float2 x0 = pend_load(sv, i0, S), x1 = pend_load(sv, i1, S);
-    const float2 y0 = cmul_add(K[1], x1, cmul_add(K[0], x0, make_float2(0, 0)));
-    const float2 y1 = cmul_add(K[3], x1, cmul_add(K[2], x0, make_float2(0, 0)));
-    sv[i0] = make_float2(y0.x * sc, y0.y * sc);
-    sv[i1] = make_float2(y1.x * sc, y1.y * sc);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) S.pend = 0;
-  __syncthreads();
-}
 
-// Applies a Pauli error op (one of three k-qubit matrices) as a gate pass.
-__device__ __noinline__ void err_apply(float2 *sv, uint32_t n, const TOp &op, double u,
-                                       const float2 *pool, float2 *Msm, Shared &S) {
-  const uint32_t which = min(2u, (uint32_t)(u / (double)op.prob * 3.0));
-  const uint32_t e = 1u << (2 * op.k);
-  stage_matrix(Msm, pool, op.mat + which * e, e);
-  TOp g = op;
-  g.stats = 0;
-  double t = 0, d = 0;
-  dispatch_gate(sv, n, g, Msm, S, t, d);
-  __syncthreads();
-  if (threadIdx.x == 0) S.pend = 0;
-  __syncthreads();
-}
+  static __device__ void set_pending(Shared &S, uint32_t mask, double gamma, double scale) {
+    if (threadIdx.x == 0) {
+      S.pend = 1;
+      S.pmask = mask;
+      const double s = sqrt(1.0 - gamma);
+      double f = scale;
+      for (uint32_t c = 0; c <= kTrajMaxQubits; ++c) {
+        S.dtab[c] = (float)f;
+        f *= s;
+      }
+    }
+    __syncthreads();
+  }
 
-// Amplitude damping on op.mask: exact sampling of the joint jump pattern.
-__device__ __noinline__ void damp_op(float2 *sv, uint32_t n, const TOp &op, Shared &S,
-                                     uint64_t seed, uint32_t traj, uint32_t &ev, double T,
-                                     double Dd, bool stats_valid) {
-  const double g = (double)op.gamma;
-  if (!stats_valid) {
-    double j;
-    stats_pass(sv, n, S, op.mask, g, 0, T, Dd, j);
+  // Elementwise single-qubit damping branch on qubit q: jump -> x0 = sqrt(g) x1, x1 = 0;
+  // no jump -> x1 *= sqrt(1 - g).
+  static __device__ __noinline__ void damp_apply(float2 *sv, uint32_t n, uint32_t q, double g, bool jump) {
+    const uint32_t npair = 1u << (n - 1);
+    const uint32_t lo = (1u << q) - 1;
+    const float sj = (float)sqrt(g), sn = (float)sqrt(1.0 - g);
+    for (uint32_t p = threadIdx.x; p < npair; p += kTThreads) {
+      const uint32_t i0 = ((p & ~lo) << 1) | (p & lo), i1 = i0 | (1u << q);
+      const float2 x1 = sv[i1];
+      if (jump) {
+        sv[i0] = make_float2(sj * x1.x, sj * x1.y);
+        sv[i1] = make_float2(0.f, 0.f);
+      } else {
+        sv[i1] = make_float2(sn * x1.x, sn * x1.y);
+      }
+    }
+    __syncthreads();
   }
-  const double u = philox_uniform(seed, traj, ev++);
-  if (u * T < Dd) {  // no jump on any qubit of the mask
-    set_pending(S, op.mask, g, 1.0 / sqrt(Dd));
-    return;
-  }
-  // at least one jump: sample qubit by qubit, conditioned on a jump occurring
-  if (S.pend) {
-    double a, b, c;
-    stats_pass(sv, n, S, 0, 0.0, 0, a, b, c);
-  }
-  bool need = true;
-  for (uint32_t q = 0; q < n; ++q) {
-    if (!((op.mask >> q) & 1)) continue;
-    const uint32_t rem = op.mask & ~((1u << q) - 1);
-    double t, zsum, j;
-    stats_pass(sv, n, S, rem, g, q, t, zsum, j);
-    const double p1 = need ? (t - zsum > 0 ? j / (t - zsum) : 1.0) : (t > 0 ? j / t : 0.0);
-    const double v = philox_uniform(seed, traj, ev++);
-    const bool jump = v < p1;
-    damp_apply(sv, n, q, g, jump);
-    if (jump) need = false;
-  }
-  double t, a, b;
-  stats_pass(sv, n, S, 0, 0.0, 0, t, a, b);
-  set_pending(S, 0, 0.0, t > 0 ? 1.0 / sqrt(t) : 1.0);
-}
 
-// End of a trajectory: <Z_q> for every qubit and one sampled bitstring.
-__device__ __noinline__ void finish(float2 *sv, uint32_t n, Shared &S, double *csum, uint64_t seed,
-                                    uint32_t traj, double *out_z, uint32_t *out_sample) {
-  {
+  // General single-qubit channel: p_j = ||K_j psi||^2 (FP64), pick j, apply K_j / sqrt(p_j).
+  static __device__ __noinline__ void chan_op(float2 *sv, uint32_t n, const TOp &op, const float2 *pool,
+                                       float2 *Msm, Shared &S, uint64_t seed, uint32_t traj,
+                                       uint32_t &ev) {
+    const uint32_t N = 1u << n;
+    stage_matrix(Msm, pool, op.mat, 4 * op.nk);
+    const uint32_t q = op.q[0];
+    const uint32_t lo = (1u << q) - 1;
+    double pj[4] = {0, 0, 0, 0};
+    for (uint32_t p = threadIdx.x; p < N / 2; p += kTThreads) {
+      const uint32_t i0 = ((p & ~lo) << 1) | (p & lo), i1 = i0 | (1u << q);
+      const float2 x0 = pend_load(sv, i0, S), x1 = pend_load(sv, i1, S);
+      for (uint32_t b = 0; b < op.nk; ++b) {
+        const float2 y0 = cmul_add(Msm[4 * b + 1], x1, cmul_add(Msm[4 * b], x0, make_float2(0, 0)));
+        const float2 y1 = cmul_add(Msm[4 * b + 3], x1, cmul_add(Msm[4 * b + 2], x0, make_float2(0, 0)));
+        pj[b] += (double)y0.x * y0.x + (double)y0.y * y0.y + (double)y1.x * y1.x + (double)y1.y * y1.y;
+      }
+    }
+    double a = pj[0], b = pj[1], c = pj[2];
+    block_sum3(S, a, b, c);
+    double d3 = pj[3], z0 = 0, z1 = 0;
+    block_sum3(S, d3, z0, z1);
+    const double tot[4] = {a, b, c, d3};
+    double sum = 0;
+    for (uint32_t bb = 0; bb < op.nk; ++bb) sum += tot[bb];
+    const double v = philox_uniform(seed, traj, ev++) * sum;
+    uint32_t pick = op.nk - 1;
+    double acc = 0;
+    for (uint32_t bb = 0; bb < op.nk; ++bb) {
+      acc += tot[bb];
+      if (v < acc) {
+        pick = bb;
+        break;
+      }
+    }
+    const float sc = (float)(tot[pick] > 0 ? 1.0 / sqrt(tot[pick]) : 0.0);
+    const float2 *K = Msm + 4 * pick;
+    for (uint32_t p = threadIdx.x; p < N / 2; p += kTThreads) {
+      const uint32_t i0 = ((p & ~lo) << 1) | (p & lo), i1 = i0 | (1u << q);
+      const float2 x0 = pend_load(sv, i0, S), x1 = pend_load(sv, i1, S);
+      const float2 y0 = cmul_add(K[1], x1, cmul_add(K[0], x0, make_float2(0, 0)));
+      const float2 y1 = cmul_add(K[3], x1, cmul_add(K[2], x0, make_float2(0, 0)));
+      sv[i0] = make_float2(y0.x * sc, y0.y * sc);
+      sv[i1] = make_float2(y1.x * sc, y1.y * sc);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) S.pend = 0;
+    __syncthreads();
+  }
+
+  // Applies a Pauli error op (one of three k-qubit matrices) as a gate pass.
+  static __device__ __noinline__ void err_apply(float2 *sv, uint32_t n, const TOp &op, double u,
+                                         const float2 *pool, float4 *Msm, Shared &S) {
+    const uint32_t which = min(2u, (uint32_t)(u / (double)op.prob * 3.0));
+    const uint32_t e = 1u << (2 * op.k);
+    stage_gate(Msm, pool, op.mat + which * e, e);
+    TOp g = op;
+    g.stats = 0;
+    double t = 0, d = 0;
+    dispatch_gate(sv, n, g, Msm, S, t, d);
+    __syncthreads();
+    if (threadIdx.x == 0) S.pend = 0;
+    __syncthreads();
+  }
+
+  // Amplitude damping on op.mask: exact sampling of the joint jump pattern.
+  static __device__ __noinline__ void damp_op(float2 *sv, uint32_t n, const TOp &op, Shared &S,
+                                       uint64_t seed, uint32_t traj, uint32_t &ev, double T,
+                                       double Dd, bool stats_valid) {
+    const double g = (double)op.gamma;
+    if (!stats_valid) {
+      double j;
+      stats_pass(sv, n, S, op.mask, g, 0, T, Dd, j);
+    }
+    const double u = philox_uniform(seed, traj, ev++);
+    if (u * T < Dd) {  // no jump on any qubit of the mask
+      set_pending(S, op.mask, g, 1.0 / sqrt(Dd));
+      return;
+    }
+    // at least one jump: sample qubit by qubit, conditioned on a jump occurring
+    if (S.pend) {
+      double a, b, c;
+      stats_pass(sv, n, S, 0, 0.0, 0, a, b, c);
+    }
+    bool need = true;
+    for (uint32_t q = 0; q < n; ++q) {
+      if (!((op.mask >> q) & 1)) continue;
+      const uint32_t rem = op.mask & ~((1u << q) - 1);
+      double t, zsum, j;
+      stats_pass(sv, n, S, rem, g, q, t, zsum, j);
+      const double p1 = need ? (t - zsum > 0 ? j / (t - zsum) : 1.0) : (t > 0 ? j / t : 0.0);
+      const double v = philox_uniform(seed, traj, ev++);
+      const bool jump = v < p1;
+      damp_apply(sv, n, q, g, jump);
+      if (jump) need = false;
+    }
     double t, a, b;
-    stats_pass(sv, n, S, 0, 0.0, 0, t, a, b);  // materialise the pending diagonal
+    stats_pass(sv, n, S, 0, 0.0, 0, t, a, b);
+    set_pending(S, 0, 0.0, t > 0 ? 1.0 / sqrt(t) : 1.0);
   }
-  const uint32_t N = 1u << n;
-  const uint32_t c = n > kTLogThreads ? n - kTLogThreads : 0;  // bits inside a thread's chunk
-  const uint32_t chunk = 1u << c;
-  const bool active = (threadIdx.x << c) < N;
-  const uint32_t base = threadIdx.x << c;
-  double my = 0;
-  if (active)
-    for (uint32_t i = 0; i < chunk; ++i) {
-      const float2 v = sv[base + i];
-      my += (double)v.x * v.x + (double)v.y * v.y;
+
+  // End of a trajectory: <Z_q> for every qubit and one sampled bitstring.
+  static __device__ __noinline__ void finish(float2 *sv, uint32_t n, Shared &S, double *csum, uint64_t seed,
+                                      uint32_t traj, double *out_z, uint32_t *out_sample) {
+    {
+      double t, a, b;
+      stats_pass(sv, n, S, 0, 0.0, 0, t, a, b);  // materialise the pending diagonal
     }
-  csum[threadIdx.x] = my;
-  __syncthreads();
-  // qubits inside a chunk, three per block reduction
-  for (uint32_t q0 = 0; q0 < c; q0 += 3) {
-    double acc[3] = {0, 0, 0};
+    const uint32_t N = 1u << n;
+    const uint32_t c = n > kTLogThreads ? n - kTLogThreads : 0;  // bits inside a thread's chunk
+    const uint32_t chunk = 1u << c;
+    const bool active = (threadIdx.x << c) < N;
+    const uint32_t base = threadIdx.x << c;
+    double my = 0;
     if (active)
       for (uint32_t i = 0; i < chunk; ++i) {
         const float2 v = sv[base + i];
+        my += (double)v.x * v.x + (double)v.y * v.y;
+      }
+    csum[threadIdx.x] = my;
+    __syncthreads();
+    // qubits inside a chunk, three per block reduction
+    for (uint32_t q0 = 0; q0 < c; q0 += 3) {
+      double acc[3] = {0, 0, 0};
+      if (active)
+        for (uint32_t i = 0; i < chunk; ++i) {
+          const float2 v = sv[base + i];
+          const double p = (double)v.x * v.x + (double)v.y * v.y;
+          for (uint32_t j = 0; j < 3; ++j)
+            if (q0 + j < c && ((i >> (q0 + j)) & 1)) acc[j] += p;
+        }
+      block_sum3(S, acc[0], acc[1], acc[2]);
+      if (threadIdx.x < 3 && q0 + threadIdx.x < c) out_z[(size_t)traj * n + q0 + threadIdx.x] = acc[threadIdx.x];
+    }
+    // qubits that index the threads: thread j sums the chunk sums with bit j set
+    const uint32_t nthr = N >> c;
+    if (threadIdx.x < n - c) {
+      double x = 0;
+      for (uint32_t tt = 0; tt < nthr; ++tt)
+        if ((tt >> threadIdx.x) & 1) x += csum[tt];
+      out_z[(size_t)traj * n + c + threadIdx.x] = x;
+    }
+    if (threadIdx.x == 0) {
+      double tot = 0;
+      for (uint32_t tt = 0; tt < nthr; ++tt) tot += csum[tt];
+      S.vals[3] = tot;
+      // inverse-CDF sample: find the chunk, then the amplitude (a target that
+      // rounding leaves past the end takes the last one of nonzero weight)
+      const double target = philox_uniform(seed, traj, 0xFFFFFFF0u) * tot;
+      double acc = 0, acc_t = 0;
+      uint32_t tsel = nthr;
+      for (uint32_t tt = 0; tt < nthr; ++tt) {
+        if (csum[tt] > 0) {
+          tsel = tt;
+          acc_t = acc;
+        }
+        if (acc + csum[tt] > target) break;
+        acc += csum[tt];
+      }
+      acc = acc_t;
+      if (tsel == nthr) tsel = 0;  // an all-zero state (cannot arise from normalised branches)
+      uint32_t isel = tsel << c;
+      for (uint32_t i = 0; i < chunk; ++i) {
+        const float2 v = sv[(tsel << c) + i];
         const double p = (double)v.x * v.x + (double)v.y * v.y;
-        for (uint32_t j = 0; j < 3; ++j)
-          if (q0 + j < c && ((i >> (q0 + j)) & 1)) acc[j] += p;
+        if (p > 0) isel = (tsel << c) + i;
+        acc += p;
+        if (acc > target) break;
       }
-    block_sum3(S, acc[0], acc[1], acc[2]);
-    if (threadIdx.x < 3 && q0 + threadIdx.x < c) out_z[(size_t)traj * n + q0 + threadIdx.x] = acc[threadIdx.x];
-  }
-  // qubits that index the threads: thread j sums the chunk sums with bit j set
-  const uint32_t nthr = N >> c;
-  if (threadIdx.x < n - c) {
-    double x = 0;
-    for (uint32_t tt = 0; tt < nthr; ++tt)
-      if ((tt >> threadIdx.x) & 1) x += csum[tt];
-    out_z[(size_t)traj * n + c + threadIdx.x] = x;
-  }
-  if (threadIdx.x == 0) {
-    double tot = 0;
-    for (uint32_t tt = 0; tt < nthr; ++tt) tot += csum[tt];
-    S.vals[3] = tot;
-    // inverse-CDF sample: find the chunk, then the amplitude
-    const double target = philox_uniform(seed, traj, 0xFFFFFFF0u) * tot;
-    double acc = 0;
-    uint32_t tsel = nthr - 1;
-    for (uint32_t tt = 0; tt < nthr; ++tt) {
-      if (acc + csum[tt] > target) {
-        tsel = tt;
-        break;
-      }
-      acc += csum[tt];
+      if (out_sample) out_sample[traj] = isel;
     }
-    uint32_t isel = (tsel << c) + chunk - 1;
-    for (uint32_t i = 0; i < chunk; ++i) {
-      const float2 v = sv[(tsel << c) + i];
-      acc += (double)v.x * v.x + (double)v.y * v.y;
-      if (acc > target) {
-        isel = (tsel << c) + i;
-        break;
-      }
+    __syncthreads();
+    const double tot = S.vals[3];
+    if (threadIdx.x < n) {
+      const double p1 = out_z[(size_t)traj * n + threadIdx.x];
+      out_z[(size_t)traj * n + threadIdx.x] = tot > 0 ? 1.0 - 2.0 * p1 / tot : 0.0;
     }
-    if (out_sample) out_sample[traj] = isel;
+    __syncthreads();
   }
-  __syncthreads();
-  const double tot = S.vals[3];
-  if (threadIdx.x < n) {
-    const double p1 = out_z[(size_t)traj * n + threadIdx.x];
-    out_z[(size_t)traj * n + threadIdx.x] = tot > 0 ? 1.0 - 2.0 * p1 / tot : 0.0;
-  }
-  __syncthreads();
-}
+};
 
-__global__ void __launch_bounds__(kTThreads, 1)
+template <int NT>
+__global__ void __launch_bounds__(NT, 1)
     k_trajectories(const TOp *__restrict__ ops, uint32_t n_ops, const float2 *__restrict__ pool,
                    float2 *__restrict__ ws, uint32_t n, const TRun *__restrict__ run,
                    double *__restrict__ out_z, uint32_t *__restrict__ out_sample) {
   __shared__ Shared S;
-  __shared__ float2 Msm[1 << (2 * kTrajMaxGate)];
-  __shared__ double csum[kTThreads];
+  __shared__ float4 Msm[1 << (2 * kTrajMaxGate)];  // gate entries (re, re, im, im)
+  __shared__ double csum[NT];
+  using Tr = Traj<NT>;
   const uint32_t n_traj = run->n_traj;
   const uint64_t seed = run->seed;
   const uint32_t N = 1u << n;
   float2 *sv = ws + ((size_t)blockIdx.x << n);
   for (uint32_t traj = blockIdx.x; traj < n_traj; traj += gridDim.x) {
-    for (uint32_t i = threadIdx.x; i < N; i += kTThreads)
+    for (uint32_t i = threadIdx.x; i < N; i += NT)
       sv[i] = make_float2(i == 0 ? 1.f : 0.f, 0.f);
     if (threadIdx.x == 0) S.pend = 0;
     __syncthreads();
@@ -516,14 +580,14 @@ __global__ void __launch_bounds__(kTThreads, 1)
     for (uint32_t oi = 0; oi < n_ops; ++oi) {
       const TOp op = ops[oi];
       if (op.type == T_GATE) {
-        if (op.stats) fill_stab(S, (double)op.sgamma);
-        stage_matrix(Msm, pool, op.mat, 1u << (2 * op.k));
+        if (op.stats) Tr::fill_stab(S, (double)op.sgamma);
+        Tr::stage_gate(Msm, pool, op.mat, 1u << (2 * op.k));
         double t = 0, d = 0, z = 0;
-        dispatch_gate(sv, n, op, Msm, S, t, d);
+        Tr::dispatch_gate(sv, n, op, Msm, S, t, d);
         __syncthreads();
         if (threadIdx.x == 0) S.pend = 0;
         if (op.stats) {
-          block_sum3(S, t, d, z);
+          Tr::block_sum3(S, t, d, z);
           T = t;
           Dd = d;
         } else {
@@ -540,7 +604,7 @@ __global__ void __launch_bounds__(kTThreads, 1)
               const TOp eo = ops[oi + 1 + e];
               const double u = philox_uniform(seed, traj, ev + e);
               if (u < (double)eo.prob) {
-                err_apply(sv, n, eo, u, pool, Msm, S);
+                Tr::err_apply(sv, n, eo, u, pool, Msm, S);
                 stats_valid = false;
               }
             }
@@ -551,18 +615,18 @@ __global__ void __launch_bounds__(kTThreads, 1)
       } else if (op.type == T_ERR) {  // not preceded by a gate block (kept for completeness)
         const double u = philox_uniform(seed, traj, ev++);
         if (u < (double)op.prob) {
-          err_apply(sv, n, op, u, pool, Msm, S);
+          Tr::err_apply(sv, n, op, u, pool, Msm, S);
           stats_valid = false;
         }
       } else if (op.type == T_DAMP) {
-        damp_op(sv, n, op, S, seed, traj, ev, T, Dd, stats_valid);
+        Tr::damp_op(sv, n, op, S, seed, traj, ev, T, Dd, stats_valid);
         stats_valid = false;
       } else if (op.type == T_CHAN) {
-        chan_op(sv, n, op, pool, Msm, S, seed, traj, ev);
+        Tr::chan_op(sv, n, op, pool, reinterpret_cast<float2 *>(Msm), S, seed, traj, ev);
         stats_valid = false;
       }
     }
-    finish(sv, n, S, csum, seed, traj, out_z, out_sample);
+    Tr::finish(sv, n, S, csum, seed, traj, out_z, out_sample);
   }
 }
 
@@ -603,12 +667,35 @@ bool l2_window(void *base, size_t bytes, cudaAccessPolicyWindow &w) {
   return true;
 }
 
-cudaError_t launch_trajectories(unsigned grid, cudaStream_t s, const cudaAccessPolicyWindow *w,
-                                const TOp *ops, uint32_t n_ops, const float2 *pool, float2 *ws,
-                                uint32_t n, const TRun *run, double *z, uint32_t *sample) {
+// Threads per CTA when the program does not fix them: 1024 for states of 15 to
+// 17 qubits (slices larger than L1 but held in L2, so passes are bound by loads
+// in flight), 512 otherwise (issue-bound gate arithmetic).
+unsigned auto_threads(uint32_t n) { return n >= 15 && n <= 17 ? 1024u : 512u; }
+
+// Trajectories in flight when the program does not fix them: one per SM, unless
+// the slices of one per SM overflow L2 while those of at least half as many
+// still fit in 89% of it (17 qubits: 112 CTAs x 1 MB instead of 148, 1.8x the
+// throughput); beyond that the passes stream from HBM either way.
+unsigned auto_ctas(uint32_t n) {
+  const unsigned sms = (unsigned)cb2::sm_count();
+  int dev = 0, l2 = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess || l2 <= 0) {
+    cudaGetLastError();
+    return sms;
+  }
+  const uint64_t slice = sizeof(float2) << n;
+  const uint64_t fit = (uint64_t)l2 * 89 / 100 / slice;
+  return fit >= sms || fit < sms / 2 ? sms : (unsigned)fit;
+}
+
+cudaError_t launch_trajectories(unsigned grid, unsigned threads, cudaStream_t s,
+                                const cudaAccessPolicyWindow *w, const TOp *ops, uint32_t n_ops,
+                                const float2 *pool, float2 *ws, uint32_t n, const TRun *run,
+                                double *z, uint32_t *sample) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(kTThreads);
+  cfg.blockDim = dim3(threads);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
@@ -618,7 +705,9 @@ cudaError_t launch_trajectories(unsigned grid, cudaStream_t s, const cudaAccessP
     cfg.attrs = attr;
     cfg.numAttrs = 1;
   }
-  return cudaLaunchKernelEx(&cfg, k_trajectories, ops, n_ops, pool, ws, n, run, z, sample);
+  if (threads == 1024)
+    return cudaLaunchKernelEx(&cfg, k_trajectories<1024>, ops, n_ops, pool, ws, n, run, z, sample);
+  return cudaLaunchKernelEx(&cfg, k_trajectories<512>, ops, n_ops, pool, ws, n, run, z, sample);
 }
 
 struct TrajProgram {
@@ -638,6 +727,9 @@ struct TrajProgram {
   cudaGraphExec_t graph = nullptr;
   void *graph_stream = nullptr;
   unsigned graph_grid = 0;
+  unsigned threads = 0;  // threads per CTA: 512, 1024, or 0 for auto_threads(n)
+  unsigned max_ctas = 0; // CTAs (trajectories in flight), or 0 for auto_ctas(n)
+  unsigned graph_threads = 0;
   std::mutex mu;
 
   ~TrajProgram() {
@@ -661,7 +753,7 @@ struct TrajProgram {
     for (size_t i = 0; i < ops.size(); ++i) {
       if (ops[i].type != T_GATE) continue;
       uint32_t e = 0;
-      while (i + 1 + e < ops.size() && ops[i + 1 + e].type == T_ERR && e < (uint32_t)kTThreads) ++e;
+      while (i + 1 + e < ops.size() && ops[i + 1 + e].type == T_ERR && e < (uint32_t)kTMinThreads) ++e;
       ops[i].nerr = e;
     }
     for (size_t i = 0; i < ops.size(); ++i) {
@@ -840,6 +932,20 @@ int cast_b200_traj_add_channel(void *prog, uint32_t qubit, const cast_complex64_
   return 0;
 }
 
+int cast_b200_traj_set_launch(void *prog, uint32_t threads, uint32_t max_ctas, char *err_buf,
+                              size_t err_buf_len) {
+  TrajProgram *p = as_traj(prog);
+  if (!p || (threads != 0 && threads != 512 && threads != 1024)) {
+    cb2::write_err(err_buf, err_buf_len, "threads per CTA must be 512, 1024 or 0 (by state size)");
+    return 1;
+  }
+  std::lock_guard<std::mutex> lock(p->mu);
+  p->threads = threads;
+  p->max_ctas = max_ctas;
+  cb2::clear_err(err_buf, err_buf_len);
+  return 0;
+}
+
 uint32_t cast_b200_traj_num_ops(const void *prog) {
   const TrajProgram *p = static_cast<const TrajProgram *>(prog);
   return p && p->magic == kTrajMagic ? (uint32_t)p->ops.size() : 0;
@@ -861,7 +967,9 @@ int cast_b200_traj_run(void *prog, uint32_t n_traj, uint64_t seed, double *out_z
       cb2::write_err(err_buf, err_buf_len, err);
       return 1;
     }
-    const unsigned grid = (unsigned)std::min<uint64_t>(n_traj, (uint64_t)cb2::sm_count());
+    const unsigned ctas = p->max_ctas ? p->max_ctas : auto_ctas(p->n);
+    const unsigned grid = (unsigned)std::min<uint64_t>(n_traj, ctas);
+    const unsigned threads = p->threads ? p->threads : auto_threads(p->n);
     if (p->ws_ctas < grid) {
       cudaFree(p->d_ws);
       p->d_ws = nullptr;
@@ -907,7 +1015,7 @@ int cast_b200_traj_run(void *prog, uint32_t n_traj, uint64_t seed, double *out_z
     cudaAccessPolicyWindow win = {};
     const bool win_ok = l2_window(p->d_ws, (sizeof(float2) << p->n) * grid, win);
     if (use_graph && s) {
-      if (p->graph && (p->graph_stream != stream || p->graph_grid != grid)) {
+      if (p->graph && (p->graph_stream != stream || p->graph_grid != grid || p->graph_threads != threads)) {
         cudaGraphExecDestroy(p->graph);
         p->graph = nullptr;
       }
@@ -918,7 +1026,7 @@ int cast_b200_traj_run(void *prog, uint32_t n_traj, uint64_t seed, double *out_z
           cb2::write_err(err_buf, err_buf_len, err);
           return 1;
         }
-        const cudaError_t lrc = launch_trajectories(grid, s, win_ok ? &win : nullptr, p->d_ops, n_ops,
+        const cudaError_t lrc = launch_trajectories(grid, threads, s, win_ok ? &win : nullptr, p->d_ops, n_ops,
                                                     p->d_pool, p->d_ws, p->n, p->d_run, p->d_z,
                                                     p->d_sample);
         const cudaError_t erc = cudaStreamEndCapture(s, &gph);
@@ -932,13 +1040,14 @@ int cast_b200_traj_run(void *prog, uint32_t n_traj, uint64_t seed, double *out_z
         cudaGraphDestroy(gph);
         p->graph_stream = stream;
         p->graph_grid = grid;
+        p->graph_threads = threads;
       }
       if (!cuda_ok(cudaGraphLaunch(p->graph, s), "cudaGraphLaunch", err)) {
         cb2::write_err(err_buf, err_buf_len, err);
         return 1;
       }
     } else {
-      if (!cuda_ok(launch_trajectories(grid, s, win_ok ? &win : nullptr, p->d_ops, n_ops, p->d_pool,
+      if (!cuda_ok(launch_trajectories(grid, threads, s, win_ok ? &win : nullptr, p->d_ops, n_ops, p->d_pool,
                                        p->d_ws, p->n, p->d_run, p->d_z, p->d_sample),
                    "trajectory kernel launch", err)) {
         cb2::write_err(err_buf, err_buf_len, err);

@@ -224,6 +224,14 @@ class TrajectoryProgram:
     def __len__(self):
         return int(L.lib().cast_b200_traj_num_ops(self.handle))
 
+    def set_launch(self, threads: int = 0, max_ctas: int = 0) -> None:
+        """Launch shape of the trajectory kernel: threads per CTA (512 or 1024)
+        and the number of CTAs, i.e. trajectories in flight; 0 chooses by the
+        number of qubits."""
+        eb = L.errbuf()
+        L.check(L.lib().cast_b200_traj_set_launch(self.handle, int(threads), int(max_ctas), eb,
+                                                  L.ERR_LEN), eb, "traj_set_launch")
+
     def run(self, n_traj: int, seed: int, stream=None, use_graph: bool = True):
         """(z, samples): <Z_q> per trajectory (n_traj x n) and one bitstring each."""
         z = np.zeros((n_traj, self.n))

@@ -171,6 +171,12 @@ int cast_b200_traj_add_damping(void *program, uint32_t qubit_mask, double gamma,
 int cast_b200_traj_add_channel(void *program, uint32_t qubit, const cast_complex64_t *kraus,
                                uint32_t n_kraus, char *err_buf, size_t err_buf_len);
 uint32_t cast_b200_traj_num_ops(const void *program);
+/* Launch shape of the trajectory kernel, a tuning knob with no counterpart in
+ * the reference.  threads: threads per CTA, 512 or 1024, or 0 (the default) to
+ * choose by state size.  max_ctas: CTAs, i.e. trajectories in flight (each owns
+ * a 2^n-amplitude slice of the workspace), or 0 (the default) for one per SM. */
+int cast_b200_traj_set_launch(void *program, uint32_t threads, uint32_t max_ctas, char *err_buf,
+                              size_t err_buf_len);
 int cast_b200_traj_run(void *program, uint32_t n_traj, uint64_t seed, double *out_z,
                        uint32_t *out_samples, void *stream, int use_graph, char *err_buf,
                        size_t err_buf_len);

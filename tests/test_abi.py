@@ -89,3 +89,23 @@ def test_bad_descriptor_rejected(cblib):
     assert b"not a cast_b200 gate module" in eb.value
     assert cblib.cast_cuda_kernel_launch(None, None, 0, 1, 4, eb, L.ERR_LEN) == 1
     assert b"must not be null" in eb.value
+
+
+def test_trajectory_threads_setting(cblib):
+    """Trajectory programs are built on the host; the launch-shape knob accepts
+    512, 1024 and 0 (by state size) threads and any CTA count."""
+    from cast_simulator_b200 import _lib as L
+
+    eb = L.errbuf()
+    prog = cblib.cast_b200_traj_create(12, eb, L.ERR_LEN)
+    assert prog
+    try:
+        for t in (0, 512, 1024):
+            assert cblib.cast_b200_traj_set_launch(prog, t, 0, eb, L.ERR_LEN) == 0
+        assert cblib.cast_b200_traj_set_launch(prog, 512, 100, eb, L.ERR_LEN) == 0
+        for t in (256, 384, 2048):
+            assert cblib.cast_b200_traj_set_launch(prog, t, 0, eb, L.ERR_LEN) == 1
+            assert b"512, 1024 or 0" in eb.value
+        assert cblib.cast_b200_traj_set_launch(None, 512, 0, eb, L.ERR_LEN) == 1
+    finally:
+        cblib.cast_b200_traj_destroy(prog)

@@ -26,3 +26,14 @@ def test_profile_and_choice(cblib):
     ch = A.choose_fusion(22, gates, "f32", tab, ks=range(2, 7))
     assert 2 <= ch.fusion_k <= 6
     assert ch.predicted_s <= min(c["predicted_s"] for c in ch.candidates) + 1e-15
+
+
+def test_trajectory_tuning_picks_the_fastest_shape(cblib):
+    from cast_simulator_b200 import autotune as A
+    from cast_simulator_b200.types import QuantumCircuit
+
+    circ = QuantumCircuit.brickwork(12, 6, 3, depolarizing=1e-3, damping=5e-4)
+    ch = A.tune_trajectories(circ, n_traj=512, ks=(2, 3), threads=(512, 1024), ctas=(0, 64))
+    assert len(ch.candidates) == 8
+    assert ch.traj_per_s == max(c["traj_per_s"] for c in ch.candidates) > 0
+    assert ch.fusion_k in (2, 3) and ch.threads in (512, 1024) and ch.max_ctas in (0, 64)

@@ -148,3 +148,72 @@ def test_graph_replay_is_deterministic(mods):
     c, _ = prog.run(300, 12, st)
     assert np.array_equal(a, b) and np.array_equal(sa, sb)
     assert not np.array_equal(a, c)
+
+
+# State sizes from well inside L2 (12 qubits: 32 KB a trajectory) to beyond it
+# (18 qubits: 2 MB a trajectory, 296 MB for 148 at once), with gates on the
+# lowest and highest qubits; both CTA sizes of the kernel.
+LAYOUT_NS = [12, 14, 15, 16, 17, 18]
+
+
+@pytest.mark.parametrize("threads", [512, 1024])
+@pytest.mark.parametrize("n", LAYOUT_NS)
+def test_layouts_noise_free_equal_statevector(mods, oracle, n, threads):
+    T, TR, S = mods
+    circ = T.QuantumCircuit.brickwork(n, 6, 40 + n)
+    sv = oracle.simulate(n, [(g.matrix(), g.qubits()) for g in circ.gates()])
+    z_ref = z_from_pops(np.abs(sv) ** 2, n)
+    n_traj = 2048
+    prog = TR.TrajectoryProgram(circ, 4)
+    prog.set_launch(threads)
+    z, smp = prog.run(n_traj, 21, S.Stream())
+    assert np.max(np.abs(z - z_ref[None, :])) < 2e-5
+    assert smp.max() < (1 << n)
+    # sampled bitstrings: P(bit q = 1) = (1 - <Z_q>) / 2
+    bits = (smp[:, None].astype(np.int64) >> np.arange(n)[None, :]) & 1
+    p1 = (1 - z_ref) / 2
+    se = np.sqrt(np.maximum(p1 * (1 - p1), 1e-4) / n_traj)
+    assert np.all(np.abs(bits.mean(axis=0) - p1) < 5 * se + 1e-3)
+
+
+def _spread(circ, T, n, active):
+    """The circuit's gates on qubits active[0] < active[1] < ... of an n-qubit
+    register (an order-preserving relabelling keeps every matrix as it is)."""
+    out = T.QuantumCircuit(n)
+    for g in circ.gates():
+        out.add(T.QuantumGate(g.matrix(), [active[q] for q in g.qubits()], g.noise_model()))
+    return out
+
+
+@pytest.mark.parametrize("n", LAYOUT_NS)
+def test_layouts_noisy_embedded_match_dm(mods, oracle, n):
+    """A noisy 6-qubit brickwork (depolarizing, damping, an unequal Pauli
+    channel) placed on low, boundary and top qubits of an n-qubit register:
+    the active qubits follow the 6-qubit DM oracle, idle qubits stay in |0>."""
+    T, TR, S = mods
+    small = T.QuantumCircuit.brickwork(6, 4, 77, depolarizing=0.03, damping=0.06)
+    small.add(T.QuantumGate.pauli_channel(5, 0.1, 0.05, 0.2))
+    small.add(T.QuantumGate.u3(0.7, 0.1, 0.3, 5))
+    z_ref = dm_reference(oracle, small)
+    active = [0, n // 3, n - 4, n - 3, n - 2, n - 1]
+    prog = TR.TrajectoryProgram(_spread(small, T, n, active), 3)
+    assert prog.stats.n_channels == 1
+    n_traj = 8192
+    z, smp = prog.run(n_traj, 1234 + n, S.Stream())
+    mean = z.mean(axis=0)
+    se = z.std(axis=0, ddof=1) / math.sqrt(n_traj)
+    assert np.all(np.abs(mean[active] - z_ref) < 5 * se[active] + 2e-3), (mean[active], z_ref)
+    idle = [q for q in range(n) if q not in active]
+    assert np.max(np.abs(z[:, idle] - 1.0)) < 1e-5
+    assert np.all((smp.astype(np.int64) >> np.array(idle)[:, None] & 1) == 0)
+
+
+@pytest.mark.parametrize("n", [14, 16])
+def test_replay_is_deterministic_both_cta_sizes(mods, n):
+    T, TR, S = mods
+    circ = T.QuantumCircuit.brickwork(n, 3, 5, depolarizing=0.02, damping=0.02)
+    prog = TR.TrajectoryProgram(circ, 3)
+    st = S.Stream()
+    a, sa = prog.run(600, 11, st)
+    b, sb = prog.run(600, 11, st)
+    assert np.array_equal(a, b) and np.array_equal(sa, sb)
