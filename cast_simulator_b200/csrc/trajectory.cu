@@ -94,17 +94,6 @@ struct Shared {
   int pend;
 };
 
-// Two FP32 fused multiply-adds in one instruction (PTX fma.rn.f32x2, sm_100a):
-// (a.x * b.x + c.x, a.y * b.y + c.y), each rounded once as fmaf.
-__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
-  uint64_t d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;"
-      : "=l"(d)
-      : "l"(*reinterpret_cast<const uint64_t *>(&a)), "l"(*reinterpret_cast<const uint64_t *>(&b)),
-        "l"(*reinterpret_cast<const uint64_t *>(&c)));
-  return *reinterpret_cast<const float2 *>(&d);
-}
-
 __device__ __forceinline__ float2 cmul_add(float2 m, float2 x, float2 acc) {
   acc.x = fmaf(m.x, x.x, acc.x);
   acc.x = fmaf(-m.y, x.y, acc.x);
@@ -114,15 +103,14 @@ __device__ __forceinline__ float2 cmul_add(float2 m, float2 x, float2 acc) {
 }
 
 // The device side of one trajectory, for CTAs of NT threads.  512-thread CTAs
-// get 128 registers a thread and use packed FMAs for the gates (the passes of
-// small and HBM-sized states are bound by instruction issue); 1024-thread CTAs
-// keep twice the loads in flight, which is what the L2-resident states of 15 to
-// 17 qubits need.
+// get 128 registers a thread, so the fused gates run without spills (the passes
+// of small and HBM-sized states are bound by instruction issue); 1024-thread
+// CTAs keep twice the loads in flight, which is what the L2-resident states of
+// 15 to 17 qubits need.
 template <int NT>
 struct Traj {
   static constexpr int kTThreads = NT;
   static constexpr uint32_t kTLogThreads = NT == 1024 ? 10 : 9;
-  static constexpr bool kPacked = NT == 512;
 
   // Block sum of up to three doubles; every thread gets the results.
   static __device__ void block_sum3(Shared &S, double &a, double &b, double &c) {
@@ -183,16 +171,12 @@ struct Traj {
   // its outputs, t += |o|^2 and d += |o|^2 (1-g)^popc(i & smask) for the damping op
   // that follows.
   //
-  // Packed: M holds each entry as (re, re, im, im); one 16-byte shared load and
-  // two packed FMAs give a += re * x and b += im * x for a complex amplitude x,
-  // and the output is (a.x - b.y, a.y + b.x).  Otherwise M holds complex
-  // entries and each product is four FMAs.  k = 1 gates take two groups a
-  // thread, so every matrix load serves both.
+  // k = 1 gates take two groups a thread, so every matrix load serves both.
   template <int K>
   static constexpr int groups_per_thread() { return K == 1 ? 2 : 1; }
 
   template <int K, bool PEND>
-  static __device__ __noinline__ void gate_pass(float2 *sv, uint32_t n, const TOp &op, const float4 *M,
+  static __device__ __noinline__ void gate_pass(float2 *sv, uint32_t n, const TOp &op, const float2 *M,
                                          const Shared &S, double &t, double &d) {
     constexpr int D = 1 << K;
     constexpr int U = groups_per_thread<K>();
@@ -233,30 +217,13 @@ struct Traj {
 #pragma unroll
       for (int r = 0; r < D; ++r) {
         float2 acc[U];
-        if constexpr (kPacked) {
-          float2 ar[U], ai[U];
 #pragma unroll
-          for (int u = 0; u < U; ++u) ar[u] = ai[u] = make_float2(0.f, 0.f);
+        for (int u = 0; u < U; ++u) acc[u] = make_float2(0.f, 0.f);
 #pragma unroll
-          for (int c = 0; c < D; ++c) {
-            const float4 m = M[r * D + c];
+        for (int c = 0; c < D; ++c) {
+          const float2 m = M[r * D + c];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-              ar[u] = ffma2(make_float2(m.x, m.y), x[u][c], ar[u]);
-              ai[u] = ffma2(make_float2(m.z, m.w), x[u][c], ai[u]);
-            }
-          }
-#pragma unroll
-          for (int u = 0; u < U; ++u) acc[u] = make_float2(ar[u].x - ai[u].y, ar[u].y + ai[u].x);
-        } else {
-#pragma unroll
-          for (int u = 0; u < U; ++u) acc[u] = make_float2(0.f, 0.f);
-#pragma unroll
-          for (int c = 0; c < D; ++c) {
-            const float2 m = reinterpret_cast<const float2 *>(M)[r * D + c];
-#pragma unroll
-            for (int u = 0; u < U; ++u) acc[u] = cmul_add(m, x[u][c], acc[u]);
-          }
+          for (int u = 0; u < U; ++u) acc[u] = cmul_add(m, x[u][c], acc[u]);
         }
         uint32_t roff = 0;
 #pragma unroll
@@ -280,7 +247,7 @@ struct Traj {
     d += ld;
   }
 
-  static __device__ void dispatch_gate(float2 *sv, uint32_t n, const TOp &op, const float4 *M, Shared &S,
+  static __device__ void dispatch_gate(float2 *sv, uint32_t n, const TOp &op, const float2 *M, Shared &S,
                                 double &t, double &d) {
     if (S.pend) {
       switch (op.k) {
@@ -302,17 +269,6 @@ struct Traj {
   // Stage a 2^k x 2^k matrix into shared memory.
   static __device__ void stage_matrix(float2 *Msm, const float2 *pool, uint32_t off, uint32_t entries) {
     for (uint32_t i = threadIdx.x; i < entries; i += kTThreads) Msm[i] = pool[off + i];
-    __syncthreads();
-  }
-
-  // Stage a 2^k x 2^k gate matrix into shared memory: (re, re, im, im) entries
-  // for the packed arithmetic, plain complex entries otherwise.
-  static __device__ void stage_gate(float4 *Msm, const float2 *pool, uint32_t off, uint32_t entries) {
-    for (uint32_t i = threadIdx.x; i < entries; i += kTThreads) {
-      const float2 m = pool[off + i];
-      if constexpr (kPacked) Msm[i] = make_float4(m.x, m.x, m.y, m.y);
-      else reinterpret_cast<float2 *>(Msm)[i] = m;
-    }
     __syncthreads();
   }
 
@@ -427,10 +383,10 @@ struct Traj {
 
   // Applies a Pauli error op (one of three k-qubit matrices) as a gate pass.
   static __device__ __noinline__ void err_apply(float2 *sv, uint32_t n, const TOp &op, double u,
-                                         const float2 *pool, float4 *Msm, Shared &S) {
+                                         const float2 *pool, float2 *Msm, Shared &S) {
     const uint32_t which = min(2u, (uint32_t)(u / (double)op.prob * 3.0));
     const uint32_t e = 1u << (2 * op.k);
-    stage_gate(Msm, pool, op.mat + which * e, e);
+    stage_matrix(Msm, pool, op.mat + which * e, e);
     TOp g = op;
     g.stats = 0;
     double t = 0, d = 0;
@@ -562,7 +518,7 @@ __global__ void __launch_bounds__(NT, 1)
                    float2 *__restrict__ ws, uint32_t n, const TRun *__restrict__ run,
                    double *__restrict__ out_z, uint32_t *__restrict__ out_sample) {
   __shared__ Shared S;
-  __shared__ float4 Msm[1 << (2 * kTrajMaxGate)];  // gate entries (re, re, im, im)
+  __shared__ float2 Msm[1 << (2 * kTrajMaxGate)];
   __shared__ double csum[NT];
   using Tr = Traj<NT>;
   const uint32_t n_traj = run->n_traj;
@@ -581,7 +537,7 @@ __global__ void __launch_bounds__(NT, 1)
       const TOp op = ops[oi];
       if (op.type == T_GATE) {
         if (op.stats) Tr::fill_stab(S, (double)op.sgamma);
-        Tr::stage_gate(Msm, pool, op.mat, 1u << (2 * op.k));
+        Tr::stage_matrix(Msm, pool, op.mat, 1u << (2 * op.k));
         double t = 0, d = 0, z = 0;
         Tr::dispatch_gate(sv, n, op, Msm, S, t, d);
         __syncthreads();
@@ -622,7 +578,7 @@ __global__ void __launch_bounds__(NT, 1)
         Tr::damp_op(sv, n, op, S, seed, traj, ev, T, Dd, stats_valid);
         stats_valid = false;
       } else if (op.type == T_CHAN) {
-        Tr::chan_op(sv, n, op, pool, reinterpret_cast<float2 *>(Msm), S, seed, traj, ev);
+        Tr::chan_op(sv, n, op, pool, Msm, S, seed, traj, ev);
         stats_valid = false;
       }
     }
