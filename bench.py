@@ -371,6 +371,37 @@ def serving_leg(n_req: int):
     return out
 
 
+def fusion_sweep_leg(n: int, depth: int):
+    """The brickwork with fusion width k = 2..7 on the CUDA-core path in complex128
+    and complex64, and on the split-BF16 tensor cores for k = 5, 6 (complex64):
+    device time per circuit (median of 2 after a warm-up), fused passes, and the
+    HBM rate those passes imply."""
+    from cast_simulator_b200 import cuda as cu
+    from cast_simulator_b200.fusion import FusionConfig, optimize_native
+    from cast_simulator_b200.types import QuantumCircuit
+
+    circ = QuantumCircuit.brickwork(n, depth, 2024)
+    out = {"workload": f"brickwork-{n}q-d{depth}", "runs": []}
+    cases = [(cu.CudaPrecision.F64, "c128", False, k) for k in range(2, 8)]
+    cases += [(cu.CudaPrecision.F32, "c64", False, k) for k in range(2, 8)]
+    cases += [(cu.CudaPrecision.F32, "c64", True, k) for k in (5, 6)]
+    fused = {k: optimize_native(n, circ.gates(), FusionConfig.size_only(k)).gates() for k in range(2, 8)}
+    for prec, label, split, k in cases:
+        gates = fused[k]
+        t, sv = _run_fused(n, gates, prec, split, reps=3)
+        b_amp = 16 if label == "c128" else 8
+        out["runs"].append({"precision": label, "tensor_cores": split, "fusion_k": k,
+                            "fused_gates": len(gates), "ms_per_circuit": t * 1e3,
+                            "hbm_gbs": len(gates) * 2 * (1 << n) * b_amp / t / 1e9})
+        del sv
+    for label in ("c128", "c64"):
+        best = min((r for r in out["runs"] if r["precision"] == label),
+                   key=lambda r: r["ms_per_circuit"])
+        out[f"best_{label}"] = {"fusion_k": best["fusion_k"], "tensor_cores": best["tensor_cores"],
+                                "ms_per_circuit": best["ms_per_circuit"]}
+    return out
+
+
 def tensor_leg(n: int, depth: int):
     """Tensor-core fused path (complex64, split BF16, k = 5 and 6) vs the plain
     CUDA-core path at its best width (k = 4): time per circuit on the full
@@ -463,6 +494,8 @@ def main(argv=None):
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip trajectory and serving legs")
+    ap.add_argument("--sweep", action="store_true",
+                    help="add the fusion-width sweep k = 2..7 (complex128, complex64, tensor cores)")
     ap.add_argument("--serve-requests", type=int, default=60)
     ap.add_argument("--largest", action="store_true",
                     help="add the 34q complex64 / 33q complex128 largest-fit leg (minutes)")
@@ -615,6 +648,8 @@ def main(argv=None):
         line["tensor_path"] = tensor_leg(n, args.depth)
         line["trajectories"] = trajectory_leg()
         line["serving"] = serving_leg(args.serve_requests)
+    if rank == 0 and ws == 1 and args.sweep:
+        line["fusion_sweep"] = fusion_sweep_leg(n, args.depth)
     if rank == 0 and ws == 1 and args.largest:
         line["largest_fit"] = largest_leg()
     if rank == 0:

@@ -17,10 +17,11 @@
 //    each of the 2^k 128-bit (f64) / 64-bit (f32) loads of a warp is one
 //    contiguous run whenever the lowest target is >= 5 and stays within the
 //    same cache lines across the 2^k loads otherwise.
-//  * k = 6, 7 ("staged" kernels): a CTA stages 32 groups (32 x 2^k amplitudes)
-//    in shared memory with coalesced loads, then computes the 2^k x 2^k by
-//    2^k x 32 complex product with each thread holding 2^k/8 accumulators and
-//    stores straight back to HBM.
+//  * k = 6, 7 ("staged" kernels): a CTA copies a tile of 32..128 groups into
+//    shared memory with asynchronous coalesced copies, then computes the
+//    2^k x 2^k by 2^k x G complex product register-tiled (each thread a block
+//    of rows x groups) and stores straight back to HBM.  These are bound by the
+//    FP32 / FP64 FMA pipes, not HBM.
 //
 // Zero / +-1 matrix scalars (classified on the host with the reference's
 // tolerances) are exact, so dense evaluation reproduces the reference's
@@ -32,6 +33,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+
+#include <cuda_pipeline.h>
 
 namespace cb2 {
 
@@ -213,57 +216,96 @@ __global__ void __launch_bounds__(TileThreads<K>::N) k_gate_tile(T *__restrict__
     psi[tile_base + a.chunk_off[i >> a.tb] + (i & low_mask)] = s[swz<LOGE>(i)];
 }
 
-// Staged kernel for k = 6, 7: tiles of G groups in shared memory.
+// Staged kernel for k = 6, 7: a register-tiled complex GEMM per tile of G
+// groups.  The CTA copies the tile's D x G amplitudes into shared memory with
+// cp.async (coalesced: consecutive threads take consecutive groups of one
+// member; every copy of the tile in flight at once, no register round trip),
+// then thread (rs, gs) computes rows rs + i*RS (i < TR) for groups gs + j*GS
+// (j < TG): per column c it loads TR matrix entries (the same for all lanes of
+// a row slot: broadcast) and TG amplitudes (consecutive lanes, conflict-free)
+// for TR*TG complex multiply-adds, so loads stay well below the FMA count.
+// The matrix sits in shared memory when it takes at most 32 KB (FP32, k = 6),
+// else it is read through L1.  Two CTAs a SM overlap one's copies with the
+// other's arithmetic.  The products go straight back to HBM, the tile having
+// been read in full.
 constexpr int kStagedThreads = 256;
-constexpr int kStagedGroups = 32;
+
+template <typename T, int K> struct StagedShape {
+  static constexpr int D = 1 << K;
+  static constexpr int TR = sizeof(T) == 4 ? 8 : 4;  // rows a thread
+  static constexpr int TG = 4;                       // groups a thread
+  static constexpr int RS = D / TR;                  // row slots
+  static constexpr int GS = kStagedThreads / RS;     // group slots
+  static constexpr int G = TG * GS;                  // groups a tile
+  static constexpr bool kMatSmem = D * D * sizeof(T) * 2 <= 32768;  // matrix in shared memory
+  static constexpr int MAT_SMEM = kMatSmem ? D * D : 0;             // its entries
+  static_assert(RS * GS == kStagedThreads, "staged tile must use every thread");
+};
 
 template <typename T, int K>
-__global__ void __launch_bounds__(kStagedThreads) k_gate_staged(
+__global__ void __launch_bounds__(kStagedThreads, 2) k_gate_staged(
     T *__restrict__ sv, uint64_t n_groups, Targets t, const typename Vec2<T>::type *__restrict__ mat) {
   using V = typename Vec2<T>::type;
-  constexpr int D = 1 << K;
-  constexpr int G = kStagedGroups;
-  constexpr int SLOTS = kStagedThreads / G;  // row slots
-  constexpr int RPT = D / SLOTS;             // rows per thread
+  using Sh = StagedShape<T, K>;
+  constexpr int D = Sh::D, TR = Sh::TR, TG = Sh::TG, RS = Sh::RS, GS = Sh::GS, G = Sh::G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  V *s = reinterpret_cast<V *>(smem_raw);    // [D][G]
+  V *s = reinterpret_cast<V *>(smem_raw);  // [D][G]
+  V *msm = s + D * G;
   V *psi = reinterpret_cast<V *>(sv);
-  const int g_lane = threadIdx.x % G;
-  const int slot = threadIdx.x / G;
+  const int rs = threadIdx.x / GS, gs = threadIdx.x % GS;
+  if constexpr (Sh::kMatSmem) {
+    for (int i = threadIdx.x; i < D * D; i += kStagedThreads) msm[i] = mat[i];
+  }
   const uint64_t n_tiles = (n_groups + G - 1) / G;
   for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const uint64_t g0 = tile * G;
-    // stage: thread i loads member a = i / G of group g0 + i % G
+    // asynchronous global -> shared copies: every load of the tile in flight at once
     for (int i = threadIdx.x; i < D * G; i += kStagedThreads) {
       const int gg = i % G, a = i / G;
       const uint64_t g = g0 + gg;
-      if (g < n_groups) s[a * G + gg] = psi[group_base<K>(g, t) + member_offset<K>(a, t)];
+      if (g < n_groups)
+        __pipeline_memcpy_async(&s[a * G + gg], &psi[group_base<K>(g, t) + member_offset<K>(a, t)],
+                                sizeof(V));
     }
+    __pipeline_commit();
+    __pipeline_wait_prior(0);
     __syncthreads();
-    const uint64_t g = g0 + g_lane;
-    if (g < n_groups) {
-      T acc_re[RPT], acc_im[RPT];
+    T re[TR][TG], im[TR][TG];
 #pragma unroll
-      for (int j = 0; j < RPT; ++j) acc_re[j] = acc_im[j] = T(0);
-#pragma unroll 4
-      for (int c = 0; c < D; ++c) {
-        const V xc = s[c * G + g_lane];
+    for (int i = 0; i < TR; ++i)
 #pragma unroll
-        for (int j = 0; j < RPT; ++j) {
-          const V m = __ldg(&mat[(slot + j * SLOTS) * D + c]);
-          acc_re[j] = fma(m.x, xc.x, acc_re[j]);
-          acc_re[j] = fma(-m.y, xc.y, acc_re[j]);
-          acc_im[j] = fma(m.x, xc.y, acc_im[j]);
-          acc_im[j] = fma(m.y, xc.x, acc_im[j]);
+      for (int j = 0; j < TG; ++j) re[i][j] = im[i][j] = T(0);
+#pragma unroll 2
+    for (int c = 0; c < D; ++c) {
+      V x[TG];
+#pragma unroll
+      for (int j = 0; j < TG; ++j) x[j] = s[c * G + gs + j * GS];
+#pragma unroll
+      for (int i = 0; i < TR; ++i) {
+        V m;
+        if constexpr (Sh::kMatSmem) m = msm[(rs + i * RS) * D + c];
+        else m = __ldg(&mat[(rs + i * RS) * D + c]);
+#pragma unroll
+        for (int j = 0; j < TG; ++j) {
+          re[i][j] = fma(m.x, x[j].x, re[i][j]);
+          re[i][j] = fma(-m.y, x[j].y, re[i][j]);
+          im[i][j] = fma(m.x, x[j].y, im[i][j]);
+          im[i][j] = fma(m.y, x[j].x, im[i][j]);
         }
       }
-      const uint64_t base = group_base<K>(g, t);
+    }
 #pragma unroll
-      for (int j = 0; j < RPT; ++j) {
-        V o;
-        o.x = acc_re[j];
-        o.y = acc_im[j];
-        psi[base + member_offset<K>(slot + j * SLOTS, t)] = o;
+    for (int j = 0; j < TG; ++j) {
+      const uint64_t g = g0 + gs + j * GS;
+      if (g < n_groups) {
+        const uint64_t base = group_base<K>(g, t);
+#pragma unroll
+        for (int i = 0; i < TR; ++i) {
+          V o;
+          o.x = re[i][j];
+          o.y = im[i][j];
+          psi[base + member_offset<K>(rs + i * RS, t)] = o;
+        }
       }
     }
     __syncthreads();
@@ -369,7 +411,8 @@ template <typename T, int K>
 bool launch_staged(const GateData &g, void *sv, uint32_t n, const Targets &t, cudaStream_t s,
                    std::string &err) {
   using V = typename Vec2<T>::type;
-  constexpr size_t smem = sizeof(V) * (1 << K) * kStagedGroups;
+  constexpr int G = StagedShape<T, K>::G;
+  constexpr size_t smem = sizeof(V) * ((1 << K) * G + StagedShape<T, K>::MAT_SMEM);
   static int blocks_per_sm = 0;
   static std::once_flag once;
   static cudaError_t attr_rc = cudaSuccess;
@@ -384,7 +427,7 @@ bool launch_staged(const GateData &g, void *sv, uint32_t n, const Targets &t, cu
     return false;
   }
   const uint64_t n_groups = 1ull << (n - K);
-  const uint64_t n_tiles = (n_groups + kStagedGroups - 1) / kStagedGroups;
+  const uint64_t n_tiles = (n_groups + G - 1) / G;
   const uint64_t cap = (uint64_t)blocks_per_sm * sm_count();
   const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min(n_tiles, cap));
   k_gate_staged<T, K><<<grid, kStagedThreads, smem, s>>>(static_cast<T *>(sv), n_groups, t,

@@ -588,41 +588,6 @@ __global__ void __launch_bounds__(NT, 1)
 
 constexpr uint32_t kTrajMagic = 0xCB2077A1u;
 
-// Access-policy window that keeps the per-CTA trajectory slices persisting in
-// L2 (each pass rereads the slice it just wrote; without it most dirty lines are
-// written back to HBM between passes and some reloads miss L2).  The persisting
-// set-aside is a limit of this process's context; it is raised once, to at most
-// the device's maximum, and never lowered.
-bool l2_window(void *base, size_t bytes, cudaAccessPolicyWindow &w) {
-  static std::mutex mu;
-  static size_t limit_set = 0;
-  int dev = 0, max_persist = 0, max_window = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev) != cudaSuccess ||
-      max_persist <= 0 || max_window <= 0) {
-    cudaGetLastError();
-    return false;
-  }
-  const size_t want = std::min(bytes, (size_t)max_persist);
-  {
-    std::lock_guard<std::mutex> lock(mu);
-    if (limit_set < want) {
-      if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-      }
-      limit_set = want;
-    }
-  }
-  w.base_ptr = base;
-  w.num_bytes = std::min(bytes, (size_t)max_window);
-  w.hitRatio = std::min(1.0f, (float)limit_set / (float)w.num_bytes);
-  w.hitProp = cudaAccessPropertyPersisting;
-  w.missProp = cudaAccessPropertyStreaming;
-  return true;
-}
-
 // Threads per CTA when the program does not fix them: 1024 for states of 15 to
 // 17 qubits (slices larger than L1 but held in L2, so passes are bound by loads
 // in flight), 512 otherwise (issue-bound gate arithmetic).
@@ -645,22 +610,18 @@ unsigned auto_ctas(uint32_t n) {
   return fit >= sms || fit < sms / 2 ? sms : (unsigned)fit;
 }
 
-cudaError_t launch_trajectories(unsigned grid, unsigned threads, cudaStream_t s,
-                                const cudaAccessPolicyWindow *w, const TOp *ops, uint32_t n_ops,
-                                const float2 *pool, float2 *ws, uint32_t n, const TRun *run,
-                                double *z, uint32_t *sample) {
+// No access-policy window: a persisting-L2 set-aside sized for the workspace
+// gave the trajectories 4% at 16 qubits but, being a limit of the whole
+// context, cut every later streaming gate pass of the process from 6.3 to
+// 2.8 TB/s until it was set back to 0.
+cudaError_t launch_trajectories(unsigned grid, unsigned threads, cudaStream_t s, const TOp *ops,
+                                uint32_t n_ops, const float2 *pool, float2 *ws, uint32_t n,
+                                const TRun *run, double *z, uint32_t *sample) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(threads);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  if (w) {
-    attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
-    attr[0].val.accessPolicyWindow = *w;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-  }
   if (threads == 1024)
     return cudaLaunchKernelEx(&cfg, k_trajectories<1024>, ops, n_ops, pool, ws, n, run, z, sample);
   return cudaLaunchKernelEx(&cfg, k_trajectories<512>, ops, n_ops, pool, ws, n, run, z, sample);
@@ -968,8 +929,6 @@ int cast_b200_traj_run(void *prog, uint32_t n_traj, uint64_t seed, double *out_z
       return 1;
     }
     const uint32_t n_ops = (uint32_t)p->ops.size();
-    cudaAccessPolicyWindow win = {};
-    const bool win_ok = l2_window(p->d_ws, (sizeof(float2) << p->n) * grid, win);
     if (use_graph && s) {
       if (p->graph && (p->graph_stream != stream || p->graph_grid != grid || p->graph_threads != threads)) {
         cudaGraphExecDestroy(p->graph);
@@ -982,9 +941,8 @@ int cast_b200_traj_run(void *prog, uint32_t n_traj, uint64_t seed, double *out_z
           cb2::write_err(err_buf, err_buf_len, err);
           return 1;
         }
-        const cudaError_t lrc = launch_trajectories(grid, threads, s, win_ok ? &win : nullptr, p->d_ops, n_ops,
-                                                    p->d_pool, p->d_ws, p->n, p->d_run, p->d_z,
-                                                    p->d_sample);
+        const cudaError_t lrc = launch_trajectories(grid, threads, s, p->d_ops, n_ops, p->d_pool,
+                                                    p->d_ws, p->n, p->d_run, p->d_z, p->d_sample);
         const cudaError_t erc = cudaStreamEndCapture(s, &gph);
         if (!cuda_ok(lrc, "trajectory kernel capture", err) ||
             !cuda_ok(erc, "cudaStreamEndCapture", err) ||
@@ -1003,8 +961,8 @@ int cast_b200_traj_run(void *prog, uint32_t n_traj, uint64_t seed, double *out_z
         return 1;
       }
     } else {
-      if (!cuda_ok(launch_trajectories(grid, threads, s, win_ok ? &win : nullptr, p->d_ops, n_ops, p->d_pool,
-                                       p->d_ws, p->n, p->d_run, p->d_z, p->d_sample),
+      if (!cuda_ok(launch_trajectories(grid, threads, s, p->d_ops, n_ops, p->d_pool, p->d_ws, p->n,
+                                       p->d_run, p->d_z, p->d_sample),
                    "trajectory kernel launch", err)) {
         cb2::write_err(err_buf, err_buf_len, err);
         return 1;

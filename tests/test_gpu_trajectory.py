@@ -217,3 +217,37 @@ def test_replay_is_deterministic_both_cta_sizes(mods, n):
     a, sa = prog.run(600, 11, st)
     b, sb = prog.run(600, 11, st)
     assert np.array_equal(a, b) and np.array_equal(sa, sb)
+
+
+def test_trajectories_leave_gate_throughput_alone(mods):
+    """A trajectory run must leave no context-wide state behind that slows the
+    statevector passes that follow in the same process (a persisting-L2
+    set-aside once cut them to less than half)."""
+    from cast_simulator_b200 import cuda as cu
+    from cast_simulator_b200.fusion import FusionConfig, optimize_native
+
+    T, TR, S = mods
+    n = 26
+    gates = optimize_native(n, T.QuantumCircuit.brickwork(n, 8, 3).gates(), FusionConfig.size_only(4)).gates()
+    prog = S.GateProgram(cu.CudaPrecision.F64, n, 1e-12, 1e-12, False)
+    for g in gates:
+        prog.add(g.matrix(), g.qubits())
+    sv = cu.CudaStatevector(n, cu.CudaPrecision.F64)
+    st = S.Stream()
+
+    def best_time():
+        e0, e1, ts = S.Event(), S.Event(), []
+        for _ in range(4):
+            sv.zero(st)
+            e0.record(st)
+            prog.run(sv, st, use_graph=True)
+            e1.record(st)
+            e1.sync()
+            ts.append(e1.elapsed_s(e0))
+        return min(ts)
+
+    before = best_time()
+    TR.TrajectoryProgram(T.QuantumCircuit.brickwork(16, 10, 1, depolarizing=1e-3, damping=5e-4), 3).run(
+        1024, 1, st)
+    after = best_time()
+    assert after < 1.3 * before, (before, after)
