@@ -154,6 +154,9 @@ CAST_B200 = [
     ("cast_b200_traj_run", C.c_int,
      [C.c_void_p, C.c_uint32, C.c_uint64, c_dp, c_u32p, C.c_void_p, C.c_int, C.c_char_p,
       C.c_size_t]),
+    ("cast_b200_traj_run_range", C.c_int,
+     [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, c_dp, c_u32p, C.c_void_p, C.c_int,
+      C.c_char_p, C.c_size_t]),
     ("cast_b200_norm_squared_noalloc", C.c_int,
      [C.c_uint64, C.c_size_t, C.c_uint8, c_dp, C.c_void_p, C.c_char_p, C.c_size_t]),
 ]

@@ -61,7 +61,7 @@ struct TOp {
 
 struct TRun {  // device-resident, rewritten before each launch
   uint32_t n_traj;
-  uint32_t pad;
+  uint32_t first;  // index of the first trajectory (its Philox stream), for ranges
   uint64_t seed;
 };
 
@@ -434,7 +434,7 @@ struct Traj {
 
   // End of a trajectory: <Z_q> for every qubit and one sampled bitstring.
   static __device__ __noinline__ void finish(float2 *sv, uint32_t n, Shared &S, double *csum, uint64_t seed,
-                                      uint32_t traj, double *out_z, uint32_t *out_sample) {
+                                      uint32_t traj, double *z_row, uint32_t *sample_slot) {
     {
       double t, a, b;
       stats_pass(sv, n, S, 0, 0.0, 0, t, a, b);  // materialise the pending diagonal
@@ -463,7 +463,7 @@ struct Traj {
             if (q0 + j < c && ((i >> (q0 + j)) & 1)) acc[j] += p;
         }
       block_sum3(S, acc[0], acc[1], acc[2]);
-      if (threadIdx.x < 3 && q0 + threadIdx.x < c) out_z[(size_t)traj * n + q0 + threadIdx.x] = acc[threadIdx.x];
+      if (threadIdx.x < 3 && q0 + threadIdx.x < c) z_row[q0 + threadIdx.x] = acc[threadIdx.x];
     }
     // qubits that index the threads: thread j sums the chunk sums with bit j set
     const uint32_t nthr = N >> c;
@@ -471,7 +471,7 @@ struct Traj {
       double x = 0;
       for (uint32_t tt = 0; tt < nthr; ++tt)
         if ((tt >> threadIdx.x) & 1) x += csum[tt];
-      out_z[(size_t)traj * n + c + threadIdx.x] = x;
+      z_row[c + threadIdx.x] = x;
     }
     if (threadIdx.x == 0) {
       double tot = 0;
@@ -500,13 +500,13 @@ struct Traj {
         acc += p;
         if (acc > target) break;
       }
-      if (out_sample) out_sample[traj] = isel;
+      if (sample_slot) *sample_slot = isel;
     }
     __syncthreads();
     const double tot = S.vals[3];
     if (threadIdx.x < n) {
-      const double p1 = out_z[(size_t)traj * n + threadIdx.x];
-      out_z[(size_t)traj * n + threadIdx.x] = tot > 0 ? 1.0 - 2.0 * p1 / tot : 0.0;
+      const double p1 = z_row[threadIdx.x];
+      z_row[threadIdx.x] = tot > 0 ? 1.0 - 2.0 * p1 / tot : 0.0;
     }
     __syncthreads();
   }
@@ -525,7 +525,8 @@ __global__ void __launch_bounds__(NT, 1)
   const uint64_t seed = run->seed;
   const uint32_t N = 1u << n;
   float2 *sv = ws + ((size_t)blockIdx.x << n);
-  for (uint32_t traj = blockIdx.x; traj < n_traj; traj += gridDim.x) {
+  for (uint32_t lt = blockIdx.x; lt < n_traj; lt += gridDim.x) {
+    const uint32_t traj = run->first + lt;  // draws depend on the global index only
     for (uint32_t i = threadIdx.x; i < N; i += NT)
       sv[i] = make_float2(i == 0 ? 1.f : 0.f, 0.f);
     if (threadIdx.x == 0) S.pend = 0;
@@ -582,7 +583,7 @@ __global__ void __launch_bounds__(NT, 1)
         stats_valid = false;
       }
     }
-    Tr::finish(sv, n, S, csum, seed, traj, out_z, out_sample);
+    Tr::finish(sv, n, S, csum, seed, traj, out_z + (size_t)lt * n, out_sample ? out_sample + lt : nullptr);
   }
 }
 
@@ -871,7 +872,18 @@ uint32_t cast_b200_traj_num_ops(const void *prog) {
 int cast_b200_traj_run(void *prog, uint32_t n_traj, uint64_t seed, double *out_z,
                        uint32_t *out_samples, void *stream, int use_graph, char *err_buf,
                        size_t err_buf_len) {
+  return cast_b200_traj_run_range(prog, 0, n_traj, seed, out_z, out_samples, stream, use_graph,
+                                  err_buf, err_buf_len);
+}
+
+int cast_b200_traj_run_range(void *prog, uint32_t first, uint32_t n_traj, uint64_t seed,
+                             double *out_z, uint32_t *out_samples, void *stream, int use_graph,
+                             char *err_buf, size_t err_buf_len) {
   TrajProgram *p = as_traj(prog);
+  if (p && (uint64_t)first + n_traj > 0xFFFFFFFFull) {
+    cb2::write_err(err_buf, err_buf_len, "trajectory range exceeds 2^32 indices");
+    return 1;
+  }
   if (!p || !out_z || n_traj == 0) {
     cb2::write_err(err_buf, err_buf_len, "invalid trajectory program, output or count");
     return 1;
@@ -922,7 +934,7 @@ int cast_b200_traj_run(void *prog, uint32_t n_traj, uint64_t seed, double *out_z
         p->graph = nullptr;
       }
     }
-    TRun r{n_traj, 0, seed};
+    TRun r{n_traj, first, seed};
     if (!cuda_ok(cudaMemcpyAsync(p->d_run, &r, sizeof(r), cudaMemcpyHostToDevice, s),
                  "cudaMemcpyAsync (run parameters)", err)) {
       cb2::write_err(err_buf, err_buf_len, err);

@@ -21,6 +21,11 @@ the same gate-application path:
     ``expectation_z`` all-reduces per-position populations (FP64) and maps them
     back to logical qubits.
 
+Trajectories shard without any exchange: ``run_trajectories_sharded`` gives
+rank r a contiguous range of trajectory indices (each trajectory's draws depend
+on its index only, so the union of the ranges is the single-GPU batch row for
+row) and all-reduces the per-qubit <Z> sums in FP64.
+
 Communication is ``torch.distributed``: NCCL on GPUs, gloo on CPU.
 """
 from __future__ import annotations
@@ -187,3 +192,39 @@ def cuda_apply_local(precision: int, ztol: float = 1e-12, otol: float = 1e-12) -
             qs.ctypes.data_as(L.c_u32p), k, ztol, otol, C.c_void_p(stream), eb, L.ERR_LEN), eb, "apply_gate")
 
     return apply
+
+
+def trajectory_range(n_traj: int, world: int, rank: int) -> tuple[int, int]:
+    """(first, count) of rank's contiguous share of n_traj trajectories; the
+    first n_traj % world ranks take one more."""
+    if world < 1 or not 0 <= rank < world or n_traj < 0:
+        raise ValueError("bad trajectory partition")
+    base, rem = divmod(n_traj, world)
+    return rank * base + min(rank, rem), base + (1 if rank < rem else 0)
+
+
+def run_trajectories_sharded(program, n_traj: int, seed: int, stream=None, group=None):
+    """Data-parallel trajectories over the ranks of ``group``: each rank runs its
+    range of ``program`` (a ``TrajectoryProgram``) and the per-qubit sums of
+    <Z> plus the trajectory count are all-reduced in FP64.  Returns
+    (mean <Z> over all n_traj trajectories, this rank's rows, this rank's first
+    index)."""
+    import torch
+    import torch.distributed as dist
+
+    on = dist.is_initialized()
+    world = dist.get_world_size(group) if on else 1
+    rank = dist.get_rank(group) if on else 0
+    first, count = trajectory_range(n_traj, world, rank)
+    n = program.n
+    if count:
+        z, _ = program.run(count, seed, stream, first=first)
+    else:
+        z = np.zeros((0, n))
+    dev = "cuda" if on and dist.get_backend(group) == "nccl" else "cpu"
+    acc = torch.tensor(np.concatenate([z.sum(axis=0), [float(count)]]), dtype=torch.float64,
+                       device=dev)
+    if world > 1:
+        dist.all_reduce(acc, group=group)
+    acc = acc.cpu().numpy()
+    return acc[:n] / acc[n], z, first

@@ -232,16 +232,19 @@ class TrajectoryProgram:
         L.check(L.lib().cast_b200_traj_set_launch(self.handle, int(threads), int(max_ctas), eb,
                                                   L.ERR_LEN), eb, "traj_set_launch")
 
-    def run(self, n_traj: int, seed: int, stream=None, use_graph: bool = True):
-        """(z, samples): <Z_q> per trajectory (n_traj x n) and one bitstring each."""
+    def run(self, n_traj: int, seed: int, stream=None, use_graph: bool = True, first: int = 0):
+        """(z, samples): <Z_q> per trajectory (n_traj x n) and one bitstring each,
+        for trajectories first .. first + n_traj - 1 of ``seed`` (row j is
+        trajectory first + j; a trajectory's draws depend on its index only)."""
         z = np.zeros((n_traj, self.n))
         smp = np.zeros(n_traj, dtype=np.uint32)
         eb = L.errbuf()
         h = stream.handle if stream is not None else None
-        L.check(L.lib().cast_b200_traj_run(self.handle, n_traj, seed & ((1 << 64) - 1),
-                                           z.ctypes.data_as(L.c_dp), smp.ctypes.data_as(L.c_u32p),
-                                           h, int(use_graph and h is not None), eb, L.ERR_LEN), eb,
-                "traj_run")
+        L.check(L.lib().cast_b200_traj_run_range(self.handle, first, n_traj, seed & ((1 << 64) - 1),
+                                                 z.ctypes.data_as(L.c_dp),
+                                                 smp.ctypes.data_as(L.c_u32p), h,
+                                                 int(use_graph and h is not None), eb, L.ERR_LEN),
+                eb, "traj_run")
         return z, smp
 
 

@@ -180,6 +180,13 @@ int cast_b200_traj_set_launch(void *program, uint32_t threads, uint32_t max_ctas
 int cast_b200_traj_run(void *program, uint32_t n_traj, uint64_t seed, double *out_z,
                        uint32_t *out_samples, void *stream, int use_graph, char *err_buf,
                        size_t err_buf_len);
+/* Trajectories first .. first + n_traj - 1 of the same seed: trajectory i draws
+ * from Philox stream (seed, i) whatever range it is run in, so ranges split over
+ * ranks or calls reproduce one cast_b200_traj_run of the whole batch row for row.
+ * Outputs are indexed from 0 (row j is trajectory first + j). */
+int cast_b200_traj_run_range(void *program, uint32_t first, uint32_t n_traj, uint64_t seed,
+                             double *out_z, uint32_t *out_samples, void *stream, int use_graph,
+                             char *err_buf, size_t err_buf_len);
 
 /* -- Allocation-free norm^2 -------------------------------------------------------
  * No counterpart in the reference: an extra variant of cast_cuda_norm_squared

@@ -100,3 +100,67 @@ def test_sharded_matches_oracle(oracle, tmp_path, world):
     z_ref = np.array([1 - 2 * p[(idx >> q) & 1 == 1].sum() for q in range(n)])
     assert np.max(np.abs(np.load(tmp_path / "z.npy") - z_ref)) < 1e-12
     assert int(np.load(tmp_path / "ex.npy")[0]) > 0  # the circuit did cross shards
+
+
+def test_trajectory_range_partition():
+    for n_traj in (0, 1, 7, 4096):
+        for world in (1, 2, 3, 8):
+            parts = [D.trajectory_range(n_traj, world, r) for r in range(world)]
+            assert sum(c for _, c in parts) == n_traj
+            nxt = 0
+            for first, count in parts:
+                assert first == nxt  # contiguous, in rank order
+                nxt = first + count
+            assert max(c for _, c in parts) - min(c for _, c in parts) <= 1
+    with pytest.raises(ValueError):
+        D.trajectory_range(10, 2, 2)
+
+
+class _IndexedProgram:
+    """Stands in for a TrajectoryProgram: row j of a run is a fixed function of
+    the global trajectory index first + j (as the device kernel's Philox streams
+    are)."""
+
+    n = 5
+
+    def run(self, count, seed, stream=None, first=0):
+        idx = np.arange(first, first + count, dtype=np.float64)[:, None]
+        q = np.arange(self.n)[None, :]
+        return np.cos(0.37 * idx * (q + 1) + seed), np.zeros(count, dtype=np.uint32)
+
+
+def _traj_worker(rank, world, port, n_traj, out_dir):
+    import sys
+
+    import torch.distributed as dist
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from cast_simulator_b200 import distributed as D
+    from tests.test_distributed import _IndexedProgram
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        mean, rows, first = D.run_trajectories_sharded(_IndexedProgram(), n_traj, 3)
+        np.save(os.path.join(out_dir, f"mean{rank}.npy"), mean)
+        np.save(os.path.join(out_dir, f"rows{rank}.npy"), rows)
+        np.save(os.path.join(out_dir, f"first{rank}.npy"), np.array([first]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,n_traj", [(2, 101), (3, 2)])
+def test_sharded_trajectories_equal_one_batch(tmp_path, world, n_traj):
+    """Ranges over gloo ranks reproduce the single batch row for row and the
+    all-reduced mean equals its mean (a rank may get no trajectories)."""
+    import torch.multiprocessing as mp
+
+    mp.start_processes(_traj_worker, args=(world, _free_port(), n_traj, str(tmp_path)),
+                       nprocs=world, join=True, start_method="spawn")
+    full, _ = _IndexedProgram().run(n_traj, 3)
+    rows = np.concatenate([np.load(tmp_path / f"rows{r}.npy") for r in range(world)])
+    assert np.array_equal(rows, full)
+    for r in range(world):
+        assert np.allclose(np.load(tmp_path / f"mean{r}.npy"), full.mean(axis=0), atol=1e-14)

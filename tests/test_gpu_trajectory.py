@@ -251,3 +251,24 @@ def test_trajectories_leave_gate_throughput_alone(mods):
         1024, 1, st)
     after = best_time()
     assert after < 1.3 * before, (before, after)
+
+
+@pytest.mark.parametrize("n", [12, 16])
+def test_ranges_reproduce_the_batch(mods, n):
+    """Trajectory i draws from Philox stream (seed, i) whatever range it runs
+    in: two ranges reproduce one batch row for row, which is what the
+    data-parallel runner relies on."""
+    from cast_simulator_b200 import distributed as D
+
+    T, TR, S = mods
+    circ = T.QuantumCircuit.brickwork(n, 4, 9, depolarizing=0.02, damping=0.02)
+    prog = TR.TrajectoryProgram(circ, 3)
+    st = S.Stream()
+    z, smp = prog.run(300, 5, st)
+    z1, s1 = prog.run(100, 5, st, first=0)
+    z2, s2 = prog.run(200, 5, st, first=100)
+    assert np.array_equal(np.concatenate([z1, z2]), z)
+    assert np.array_equal(np.concatenate([s1, s2]), smp)
+    mean, rows, first = D.run_trajectories_sharded(prog, 300, 5, st)
+    assert first == 0 and np.array_equal(rows, z)
+    assert np.allclose(mean, z.mean(axis=0), atol=1e-14)
