@@ -124,8 +124,10 @@ __global__ void __launch_bounds__(kRegThreads) k_gate_reg(T *__restrict__ sv, ui
 // Tile kernel for gates with targets among the low (intra-cache-line) qubits.
 // A CTA owns one tile: the 2^(tb + k_hi) amplitudes whose "outer" bits are
 // fixed, i.e. 2^k_hi chunks (one per combination of the targets >= tb) of
-// 2^tb contiguous amplitudes.  The chunks are read and written with fully
-// coalesced 128/64-bit accesses; the gate is applied inside shared memory,
+// 2^tb contiguous amplitudes.  The chunks are read with fully coalesced
+// asynchronous copies (cp.async, the whole tile in flight, no register round
+// trip) and written with coalesced 128/64-bit stores; the gate is applied inside
+// shared memory,
 // where the tile-local layout puts the high targets at bits tb..tb+k_hi-1.
 // Shared memory is XOR-swizzled inside each 128-byte block so that both the
 // contiguous phases and the strided gather of group members avoid bank
@@ -146,7 +148,10 @@ __device__ __forceinline__ uint32_t swz(uint32_t i) {
   return i ^ ((i >> LOGE) & ((1u << LOGE) - 1));
 }
 
-constexpr uint32_t kTileBits = 11;  // 2048 amplitudes per tile: 32 KB (f64) / 16 KB (f32)
+// Amplitudes per tile: 4096 for k = 3, 2048 otherwise (measured at 30 qubits with
+// targets 0..k-1: k = 3 runs at 6.9 instead of 6.1 TB/s (FP64) with the larger
+// tile, k = 2 and 4 lose with it).
+constexpr uint32_t tile_bits(uint32_t k) { return k == 3 ? 12u : 11u; }
 
 template <typename T, int K>
 __global__ void __launch_bounds__(TileThreads<K>::N) k_gate_tile(T *__restrict__ sv, TileArgs a,
@@ -154,7 +159,7 @@ __global__ void __launch_bounds__(TileThreads<K>::N) k_gate_tile(T *__restrict__
   constexpr int kTileThreads = TileThreads<K>::N;
   using V = typename Vec2<T>::type;
   constexpr int D = 1 << K;
-  constexpr uint32_t TILE = 1u << kTileBits;
+  constexpr uint32_t TILE = 1u << tile_bits(K);
   constexpr int LOGE = sizeof(V) == 16 ? 3 : 4;  // elements per 128-byte block
   // groups per thread, fully unrolled (a runtime loop would let the compiler
   // hoist the matrix out of the constant bank into registers)
@@ -166,9 +171,12 @@ __global__ void __launch_bounds__(TileThreads<K>::N) k_gate_tile(T *__restrict__
   uint64_t tile_base = (uint64_t)blockIdx.x << a.tb;
   for (uint32_t j = 0; j < a.k_hi; ++j)
     tile_base = ((tile_base & ~a.hi_lo_mask[j]) << 1) | (tile_base & a.hi_lo_mask[j]);
-#pragma unroll 4
+  // asynchronous global -> shared copies: the whole tile in flight at once
   for (uint32_t i = threadIdx.x; i < TILE; i += kTileThreads)
-    s[swz<LOGE>(i)] = psi[tile_base + a.chunk_off[i >> a.tb] + (i & low_mask)];
+    __pipeline_memcpy_async(&s[swz<LOGE>(i)], &psi[tile_base + a.chunk_off[i >> a.tb] + (i & low_mask)],
+                            sizeof(V));
+  __pipeline_commit();
+  __pipeline_wait_prior(0);
   __syncthreads();
 #pragma unroll
   for (int u = 0; u < GPT; ++u) {
@@ -346,7 +354,7 @@ bool launch_reg(const GateData &g, void *sv, uint32_t n, const Targets &t, cudaS
 
 // Tile geometry for a gate: returns false when the tile kernel does not apply.
 bool tile_geometry(const GateData &g, uint32_t n, TileArgs &a) {
-  const uint32_t target = kTileBits;
+  const uint32_t target = tile_bits(g.k);
   if (n < target) return false;
   uint32_t need = 0;  // every target below 5 must sit inside a chunk
   for (uint32_t b = 0; b < g.k; ++b)
@@ -392,11 +400,11 @@ bool launch_tile(const GateData &g, void *sv, uint32_t n, const TileArgs &a, cud
   static cudaError_t attr_rc = cudaSuccess;
   std::call_once(once, [] {
     attr_rc = cudaFuncSetAttribute(k_gate_tile<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(sizeof(V) << kTileBits));
+                                   (int)(sizeof(V) << tile_bits(K)));
   });
   if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(tile gate kernel)", err)) return false;
-  const uint64_t n_tiles = 1ull << (n - kTileBits);
-  const size_t smem = sizeof(V) << kTileBits;
+  const uint64_t n_tiles = 1ull << (n - tile_bits(K));
+  const size_t smem = sizeof(V) << tile_bits(K);
   const MatParam<T, K> *mp;
   if constexpr (sizeof(T) == 8) mp = reinterpret_cast<const MatParam<T, K> *>(g.m64.data());
   else mp = reinterpret_cast<const MatParam<T, K> *>(g.m32.data());
@@ -454,16 +462,23 @@ bool try_tile(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::stri
   if (g.k > 4) return true;
   const int ov = gate_path_override();
   if (ov == 1) return true;
-  // Measured on B200 (30 qubits): the register kernel loses 40-70% of its
-  // bandwidth once a warp's loads of one member touch 32 distinct cache lines
-  // (f64: targets {0,1,2} all present) or use 8 of every 32 sector bytes
-  // (f32: targets {0,1} both present); elsewhere it is at or above the tile
-  // kernel.
+  // Measured on B200 (30 qubits, every placement of k = 1..4 with low
+  // targets): the register kernel loses bandwidth when a warp's loads of one
+  // member touch many cache lines for a few bytes each and the lines do not
+  // survive in L1 until the group's other members are loaded.  FP64: the tile
+  // kernel runs at 6.9 TB/s and is at or above the register kernel once two
+  // targets lie below qubit 5 (k = 4 on qubits 1..4: 6.9 against 6.1).  FP32:
+  // with targets 0 and 1 (register kernel 2.0-4.2 TB/s), or with the lowest
+  // target 1 and three targets below 5 (k = 3 on 1..3: 6.0 against 4.1);
+  // elsewhere the register kernel is faster (k = 3 on 2..4: 6.4 against 6.0).
   uint32_t low_bits = 0;
   for (uint32_t b = 0; b < g.k; ++b)
     if (g.qubits[b] < 5) low_bits |= 1u << g.qubits[b];
-  const uint32_t bad = g.precision == 1 ? 0x7u : 0x3u;
-  if (ov != 2 && (low_bits & bad) != bad) return true;
+  const int n_low = __builtin_popcount(low_bits);
+  const bool tile_wins = g.precision == 1
+                             ? n_low >= 2
+                             : ((low_bits & 0x3u) == 0x3u || (g.qubits[0] == 1 && n_low >= 3));
+  if (ov != 2 && !tile_wins) return true;
   if (ov == 2 && low_bits == 0) return true;
   TileArgs a;
   std::memset(&a, 0, sizeof(a));
