@@ -120,10 +120,9 @@ def build_fused(n: int, depth: int, k: int, seed: int = 2024):
     return circ, g.gates_in_row_order()
 
 
-def cpu_baseline_run(n: int, gates, precision: str, budget_s: float, threads: int):
-    """Time the threaded SIMD CPU restatement (oracle/cpu_baseline.cpp) on the
-    host cores: as many fused-gate passes as fit in the budget.  Returns
-    (GB/s, passes, seconds)."""
+def _cpu_baseline_lib():
+    """The threaded SIMD CPU restatement of CAST's CPU kernels (oracle/), built
+    on first use: the timed CPU baseline and the checker of the GPU result."""
     import ctypes as C
 
     from oracle import oracle as O
@@ -134,8 +133,54 @@ def cpu_baseline_run(n: int, gates, precision: str, budget_s: float, threads: in
     lib.cb_alloc.argtypes = [C.c_uint32, C.c_int]
     lib.cb_free.argtypes = [C.c_void_p]
     lib.cb_zero.argtypes = [C.c_void_p]
+    lib.cb_store.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.cb_apply.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint32), C.c_uint32,
                              C.c_int]
+    return lib
+
+
+def cpu_parity(n: int, depth: int, k: int, precision: str, threads: int) -> dict:
+    """Parity of the GPU result against CAST's FP64 CPU statevector path (its
+    restatement in oracle/): the benchmark's brickwork construction at n qubits,
+    fused at width k, run once from |0> on the CPU in FP64 and on the GPU in the
+    benchmark's precision through the public gate-program API."""
+    import ctypes as C
+
+    from cast_simulator_b200 import cuda as cu
+
+    lib = _cpu_baseline_lib()
+    _, gates = build_fused(n, depth, k)
+    sv = lib.cb_alloc(n, 0)
+    if not sv:
+        raise MemoryError("cpu parity allocation failed")
+    try:
+        lib.cb_zero(sv)
+        for g in gates:
+            m = np.ascontiguousarray(g.matrix()).view(np.float64)
+            q = np.asarray(g.qubits(), dtype=np.uint32)
+            lib.cb_apply(sv, m.ctypes.data_as(C.POINTER(C.c_double)),
+                         q.ctypes.data_as(C.POINTER(C.c_uint32)), q.size, threads)
+        ref = np.empty(1 << n, dtype=np.complex128)
+        lib.cb_store(sv, ref.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
+    finally:
+        lib.cb_free(sv)
+    prec = cu.CudaPrecision.F64 if precision == "f64" else cu.CudaPrecision.F32
+    _, gsv = _run_fused(n, gates, prec, reps=1)
+    psi = gsv.download()
+    ov = abs(np.vdot(ref, psi)) / (np.linalg.norm(ref) * np.linalg.norm(psi))
+    return {"workload": f"brickwork-{n}q-d{depth} fused k={k} ({len(gates)} passes), from |0>",
+            "reference": "FP64 CPU restatement of CAST's statevector path",
+            "one_minus_abs_overlap": float(1.0 - ov),
+            "max_abs_err": float(np.max(np.abs(ref - psi)))}
+
+
+def cpu_baseline_run(n: int, gates, precision: str, budget_s: float, threads: int):
+    """Time the threaded SIMD CPU restatement (oracle/cpu_baseline.cpp) on the
+    host cores: as many fused-gate passes as fit in the budget.  Returns
+    (GB/s, passes, seconds)."""
+    import ctypes as C
+
+    lib = _cpu_baseline_lib()
     f32 = precision == "f32"
     sv = lib.cb_alloc(n, int(f32))
     if not sv:
@@ -640,7 +685,8 @@ def main(argv=None):
         gbs, passes, el = cpu_baseline_run(n_cpu, cgates, args.precision, args.cpu_budget, threads)
         line["cpu_baseline"] = {
             "value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
-            "sample": f"{passes} fused-gate passes of the {n_cpu}-qubit brickwork (k={args.k}) in {el:.1f} s"}
+            "sample": f"{passes} fused-gate passes of the {n_cpu}-qubit brickwork (k={args.k}) in {el:.1f} s",
+            "parity": cpu_parity(min(n, 22), args.depth, args.k, args.precision, threads)}
     # the extra legs run on one GPU only: under torchrun the other ranks would sit
     # in the closing barrier for the minutes they take
     if rank == 0 and ws == 1 and not args.no_extras:
