@@ -56,10 +56,7 @@ struct Program {
 
   ~Program() {
     for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
-    for (auto &g : gates) {
-      if (g.d_mat) cudaFree(g.d_mat);
-      if (g.d_tc) cudaFree(g.d_tc);
-    }
+    for (auto &g : gates) cb2::free_gate_device(g);
   }
 
   void drop_graphs() {
@@ -150,11 +147,13 @@ int cast_b200_apply_gate(uint64_t sv_dptr, uint32_t sv_n_qubits, uint8_t precisi
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     bool ok;
-    if (g.k >= 6) {
-      ok = cb2::upload_gate_matrix(g, err) &&
+    const bool sparse = cb2::sparse_gate(g);
+    if (sparse || g.k >= 6) {
+      // the device copy is freed once the launch that reads it has finished
+      ok = (sparse ? cb2::upload_sparse(g, err) : cb2::upload_gate_matrix(g, err)) &&
            cb2::launch_gate(g, reinterpret_cast<void *>(sv_dptr), sv_n_qubits, s, err) &&
            cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize", err);
-      if (g.d_mat) cudaFree(g.d_mat);
+      cb2::free_gate_device(g);
     } else {
       ok = cb2::launch_gate(g, reinterpret_cast<void *>(sv_dptr), sv_n_qubits, s, err);
     }
@@ -201,9 +200,16 @@ int cast_b200_program_add_gate(void *program, const cast_complex64_t *matrix,
   try {
     GateData g;
     std::string err;
-    if (!make_gate(p->precision, matrix, qubits, n_gate_qubits, p->ztol, p->otol, g, err) ||
-        !cb2::check_gate(g, p->n, err) || (g.k >= 6 && !cb2::upload_gate_matrix(g, err)) ||
-        (p->split && cb2::tensor_path_supported(g) && !cb2::prepare_tensor_gate(g, err))) {
+    bool ok = make_gate(p->precision, matrix, qubits, n_gate_qubits, p->ztol, p->otol, g, err) &&
+              cb2::check_gate(g, p->n, err);
+    if (ok) {
+      if (cb2::sparse_gate(g)) ok = cb2::upload_sparse(g, err);  // CSR kernel, any precision mode
+      else
+        ok = (g.k < 6 || cb2::upload_gate_matrix(g, err)) &&
+             (!p->split || !cb2::tensor_path_supported(g) || cb2::prepare_tensor_gate(g, err));
+    }
+    if (!ok) {
+      cb2::free_gate_device(g);
       write_err(err_buf, err_buf_len, err);
       return 1;
     }

@@ -402,7 +402,9 @@ void *cast_cuda_cubin_load(const uint8_t *cubin_data, size_t cubin_len, char *er
     std::memcpy(m->gate.m64.data(), cubin_data + sizeof(h), h.n_scalars * sizeof(double));
     m->gate.m32.resize(h.n_scalars);
     for (size_t i = 0; i < h.n_scalars; ++i) m->gate.m32[i] = (float)m->gate.m64[i];
-    if (!cb2::upload_gate_matrix(m->gate, err)) {
+    if (!cb2::upload_gate_matrix(m->gate, err) ||
+        (cb2::sparse_gate(m->gate) && !cb2::upload_sparse(m->gate, err))) {
+      cb2::free_gate_device(m->gate);
       delete m;
       write_err(err_buf, err_buf_len, err);
       return nullptr;
@@ -418,7 +420,7 @@ void *cast_cuda_cubin_load(const uint8_t *cubin_data, size_t cubin_len, char *er
 void cast_cuda_module_unload(void *cu_module) {
   Module *m = static_cast<Module *>(cu_module);
   if (!m || m->magic != kModuleMagic) return;
-  if (m->gate.d_mat) cudaFree(m->gate.d_mat);
+  cb2::free_gate_device(m->gate);
   m->magic = 0;
   delete m;
 }

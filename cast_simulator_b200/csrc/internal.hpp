@@ -23,6 +23,7 @@ struct GateData {
   std::vector<float> m32;
   void *d_mat = nullptr;  // device copy in the gate's precision (owned by the holder)
   void *d_tc = nullptr;   // split-BF16 tensor-core gate operand (owned by the holder), if any
+  void *d_sparse = nullptr;  // CSR copy for the sparse kernel (owned by the holder), if any
 };
 
 // Error helper: fills `err` and returns false on a CUDA failure.
@@ -48,6 +49,13 @@ bool check_gate(const GateData &g, uint32_t n, std::string &err);
 
 // Enqueues one gate application on `stream` (in place on `sv`).
 bool launch_gate(const GateData &g, void *sv, uint32_t n, cudaStream_t stream, std::string &err);
+
+// Sparse gates (k >= 5, at most 2^k / 4 nonzero entries a row on average after
+// snapping) run on the CSR kernel instead of the dense ones; upload_sparse
+// fills g.d_sparse.  free_gate_device releases every device copy of a gate.
+bool sparse_gate(const GateData &g);
+bool upload_sparse(GateData &g, std::string &err);
+void free_gate_device(GateData &g);
 
 // Classifies matrix scalars as 0 / +-1 / immediate with tolerances scaled by
 // 1/2^k and fills g.m64 / g.m32 (src/cpp/cuda/cuda_gen.cpp:84-103).

@@ -94,6 +94,63 @@ def test_qft14_golden_on_gpu(cu, oracle):
     assert np.max(np.abs(got - golden)) < 1e-10
 
 
+def _monomial(rng, k):
+    """A permutation with unit phases: one nonzero a row (fused CX / phase blocks)."""
+    d = 1 << k
+    m = np.zeros((d, d), dtype=complex)
+    m[np.arange(d), rng.permutation(d)] = np.exp(2j * np.pi * rng.random(d))
+    return m
+
+
+def _block_sparse(rng, k):
+    """Identity on k - 2 qubits times a dense 2-qubit gate: 4 nonzeros a row."""
+    return np.kron(np.eye(1 << (k - 2)), haar(rng, 4))
+
+
+@pytest.mark.parametrize("prec", [1, 0])
+@pytest.mark.parametrize("k", [3, 4, 5, 6, 7])
+def test_sparse_gates_all_placements(cu, oracle, prec, k):
+    """Gates with at most 2^k / 4 nonzeros a row (CSR kernel from k = 5, dense
+    kernels below): monomial and block-sparse matrices, low, high and random
+    targets, small and partial grids (fewer groups than a CTA holds)."""
+    rng = np.random.default_rng(300 + k)
+    for n in sorted({k, k + 1, 12, 17}):
+        placements = [tuple(range(k)), tuple(range(n - k, n))]
+        placements.append(tuple(sorted(rng.choice(n, size=k, replace=False).tolist())))
+        for q in placements:
+            for make in (_monomial, _block_sparse):
+                m = make(rng, k)
+                init = oracle.random_state(n, 11 + k)
+                ref = init.copy()
+                oracle.apply_gate(ref, m, q)
+                got = run_gates(cu, n, [_G(m, q)], init, prec)
+                err = np.max(np.abs(got - ref))
+                assert err < TOL[prec], (n, q, make.__name__, err)
+
+
+def test_sparse_gates_in_programs(cu, oracle):
+    """The gate-program path (graph replay, split precision on) routes sparse
+    5- and 6-qubit gates to the CSR kernel in exact FP32."""
+    from cast_simulator_b200.simulator import GateProgram, Stream
+
+    rng = np.random.default_rng(5)
+    n = 16
+    gates = [(_monomial(rng, 6), (0, 3, 5, 9, 12, 15)), (_block_sparse(rng, 5), (1, 2, 7, 8, 14)),
+             (haar(rng, 8), (4, 6, 10))]
+    init = oracle.random_state(n, 2)
+    ref = oracle.simulate(n, gates, init)
+    for split in (False, True):
+        prog = GateProgram(cu.CudaPrecision.F32, n, 1e-6, 1e-6, split)
+        for m, q in gates:
+            prog.add(m, q)
+        sv = cu.CudaStatevector(n, cu.CudaPrecision.F32)
+        sv.upload(init)
+        st = Stream()
+        prog.run(sv, st, use_graph=True)
+        st.sync()
+        assert np.max(np.abs(sv.download() - ref)) < 1e-5
+
+
 def test_sparse_entries_snapped(cu, oracle):
     """Scalars within ztol/K of 0 and otol/K of +-1 behave as exact 0 / +-1
     (cuda_gen.cpp:84-103): the GPU matches the oracle run on the snapped matrix."""
