@@ -331,9 +331,11 @@ __global__ void __launch_bounds__(kStagedThreads, 2) k_gate_staged(
 // store of a warp covers 32 consecutive groups of one row (coalesced for high
 // targets; for low ones L1 absorbs the gather).  The first nonzero of each of a
 // thread's rows is fetched before any arithmetic: a monomial gate keeps RPT
-// loads in flight a thread, as the dense register kernel does.  The CTA barrier
-// between the reads and the in-place writes keeps every group's inputs intact
-// until all its rows are computed.
+// loads in flight a thread, as the dense register kernel does.  The CSR table
+// and the 2^k member offsets are staged in shared memory once a CTA, so a row's
+// bookkeeping is broadcast shared loads.  The CTA barrier between the reads and
+// the in-place writes keeps every group's inputs intact until all its rows are
+// computed.
 template <typename T, int K> struct SparseShape {
   static constexpr int THREADS = 512;
   static constexpr int D = 1 << K;
@@ -346,11 +348,26 @@ template <typename T, int K> struct SparseShape {
 
 template <typename T, int K>
 __global__ void __launch_bounds__(SparseShape<T, K>::THREADS, 2) k_gate_sparse(
-    T *__restrict__ sv, uint64_t n_groups, Targets t, const typename Vec2<T>::type *__restrict__ vals,
-    const uint32_t *__restrict__ row_start, const uint32_t *__restrict__ cols) {
+    T *__restrict__ sv, uint64_t n_groups, Targets t, const typename Vec2<T>::type *__restrict__ g_vals,
+    const uint32_t *__restrict__ g_rows, const uint32_t *__restrict__ g_cols, uint32_t nnz) {
   using V = typename Vec2<T>::type;
   using Sh = SparseShape<T, K>;
-  constexpr int RPT = Sh::RPT, W = Sh::W, G = Sh::G;
+  constexpr int D = 1 << K, RPT = Sh::RPT, W = Sh::W, G = Sh::G;
+  // the CSR table and the member offsets, staged once a CTA (uniform reads)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V *vals = reinterpret_cast<V *>(smem_raw);
+  uint64_t *offs = reinterpret_cast<uint64_t *>(smem_raw + ((nnz * sizeof(V) + 15) & ~size_t(15)));
+  uint32_t *row_start = reinterpret_cast<uint32_t *>(offs + D);
+  uint32_t *cols = row_start + D + 1;
+  for (uint32_t i = threadIdx.x; i < nnz; i += Sh::THREADS) {
+    vals[i] = __ldg(&g_vals[i]);
+    cols[i] = __ldg(&g_cols[i]);
+  }
+  for (uint32_t i = threadIdx.x; i <= (uint32_t)D; i += Sh::THREADS) {
+    row_start[i] = __ldg(&g_rows[i]);
+    if (i < (uint32_t)D) offs[i] = member_offset<K>((int)i, t);
+  }
+  __syncthreads();
   V *psi = reinterpret_cast<V *>(sv);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int r0 = (w % W) * RPT;  // first row of this thread's chunk
@@ -361,21 +378,21 @@ __global__ void __launch_bounds__(SparseShape<T, K>::THREADS, 2) k_gate_sparse(
   V x0[RPT];
 #pragma unroll
   for (int i = 0; i < RPT; ++i) {
-    js[i] = __ldg(&row_start[r0 + i]);
-    je[i] = __ldg(&row_start[r0 + i + 1]);
-    if (live && js[i] < je[i]) x0[i] = psi[base + member_offset<K>((int)__ldg(&cols[js[i]]), t)];
+    js[i] = row_start[r0 + i];
+    je[i] = row_start[r0 + i + 1];
+    if (live && js[i] < je[i]) x0[i] = psi[base + offs[cols[js[i]]]];
   }
   T re[RPT], im[RPT];
 #pragma unroll
   for (int i = 0; i < RPT; ++i) {
     re[i] = im[i] = T(0);
     if (!live || js[i] >= je[i]) continue;
-    V m = __ldg(&vals[js[i]]);
+    V m = vals[js[i]];
     re[i] = fma(m.x, x0[i].x, -m.y * x0[i].y);
     im[i] = fma(m.x, x0[i].y, m.y * x0[i].x);
     for (uint32_t j = js[i] + 1; j < je[i]; ++j) {
-      m = __ldg(&vals[j]);
-      const V x = psi[base + member_offset<K>((int)__ldg(&cols[j]), t)];
+      m = vals[j];
+      const V x = psi[base + offs[cols[j]]];
       re[i] = fma(m.x, x.x, fma(-m.y, x.y, re[i]));
       im[i] = fma(m.x, x.y, fma(m.y, x.x, im[i]));
     }
@@ -387,9 +404,87 @@ __global__ void __launch_bounds__(SparseShape<T, K>::THREADS, 2) k_gate_sparse(
       V o;
       o.x = re[i];
       o.y = im[i];
-      psi[base + member_offset<K>(r0 + i, t)] = o;
+      psi[base + offs[r0 + i]] = o;
     }
   }
+}
+
+// Sparse gate with targets among the low qubits: the tile kernel's geometry
+// (tile_geometry, whole groups inside a tile of 2048 amplitudes) with the CSR
+// arithmetic.  The tile is copied in with cp.async; thread t computes tile
+// amplitudes t, t + 512, ...: row r = the target bits of the tile-local index,
+// inputs read from shared memory at the group base plus the tile-local member
+// offsets of the row's columns.  After a barrier the outputs go back into the
+// tile and the tile is stored coalesced.
+constexpr int kSparseTileThreads = 512;
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kSparseTileThreads) k_gate_sparse_tile(
+    T *__restrict__ sv, TileArgs a, const typename Vec2<T>::type *__restrict__ g_vals,
+    const uint32_t *__restrict__ g_rows, const uint32_t *__restrict__ g_cols, uint32_t nnz) {
+  using V = typename Vec2<T>::type;
+  constexpr int D = 1 << K;
+  constexpr uint32_t TILE = 1u << 11;
+  constexpr int OPT = TILE / kSparseTileThreads;  // outputs a thread
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V *tile = reinterpret_cast<V *>(smem_raw);
+  V *vals = tile + TILE;
+  uint32_t *offs = reinterpret_cast<uint32_t *>(smem_raw + sizeof(V) * TILE +
+                                                ((nnz * sizeof(V) + 15) & ~size_t(15)));
+  uint32_t *row_start = offs + D;
+  uint32_t *cols = row_start + D + 1;
+  V *psi = reinterpret_cast<V *>(sv);
+  const uint32_t low_mask = (1u << a.tb) - 1;
+  uint64_t tile_base = (uint64_t)blockIdx.x << a.tb;
+  for (uint32_t j = 0; j < a.k_hi; ++j)
+    tile_base = ((tile_base & ~a.hi_lo_mask[j]) << 1) | (tile_base & a.hi_lo_mask[j]);
+  for (uint32_t i = threadIdx.x; i < TILE; i += kSparseTileThreads)
+    __pipeline_memcpy_async(&tile[i], &psi[tile_base + a.chunk_off[i >> a.tb] + (i & low_mask)],
+                            sizeof(V));
+  __pipeline_commit();
+  uint32_t tmask = 0;  // tile-local target bits
+#pragma unroll
+  for (int b = 0; b < K; ++b) tmask |= a.loc_lo_mask[b] + 1;
+  for (uint32_t i = threadIdx.x; i < nnz; i += kSparseTileThreads) {
+    vals[i] = __ldg(&g_vals[i]);
+    cols[i] = __ldg(&g_cols[i]);
+  }
+  for (uint32_t i = threadIdx.x; i <= (uint32_t)D; i += kSparseTileThreads) {
+    row_start[i] = __ldg(&g_rows[i]);
+    if (i < (uint32_t)D) {
+      uint32_t o = 0;
+#pragma unroll
+      for (int b = 0; b < K; ++b)
+        if ((i >> b) & 1) o += a.loc_lo_mask[b] + 1;
+      offs[i] = o;
+    }
+  }
+  __pipeline_wait_prior(0);
+  __syncthreads();
+  V out[OPT];
+#pragma unroll
+  for (int u = 0; u < OPT; ++u) {
+    const uint32_t o = threadIdx.x + u * kSparseTileThreads;
+    uint32_t r = 0;
+#pragma unroll
+    for (int b = 0; b < K; ++b) r |= ((o & (a.loc_lo_mask[b] + 1)) != 0) << b;
+    const uint32_t gb = o & ~tmask;
+    T re = T(0), im = T(0);
+    for (uint32_t j = row_start[r]; j < row_start[r + 1]; ++j) {
+      const V m = vals[j];
+      const V x = tile[gb + offs[cols[j]]];
+      re = fma(m.x, x.x, fma(-m.y, x.y, re));
+      im = fma(m.x, x.y, fma(m.y, x.x, im));
+    }
+    out[u].x = re;
+    out[u].y = im;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < OPT; ++u) tile[threadIdx.x + u * kSparseTileThreads] = out[u];
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < TILE; i += kSparseTileThreads)
+    psi[tile_base + a.chunk_off[i >> a.tb] + (i & low_mask)] = tile[i];
 }
 
 // Device CSR table of a sparse gate: values (interleaved, the gate's
@@ -405,6 +500,12 @@ SparseLayout sparse_layout(uint32_t k, uint8_t precision, size_t nnz) {
   l.col_off = align16(l.row_off + sizeof(uint32_t) * ((1u << k) + 1));
   l.bytes = l.col_off + sizeof(uint32_t) * std::max<size_t>(nnz, 1);
   return l;
+}
+
+// Shared memory of the sparse kernel: values, member offsets, row starts, columns.
+size_t sparse_smem_bytes(uint32_t k, size_t v_bytes, uint32_t nnz) {
+  return ((nnz * v_bytes + 15) & ~size_t(15)) + sizeof(uint64_t) * (1u << k) +
+         sizeof(uint32_t) * ((1u << k) + 1 + nnz);
 }
 
 size_t gate_nnz(const GateData &g) {
@@ -458,16 +559,71 @@ bool launch_sparse(const GateData &g, void *sv, uint32_t n, const Targets &t, cu
     err = "statevector too large for the sparse gate kernel grid";
     return false;
   }
-  k_gate_sparse<T, K><<<(unsigned)blocks, SparseShape<T, K>::THREADS, 0, s>>>(
+  const uint32_t nnz = (uint32_t)gate_nnz(g);
+  const size_t smem = sparse_smem_bytes(K, sizeof(V), nnz);
+  static std::once_flag once;
+  static cudaError_t attr_rc = cudaSuccess;
+  std::call_once(once, [] {  // the largest table: 2^(2k) / 4 entries
+    attr_rc = cudaFuncSetAttribute(k_gate_sparse<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)sparse_smem_bytes(K, sizeof(V), 1u << (2 * K - 2)));
+  });
+  if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(sparse gate kernel)", err)) return false;
+  k_gate_sparse<T, K><<<(unsigned)blocks, SparseShape<T, K>::THREADS, smem, s>>>(
       static_cast<T *>(sv), n_groups, t, reinterpret_cast<const V *>(base),
       reinterpret_cast<const uint32_t *>(base + l.row_off),
-      reinterpret_cast<const uint32_t *>(base + l.col_off));
+      reinterpret_cast<const uint32_t *>(base + l.col_off), nnz);
   return cuda_ok(cudaGetLastError(), "sparse gate kernel launch", err);
 }
 
+bool tile_geometry(const GateData &g, uint32_t n, TileArgs &a);
+
+size_t sparse_tile_smem_bytes(uint32_t k, size_t v_bytes, uint32_t nnz) {
+  return v_bytes * 2048 + ((nnz * v_bytes + 15) & ~size_t(15)) +
+         sizeof(uint32_t) * (2 * (1u << k) + 1 + nnz);
+}
+
+template <typename T, int K>
+bool launch_sparse_tile(const GateData &g, void *sv, uint32_t n, const TileArgs &a, cudaStream_t s,
+                        std::string &err) {
+  using V = typename Vec2<T>::type;
+  const uint32_t nnz = (uint32_t)gate_nnz(g);
+  const SparseLayout l = sparse_layout(K, g.precision, nnz);
+  const char *base = static_cast<const char *>(g.d_sparse);
+  static std::once_flag once;
+  static cudaError_t attr_rc = cudaSuccess;
+  std::call_once(once, [] {  // the largest table: 2^(2k) / 4 entries
+    attr_rc = cudaFuncSetAttribute(k_gate_sparse_tile<T, K>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)sparse_tile_smem_bytes(K, sizeof(V), 1u << (2 * K - 2)));
+  });
+  if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(sparse tile kernel)", err)) return false;
+  const uint64_t n_tiles = 1ull << (n - 11);
+  k_gate_sparse_tile<T, K><<<(unsigned)n_tiles, kSparseTileThreads,
+                             sparse_tile_smem_bytes(K, sizeof(V), nnz), s>>>(
+      static_cast<T *>(sv), a, reinterpret_cast<const V *>(base),
+      reinterpret_cast<const uint32_t *>(base + l.row_off),
+      reinterpret_cast<const uint32_t *>(base + l.col_off), nnz);
+  return cuda_ok(cudaGetLastError(), "sparse tile kernel launch", err);
+}
+
+// Sparse gates with a target below qubit 5 run tiled (a warp's direct loads
+// would each gather from 32 groups 2^k amplitudes apart); the others read
+// global memory directly.
 template <typename T>
 bool launch_sparse_t(const GateData &g, void *sv, uint32_t n, const Targets &t, cudaStream_t s,
                      std::string &err) {
+  if (g.qubits[0] < 5) {
+    TileArgs a;
+    std::memset(&a, 0, sizeof(a));
+    if (tile_geometry(g, n, a)) {
+      switch (g.k) {
+      case 5: return launch_sparse_tile<T, 5>(g, sv, n, a, s, err);
+      case 6: return launch_sparse_tile<T, 6>(g, sv, n, a, s, err);
+      case 7: return launch_sparse_tile<T, 7>(g, sv, n, a, s, err);
+      default: break;
+      }
+    }
+  }
   switch (g.k) {
   case 5: return launch_sparse<T, 5>(g, sv, n, t, s, err);
   case 6: return launch_sparse<T, 6>(g, sv, n, t, s, err);
