@@ -42,8 +42,11 @@ import numpy as np
 
 from .fusion import FusionConfig, HardwareProfile, optimize_native
 
-MODES = ("f64", "f32", "tc")  # CUDA-core FP64 / FP32, split-BF16 tensor cores (complex64)
+# CUDA-core FP64 / FP32, split-BF16 tensor cores (complex64), and the sparse
+# (CSR) kernels that gates with k >= 5 and at most 2^k / 4 nonzeros a row take
+MODES = ("f64", "f32", "tc", "sf64", "sf32")
 TENSOR_KS = (5, 6)
+SPARSE_KS = (5, 6, 7)
 
 
 def haar(k: int, rng: np.random.Generator) -> np.ndarray:
@@ -51,6 +54,23 @@ def haar(k: int, rng: np.random.Generator) -> np.ndarray:
     z = rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))
     q, r = np.linalg.qr(z)
     return q * (np.diag(r) / np.abs(np.diag(r)))
+
+
+def monomial(k: int, rng: np.random.Generator) -> np.ndarray:
+    """A permutation with unit phases (one nonzero a row), the shape of fused
+    CX / phase blocks."""
+    d = 1 << k
+    m = np.zeros((d, d), dtype=complex)
+    m[np.arange(d), rng.permutation(d)] = np.exp(2j * np.pi * rng.random(d))
+    return m
+
+
+def is_sparse(matrix: np.ndarray, ztol: float = 1e-12) -> bool:
+    """Whether a gate runs on the sparse kernels: k >= 5 and at most 2^k / 4
+    nonzeros a row after the generator's snapping (|entry| < ztol / 2^k is zero)."""
+    d = matrix.shape[0]
+    k = d.bit_length() - 1
+    return k >= 5 and int((np.abs(matrix) >= ztol / d).sum()) * 4 <= d * d
 
 
 def dense_ai(k: int) -> float:
@@ -68,10 +88,13 @@ def time_gate(n: int, k: int, mode: str, low: bool = False, reps: int = 5, seed:
 
     if mode not in MODES:
         raise ValueError(f"mode must be one of {MODES}")
-    prec = CudaPrecision.F64 if mode == "f64" else CudaPrecision.F32
+    if mode.startswith("s") and k < 5:
+        raise ValueError("the sparse kernels take gates of 5 or more qubits")
+    prec = CudaPrecision.F64 if mode in ("f64", "sf64") else CudaPrecision.F32
     q = tuple(range(k)) if low else tuple(range(n - k, n))
     prog = GateProgram(prec, n, 1e-12, 1e-12, split_precision=(mode == "tc"))
-    prog.add(haar(k, np.random.default_rng(seed)), q)
+    rng = np.random.default_rng(seed)
+    prog.add(monomial(k, rng) if mode.startswith("s") else haar(k, rng), q)
     sv = CudaStatevector(n, prec)
     sv.zero()
     st = Stream()
@@ -169,18 +192,27 @@ class PassTable:
 
 
 def measure_pass_table(n: int, precision: str, ks=range(1, 8), tensor: bool = True,
-                       reps: int = 3) -> PassTable:
+                       reps: int = 3, sparse: bool = True) -> PassTable:
     tab = PassTable(n)
     for k in ks:
         tab.seconds[(k, precision)] = time_gate(n, k, precision, reps=reps)
     if tensor and precision == "f32":
         for k in TENSOR_KS:
             tab.seconds[(k, "tc")] = time_gate(n, k, "tc", reps=reps)
+    if sparse:
+        for k in SPARSE_KS:
+            if k in ks:
+                tab.seconds[(k, "s" + precision)] = time_gate(n, k, "s" + precision, reps=reps)
     return tab
 
 
-def engine_for(k: int, precision: str, split: bool) -> str:
-    """The kernel family a fused k-qubit gate runs on in a program."""
+def engine_for(k: int, precision: str, split: bool, sparse: bool = False) -> str:
+    """The kernel family a fused k-qubit gate runs on in a program: the sparse
+    kernels for sparse gates of 5 or more qubits (in either precision mode),
+    else the tensor cores for 5- and 6-qubit gates of split-precision complex64
+    programs, else the CUDA-core kernels."""
+    if sparse and k in SPARSE_KS:
+        return "s" + precision
     return "tc" if split and precision == "f32" and k in TENSOR_KS else precision
 
 
@@ -197,13 +229,15 @@ def choose_fusion(n: int, gates, precision: str, table: PassTable, ks=range(2, 7
     """Fuse ``gates`` at each width in ``ks`` (size-only cost, the reference's
     default) and predict the circuit time from ``table``; returns the width and
     engine (CUDA cores, or tensor cores for 5- and 6-qubit gates) with the least
-    predicted time."""
+    predicted time.  Sparse fused gates are priced at the sparse kernels' pass
+    time (the table's "sf64" / "sf32" entries)."""
     cands = []
     splits = (False, True) if (allow_tensor and precision == "f32") else (False,)
     for k in ks:
         fused = optimize_native(n, gates, FusionConfig.size_only(k)).gates()
         for split in splits:
-            t = sum(table.predict(g.n_qubits(), engine_for(g.n_qubits(), precision, split), n)
+            t = sum(table.predict(g.n_qubits(),
+                                  engine_for(g.n_qubits(), precision, split, is_sparse(g.matrix())), n)
                     for g in fused)
             cands.append({"fusion_k": k, "split_precision": split, "fused_gates": len(fused),
                           "predicted_s": t})

@@ -3,6 +3,8 @@
 choice from a pass-time table."""
 import math
 
+import numpy as np
+
 import pytest
 
 from cast_simulator_b200 import autotune as A
@@ -42,6 +44,44 @@ def test_engine_for():
     assert A.engine_for(4, "f32", True) == "f32"
     assert A.engine_for(6, "f64", True) == "f64"
     assert A.engine_for(6, "f32", False) == "f32"
+
+
+def test_engine_for_sparse_gates():
+    assert A.engine_for(6, "f64", False, sparse=True) == "sf64"
+    assert A.engine_for(6, "f32", True, sparse=True) == "sf32"  # ahead of the tensor cores
+    assert A.engine_for(4, "f32", True, sparse=True) == "f32"   # dense kernels below k = 5
+
+
+def test_is_sparse_rule():
+    rng = np.random.default_rng(0)
+    assert A.is_sparse(A.monomial(5, rng))
+    assert not A.is_sparse(A.monomial(4, rng))  # k < 5
+    assert not A.is_sparse(A.haar(5, rng))
+    blk = np.kron(np.eye(16), A.haar(2, rng))   # 4 nonzeros a row of 64
+    assert A.is_sparse(blk)
+    edge = np.kron(np.eye(4), A.haar(4, rng))   # 16 nonzeros a row of 64: the limit
+    assert A.is_sparse(edge)
+    dense = np.kron(np.eye(2), A.haar(5, rng))  # 32 nonzeros a row of 64
+    assert not A.is_sparse(dense)
+    tiny = A.monomial(5, rng) + 1e-16           # below ztol / 2^k: snapped to zero
+    assert A.is_sparse(tiny)
+
+
+def test_choose_fusion_prices_sparse_gates(cblib):
+    """QFT-CX fuses into sparse blocks: with cheap sparse passes and dense wide
+    passes priced high, the chooser still fuses wide."""
+    from cast_simulator_b200.types import QuantumCircuit
+
+    n = 14
+    gates = QuantumCircuit.qft_cx(n).gates()
+    tab = {(k, "f64"): 1.0 if k <= 4 else 3.0 for k in range(1, 8)}
+    tab.update({(k, "sf64"): 1.1 for k in (5, 6, 7)})
+    ch = A.choose_fusion(n, gates, "f64", A.PassTable(n, tab), ks=range(2, 7))
+    assert ch.fusion_k >= 5
+    without = A.choose_fusion(n, gates, "f64",
+                              A.PassTable(n, {**tab, **{(k, "sf64"): 50.0 for k in (5, 6, 7)}}),
+                              ks=range(2, 7))
+    assert without.fusion_k <= 4
 
 
 def _brickwork(n, depth):
