@@ -122,7 +122,7 @@ class Probe:
 
 def probe(n: int, k: int, mode: str, reps: int = 3) -> Probe:
     t = time_gate(n, k, mode, reps=reps)
-    scalar = 8 if mode == "f64" else 4
+    scalar = 8 if mode in ("f64", "sf64") else 4
     sv_bytes = (1 << n) * 2 * scalar
     ai = dense_ai(k)
     return Probe(k, mode, ai, t, ai * (1 << n) * 2.0 / t / 1e9, 2.0 * sv_bytes / t / (1 << 30))
@@ -318,7 +318,7 @@ def _main(argv=None) -> None:
                           "traj_per_s": ch.traj_per_s, "candidates": ch.candidates}))
     elif a.cmd == "gate":
         t = time_gate(a.n, a.k, a.mode, a.low, a.reps)
-        b = 2 * (1 << a.n) * (16 if a.mode == "f64" else 8)
+        b = 2 * (1 << a.n) * (16 if a.mode in ("f64", "sf64") else 8)
         print(json.dumps({"k": a.k, "n": a.n, "mode": a.mode, "low_targets": a.low,
                           "ms": t * 1e3, "gb_s": b / t / 1e9}))
     elif a.cmd == "profile":
