@@ -128,6 +128,25 @@ def test_sparse_gates_all_placements(cu, oracle, prec, k):
                 assert err < TOL[prec], (n, q, make.__name__, err)
 
 
+@pytest.mark.parametrize("prec", [1, 0])
+def test_sparse_gates_with_empty_rows(cu, oracle, prec):
+    """Non-unitary sparse matrices (a projector on one wire of a 5-qubit block,
+    and the zero matrix): rows without nonzeros write exact zeros, in both the
+    direct (high targets) and the tiled (low targets) CSR kernels."""
+    rng = np.random.default_rng(17)
+    proj = np.kron(np.eye(16), np.diag([1.0, 0.0])).astype(complex)  # rows of |1> on wire 0 empty
+    zero = np.zeros((32, 32), dtype=complex)
+    n = 13
+    for m in (proj, zero):
+        for q in ((0, 1, 2, 3, 4), (8, 9, 10, 11, 12)):
+            init = oracle.random_state(n, int(rng.integers(100)))
+            ref = init.copy()
+            oracle.apply_gate(ref, m, q)
+            got = run_gates(cu, n, [_G(m, q)], init, prec)
+            assert np.max(np.abs(got - ref)) < TOL[prec], q
+            assert np.all(got[ref == 0] == 0)
+
+
 def test_sparse_gates_in_programs(cu, oracle):
     """The gate-program path (graph replay, split precision on) routes sparse
     5- and 6-qubit gates to the CSR kernel in exact FP32."""
