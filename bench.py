@@ -381,9 +381,10 @@ def serving_leg(n_req: int):
     half complex64 / half complex128, 20% noisy; p50/p99 latency and circuits/s
     at two arrival rates, against a sequential FIFO of plain-path service times
     (per-gate C-ABI launches; noisy requests scaled from 8 host-driven
-    trajectories).  One unmeasured pass of the stream goes first: the first
-    launch of each kernel loads its module, which would otherwise land on the
-    first measured requests."""
+    trajectories).  One unmeasured pass of the stream goes first, so that
+    first-use costs (kernel module loading on first launch, first allocations
+    of each statevector size, trajectory workspaces) do not land on the first
+    measured requests."""
     from cast_simulator_b200 import serving as S
 
     out = {"requests": n_req, "rates": [], "warmup": "one unmeasured pass of the 160 Hz stream"}
