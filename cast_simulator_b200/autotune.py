@@ -29,6 +29,7 @@ Command line:
     python -m cast_simulator_b200.autotune gate --k 6 --n 26 --mode tc [--low]
     python -m cast_simulator_b200.autotune profile --n 26 --precision f32 [--out prof.json]
     python -m cast_simulator_b200.autotune choose --n 30 --depth 20 --precision f32
+    python -m cast_simulator_b200.autotune choose --circuit qft --n 30 --precision f64
     python -m cast_simulator_b200.autotune traj --n 16 --depth 30
 """
 from __future__ import annotations
@@ -297,9 +298,10 @@ def _main(argv=None) -> None:
     p.add_argument("--n", type=int, default=26)
     p.add_argument("--precision", choices=("f64", "f32"), default="f32")
     p.add_argument("--out")
-    c = sub.add_parser("choose", help="fusion width / engine for a brickwork circuit")
+    c = sub.add_parser("choose", help="fusion width / engine for a brickwork or QFT-CX circuit")
+    c.add_argument("--circuit", choices=("brickwork", "qft"), default="brickwork")
     c.add_argument("--n", type=int, default=30)
-    c.add_argument("--depth", type=int, default=20)
+    c.add_argument("--depth", type=int, default=20, help="brickwork depth")
     c.add_argument("--precision", choices=("f64", "f32"), default="f32")
     c.add_argument("--profile-n", type=int, default=26)
     t = sub.add_parser("traj", help="fusion width / launch shape for noisy brickwork trajectories")
@@ -332,7 +334,8 @@ def _main(argv=None) -> None:
     else:
         from .types import QuantumCircuit
 
-        circ = QuantumCircuit.brickwork(a.n, a.depth, 2024)
+        circ = (QuantumCircuit.brickwork(a.n, a.depth, 2024) if a.circuit == "brickwork"
+                else QuantumCircuit.qft_cx(a.n))
         tab = measure_pass_table(a.profile_n, a.precision)
         ch = choose_fusion(a.n, circ.gates(), a.precision, tab)
         print(json.dumps({"fusion_k": ch.fusion_k, "split_precision": ch.split_precision,
