@@ -418,13 +418,13 @@ __global__ void __launch_bounds__(SparseShape<T, K>::THREADS, 2) k_gate_sparse(
 // tile and the tile is stored coalesced.
 constexpr int kSparseTileThreads = 512;
 
-template <typename T, int K>
+template <typename T, int K, int TB>
 __global__ void __launch_bounds__(kSparseTileThreads) k_gate_sparse_tile(
     T *__restrict__ sv, TileArgs a, const typename Vec2<T>::type *__restrict__ g_vals,
     const uint32_t *__restrict__ g_rows, const uint32_t *__restrict__ g_cols, uint32_t nnz) {
   using V = typename Vec2<T>::type;
   constexpr int D = 1 << K;
-  constexpr uint32_t TILE = 1u << 11;
+  constexpr uint32_t TILE = 1u << TB;
   constexpr int OPT = TILE / kSparseTileThreads;  // outputs a thread
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V *tile = reinterpret_cast<V *>(smem_raw);
@@ -575,10 +575,13 @@ bool launch_sparse(const GateData &g, void *sv, uint32_t n, const Targets &t, cu
   return cuda_ok(cudaGetLastError(), "sparse gate kernel launch", err);
 }
 
-bool tile_geometry(const GateData &g, uint32_t n, TileArgs &a);
+bool tile_geometry(const GateData &g, uint32_t n, TileArgs &a, uint32_t target);
 
-size_t sparse_tile_smem_bytes(uint32_t k, size_t v_bytes, uint32_t nnz) {
-  return v_bytes * 2048 + ((nnz * v_bytes + 15) & ~size_t(15)) +
+// Tile of the sparse tile kernel: 4096 amplitudes in FP32 (32 KB), 2048 in FP64.
+template <typename T> constexpr uint32_t sparse_tile_bits() { return sizeof(T) == 4 ? 12u : 11u; }
+
+size_t sparse_tile_smem_bytes(uint32_t k, size_t v_bytes, uint32_t nnz, uint32_t tb) {
+  return (v_bytes << tb) + ((nnz * v_bytes + 15) & ~size_t(15)) +
          sizeof(uint32_t) * (2 * (1u << k) + 1 + nnz);
 }
 
@@ -589,17 +592,18 @@ bool launch_sparse_tile(const GateData &g, void *sv, uint32_t n, const TileArgs 
   const uint32_t nnz = (uint32_t)gate_nnz(g);
   const SparseLayout l = sparse_layout(K, g.precision, nnz);
   const char *base = static_cast<const char *>(g.d_sparse);
+  constexpr uint32_t TB = sparse_tile_bits<T>();
   static std::once_flag once;
   static cudaError_t attr_rc = cudaSuccess;
   std::call_once(once, [] {  // the largest table: 2^(2k) / 4 entries
-    attr_rc = cudaFuncSetAttribute(k_gate_sparse_tile<T, K>,
+    attr_rc = cudaFuncSetAttribute(k_gate_sparse_tile<T, K, TB>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)sparse_tile_smem_bytes(K, sizeof(V), 1u << (2 * K - 2)));
+                                   (int)sparse_tile_smem_bytes(K, sizeof(V), 1u << (2 * K - 2), TB));
   });
   if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(sparse tile kernel)", err)) return false;
-  const uint64_t n_tiles = 1ull << (n - 11);
-  k_gate_sparse_tile<T, K><<<(unsigned)n_tiles, kSparseTileThreads,
-                             sparse_tile_smem_bytes(K, sizeof(V), nnz), s>>>(
+  const uint64_t n_tiles = 1ull << (n - TB);
+  k_gate_sparse_tile<T, K, TB><<<(unsigned)n_tiles, kSparseTileThreads,
+                                 sparse_tile_smem_bytes(K, sizeof(V), nnz, TB), s>>>(
       static_cast<T *>(sv), a, reinterpret_cast<const V *>(base),
       reinterpret_cast<const uint32_t *>(base + l.row_off),
       reinterpret_cast<const uint32_t *>(base + l.col_off), nnz);
@@ -615,7 +619,7 @@ bool launch_sparse_t(const GateData &g, void *sv, uint32_t n, const Targets &t, 
   if (g.qubits[0] < 5) {
     TileArgs a;
     std::memset(&a, 0, sizeof(a));
-    if (tile_geometry(g, n, a)) {
+    if (tile_geometry(g, n, a, sparse_tile_bits<T>())) {
       switch (g.k) {
       case 5: return launch_sparse_tile<T, 5>(g, sv, n, a, s, err);
       case 6: return launch_sparse_tile<T, 6>(g, sv, n, a, s, err);
@@ -633,8 +637,7 @@ bool launch_sparse_t(const GateData &g, void *sv, uint32_t n, const Targets &t, 
 }
 
 // Tile geometry for a gate: returns false when the tile kernel does not apply.
-bool tile_geometry(const GateData &g, uint32_t n, TileArgs &a) {
-  const uint32_t target = tile_bits(g.k);
+bool tile_geometry(const GateData &g, uint32_t n, TileArgs &a, uint32_t target) {
   if (n < target) return false;
   uint32_t need = 0;  // every target below 5 must sit inside a chunk
   for (uint32_t b = 0; b < g.k; ++b)
@@ -762,7 +765,7 @@ bool try_tile(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::stri
   if (ov == 2 && low_bits == 0) return true;
   TileArgs a;
   std::memset(&a, 0, sizeof(a));
-  if (!tile_geometry(g, n, a)) return true;
+  if (!tile_geometry(g, n, a, tile_bits(g.k))) return true;
   done = true;
   switch (g.k) {
   case 1: return launch_tile<T, 1>(g, sv, n, a, s, err);
