@@ -133,6 +133,27 @@ int cast_b200_set_device(int device, char *err_buf, size_t err_buf_len) {
 
 int cast_b200_set_gate_path(int path) { return cb2::set_gate_path(path); }
 
+int cast_b200_gate_engine(uint8_t precision, uint32_t sv_n_qubits, const cast_complex64_t *matrix,
+                          const uint32_t *qubits, uint32_t n_gate_qubits, double ztol,
+                          double otol, int split, char *err_buf, size_t err_buf_len) {
+  try {
+    GateData g;
+    std::string err;
+    if (!make_gate(precision, matrix, qubits, n_gate_qubits, ztol, otol, g, err) ||
+        !cb2::check_gate(g, sv_n_qubits, err)) {
+      write_err(err_buf, err_buf_len, err);
+      return -1;
+    }
+    const bool sparse = cb2::sparse_gate(g);
+    const bool tensor = !sparse && split && cb2::tensor_path_supported(g);
+    clear_err(err_buf, err_buf_len);
+    return cb2::gate_engine(g, sv_n_qubits, tensor, sparse);
+  } catch (const std::exception &ex) {
+    write_err(err_buf, err_buf_len, ex.what());
+    return -1;
+  }
+}
+
 int cast_b200_apply_gate(uint64_t sv_dptr, uint32_t sv_n_qubits, uint8_t precision,
                          const cast_complex64_t *matrix, const uint32_t *qubits,
                          uint32_t n_gate_qubits, double ztol, double otol, void *stream,

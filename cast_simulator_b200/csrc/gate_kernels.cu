@@ -613,13 +613,18 @@ bool launch_sparse_tile(const GateData &g, void *sv, uint32_t n, const TileArgs 
 // Sparse gates with a target below qubit 5 run tiled (a warp's direct loads
 // would each gather from 32 groups 2^k amplitudes apart); the others read
 // global memory directly.
+bool sparse_tile_chosen(const GateData &g, uint32_t n, TileArgs &a) {
+  if (g.qubits[0] >= 5) return false;
+  std::memset(&a, 0, sizeof(a));
+  return tile_geometry(g, n, a, g.precision == 1 ? sparse_tile_bits<double>() : sparse_tile_bits<float>());
+}
+
 template <typename T>
 bool launch_sparse_t(const GateData &g, void *sv, uint32_t n, const Targets &t, cudaStream_t s,
                      std::string &err) {
-  if (g.qubits[0] < 5) {
+  {
     TileArgs a;
-    std::memset(&a, 0, sizeof(a));
-    if (tile_geometry(g, n, a, sparse_tile_bits<T>())) {
+    if (sparse_tile_chosen(g, n, a)) {
       switch (g.k) {
       case 5: return launch_sparse_tile<T, 5>(g, sv, n, a, s, err);
       case 6: return launch_sparse_tile<T, 6>(g, sv, n, a, s, err);
@@ -738,14 +743,8 @@ std::atomic<int> g_gate_path{[] {
 
 int gate_path_override() { return g_gate_path.load(std::memory_order_relaxed); }
 
-template <typename T>
-bool try_tile(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::string &err,
-              bool &done) {
-  done = false;
-  if (g.k > 4) return true;
-  const int ov = gate_path_override();
-  if (ov == 1) return true;
-  // Measured on B200 (30 qubits, every placement of k = 1..4 with low
+// Whether a dense gate of k <= 4 runs on the tile kernel (fills `a` when it
+// does).  Measured on B200 (30 qubits, every placement of k = 1..4 with low
   // targets): the register kernel loses bandwidth when a warp's loads of one
   // member touch many cache lines for a few bytes each and the lines do not
   // survive in L1 until the group's other members are loaded.  FP64: the tile
@@ -754,6 +753,10 @@ bool try_tile(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::stri
   // with targets 0 and 1 (register kernel 2.0-4.2 TB/s), or with the lowest
   // target 1 and three targets below 5 (k = 3 on 1..3: 6.0 against 4.1);
   // elsewhere the register kernel is faster (k = 3 on 2..4: 6.4 against 6.0).
+bool tile_chosen(const GateData &g, uint32_t n, TileArgs &a) {
+  if (g.k > 4) return false;
+  const int ov = gate_path_override();
+  if (ov == 1) return false;
   uint32_t low_bits = 0;
   for (uint32_t b = 0; b < g.k; ++b)
     if (g.qubits[b] < 5) low_bits |= 1u << g.qubits[b];
@@ -761,11 +764,18 @@ bool try_tile(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::stri
   const bool tile_wins = g.precision == 1
                              ? n_low >= 2
                              : ((low_bits & 0x3u) == 0x3u || (g.qubits[0] == 1 && n_low >= 3));
-  if (ov != 2 && !tile_wins) return true;
-  if (ov == 2 && low_bits == 0) return true;
-  TileArgs a;
+  if (ov != 2 && !tile_wins) return false;
+  if (ov == 2 && low_bits == 0) return false;
   std::memset(&a, 0, sizeof(a));
-  if (!tile_geometry(g, n, a, tile_bits(g.k))) return true;
+  return tile_geometry(g, n, a, tile_bits(g.k));
+}
+
+template <typename T>
+bool try_tile(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::string &err,
+              bool &done) {
+  done = false;
+  TileArgs a;
+  if (!tile_chosen(g, n, a)) return true;
   done = true;
   switch (g.k) {
   case 1: return launch_tile<T, 1>(g, sv, n, a, s, err);
@@ -860,6 +870,14 @@ bool launch_gate(const GateData &g, void *sv, uint32_t n, cudaStream_t stream, s
                             : launch_sparse_t<float>(g, sv, n, t, stream, err);
   return g.precision == 1 ? launch_t<double>(g, sv, n, t, stream, err)
                           : launch_t<float>(g, sv, n, t, stream, err);
+}
+
+int gate_engine(const GateData &g, uint32_t n, bool tensor, bool sparse) {
+  if (tensor) return kEngineTensor;
+  TileArgs a;
+  if (sparse) return sparse_tile_chosen(g, n, a) ? kEngineSparseTile : kEngineSparse;
+  if (tile_chosen(g, n, a)) return kEngineTile;
+  return g.k >= 6 ? kEngineStaged : kEngineRegister;
 }
 
 // Only from k = 5: below that the dense kernels are bound by HBM, not the FMA

@@ -54,6 +54,14 @@ bool launch_gate(const GateData &g, void *sv, uint32_t n, cudaStream_t stream, s
 // snapping) run on the CSR kernel instead of the dense ones; upload_sparse
 // fills g.d_sparse.  free_gate_device releases every device copy of a gate.
 bool sparse_gate(const GateData &g);
+
+// The kernel family a gate runs on (the same decisions launch_gate takes):
+// `tensor` = the gate carries a tensor-core operand, `sparse` = a CSR table.
+enum : int {
+  kEngineRegister = 0, kEngineTile = 1, kEngineStaged = 2, kEngineSparse = 3,
+  kEngineSparseTile = 4, kEngineTensor = 5
+};
+int gate_engine(const GateData &g, uint32_t n, bool tensor, bool sparse);
 bool upload_sparse(GateData &g, std::string &err);
 void free_gate_device(GateData &g);
 

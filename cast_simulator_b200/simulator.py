@@ -134,6 +134,29 @@ def tensor_status() -> int:
     return out.value
 
 
+ENGINES = ("register", "tile", "staged", "sparse", "sparse_tile", "tensor")
+
+
+def gate_engine(matrix: np.ndarray, qubits, n_qubits: int, precision: CudaPrecision,
+                split_precision: bool = False, ztol: float = 1e-12, otol: float = 1e-12) -> str:
+    """The kernel family a gate would run on in a gate program of ``n_qubits``
+    (one of ``ENGINES``), decided by the library exactly as a launch decides
+    it, without touching the device."""
+    from .types import _canonicalize
+
+    m, qs = _canonicalize(np.asarray(matrix, dtype=np.complex128), list(qubits))
+    m = np.ascontiguousarray(m)
+    q = np.ascontiguousarray(qs, dtype=np.uint32)
+    eb = L.errbuf()
+    e = L.lib().cast_b200_gate_engine(int(precision), n_qubits,
+                                      m.view(np.float64).ctypes.data_as(C.POINTER(L.Complex64)),
+                                      q.ctypes.data_as(L.c_u32p), q.size, ztol, otol,
+                                      int(split_precision), eb, L.ERR_LEN)
+    if e < 0:
+        raise RuntimeError(f"gate_engine failed: {eb.value.decode()}")
+    return ENGINES[e]
+
+
 def inner_product(a: CudaStatevector, b: CudaStatevector, stream: Stream | None = None) -> complex:
     if a.n_qubits() != b.n_qubits() or a.precision() != b.precision():
         raise ValueError("statevector size/precision mismatch")

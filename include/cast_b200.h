@@ -48,12 +48,23 @@ int cast_b200_set_gate_path(int path);
  * Snap (ztol/otol scaled by 1/2^k, as cuda_gen.cpp:84-103) and apply one gate
  * in place on `stream`.  Takes over the compile -> load -> launch sequence of
  * CudaKernelManager::{generate,apply} (src/cuda/kernel.rs:778-924) for callers
- * that hold the matrix as data.  k <= 7; for k >= 6 the matrix is staged in a
- * device buffer owned by the library, so the call is synchronous. */
+ * that hold the matrix as data.  k <= 7; for k >= 6, and for sparse gates, the
+ * matrix is staged in a device buffer owned by the library, so the call is
+ * synchronous. */
 int cast_b200_apply_gate(uint64_t sv_dptr, uint32_t sv_n_qubits, uint8_t precision,
                          const cast_complex64_t *matrix, const uint32_t *qubits,
                          uint32_t n_gate_qubits, double ztol, double otol, void *stream,
                          char *err_buf, size_t err_buf_len);
+
+/* The kernel family a gate would run on in a program (split = the program's
+ * split-precision mode), decided exactly as a launch decides it; touches no
+ * device.  0 register kernel, 1 tile kernel (low targets), 2 staged wide-gate
+ * kernel, 3 sparse CSR kernel, 4 tiled sparse CSR kernel, 5 tcgen05 tensor
+ * path; -1 on an invalid gate (message in err_buf).  No counterpart in the
+ * reference, whose generator emits one kernel per gate. */
+int cast_b200_gate_engine(uint8_t precision, uint32_t sv_n_qubits, const cast_complex64_t *matrix,
+                          const uint32_t *qubits, uint32_t n_gate_qubits, double ztol,
+                          double otol, int split, char *err_buf, size_t err_buf_len);
 
 /* -- Gate programs ---------------------------------------------------------------
  * An ordered list of gates for one statevector size and precision, uploaded

@@ -109,3 +109,51 @@ def test_trajectory_threads_setting(cblib):
         assert cblib.cast_b200_traj_set_launch(None, 512, 0, eb, L.ERR_LEN) == 1
     finally:
         cblib.cast_b200_traj_destroy(prog)
+
+
+def test_gate_engine_routing(cblib):
+    """Kernel routing is a pure host decision, the same one a launch takes: dense
+    gates by width and low targets, sparse gates (at most 2^k / 4 nonzeros a row,
+    k >= 5) on the CSR kernels, split-precision complex64 k = 5, 6 on the tensor
+    cores."""
+    from cast_simulator_b200.cuda import CudaPrecision as P
+    from cast_simulator_b200.simulator import gate_engine
+
+    rng = np.random.default_rng(3)
+
+    def haar(k):
+        z = rng.standard_normal((1 << k, 1 << k)) + 1j * rng.standard_normal((1 << k, 1 << k))
+        return np.linalg.qr(z)[0]
+
+    def mono(k):
+        d = 1 << k
+        m = np.zeros((d, d), dtype=complex)
+        m[np.arange(d), rng.permutation(d)] = 1.0
+        return m
+
+    F64, F32 = P.F64, P.F32
+    assert gate_engine(haar(4), (16, 17, 18, 19), 20, F64) == "register"
+    assert gate_engine(haar(4), (0, 1, 2, 3), 20, F64) == "tile"
+    assert gate_engine(haar(4), (0, 1, 2, 3), 10, F64) == "register"  # no 2048-amplitude tile
+    assert gate_engine(haar(3), (0, 1, 2), 12, F64) == "tile"          # 4096-amplitude tile
+    assert gate_engine(haar(3), (0, 1, 2), 11, F64) == "register"
+    assert gate_engine(haar(3), (1, 2, 3), 20, F32) == "tile"
+    assert gate_engine(haar(3), (2, 3, 4), 20, F32) == "register"
+    assert gate_engine(haar(2), (0, 9), 20, F64) == "register"          # one low target
+    assert gate_engine(haar(5), (10, 11, 12, 13, 14), 20, F64) == "register"
+    assert gate_engine(haar(6), tuple(range(10, 16)), 20, F64) == "staged"
+    assert gate_engine(mono(6), tuple(range(10, 16)), 20, F64) == "sparse"
+    assert gate_engine(mono(6), tuple(range(6)), 20, F64) == "sparse_tile"
+    assert gate_engine(mono(6), tuple(range(6)), 10, F64) == "sparse"
+    assert gate_engine(mono(6), tuple(range(6)), 11, F32) == "sparse"    # FP32 tile: 4096
+    assert gate_engine(mono(6), tuple(range(6)), 12, F32) == "sparse_tile"
+    assert gate_engine(mono(4), tuple(range(4)), 20, F64) == "tile"      # sparse only from k = 5
+    assert gate_engine(haar(6), tuple(range(10, 16)), 20, F32, split_precision=True) == "tensor"
+    assert gate_engine(haar(5), (0, 2, 4, 6, 8), 20, F32, split_precision=True) == "tensor"
+    assert gate_engine(mono(6), tuple(range(10, 16)), 20, F32, split_precision=True) == "sparse"
+    assert gate_engine(haar(6), tuple(range(10, 16)), 20, F64, split_precision=True) == "staged"
+    assert gate_engine(haar(4), (0, 1, 2, 3), 20, F32, split_precision=True) == "tile"
+    # unsorted qubits are canonicalised like every other entry point
+    assert gate_engine(mono(6), (15, 10, 11, 12, 13, 14), 20, F64) == "sparse"
+    with pytest.raises(RuntimeError, match="outside"):
+        gate_engine(haar(2), (0, 25), 20, F64)
