@@ -230,15 +230,23 @@ def choose_fusion(n: int, gates, precision: str, table: PassTable, ks=range(2, 7
     """Fuse ``gates`` at each width in ``ks`` (size-only cost, the reference's
     default) and predict the circuit time from ``table``; returns the width and
     engine (CUDA cores, or tensor cores for 5- and 6-qubit gates) with the least
-    predicted time.  Sparse fused gates are priced at the sparse kernels' pass
-    time (the table's "sf64" / "sf32" entries)."""
+    predicted time.  Each fused gate is priced at the pass time of the kernel
+    family the library routes it to (``simulator.gate_engine``): sparse gates at
+    the table's "sf64" / "sf32" entries, split-precision tensor gates at "tc"."""
+    from .cuda import CudaPrecision
+    from .simulator import gate_engine
+
+    prec = CudaPrecision.F64 if precision == "f64" else CudaPrecision.F32
+    mode_of = {"sparse": "s" + precision, "sparse_tile": "s" + precision, "tensor": "tc"}
     cands = []
     splits = (False, True) if (allow_tensor and precision == "f32") else (False,)
     for k in ks:
         fused = optimize_native(n, gates, FusionConfig.size_only(k)).gates()
         for split in splits:
+            # the library's own routing decides each gate's kernel family
             t = sum(table.predict(g.n_qubits(),
-                                  engine_for(g.n_qubits(), precision, split, is_sparse(g.matrix())), n)
+                                  mode_of.get(gate_engine(g.matrix(), g.qubits(), n, prec, split),
+                                              precision), n)
                     for g in fused)
             cands.append({"fusion_k": k, "split_precision": split, "fused_gates": len(fused),
                           "predicted_s": t})
