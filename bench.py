@@ -291,8 +291,13 @@ def qft_leg(n: int = 22, seed: int = 7):
     _, sv_u = _run_fused(n, circ.gates(), cu.CudaPrecision.F64, initial=init, reps=1)
     ref = sv_u.download()
     passes = len(fused)
+    from collections import Counter
+
+    from cast_simulator_b200.simulator import gate_engine
+
+    engines = Counter(gate_engine(g.matrix(), g.qubits(), n, cu.CudaPrecision.F64) for g in fused)
     return {"workload": f"qft-cx-{n}q-c128-default-fusion", "unfused_gates": len(circ),
-            "fused_gates": passes, "ms": t * 1e3,
+            "fused_gates": passes, "engines": dict(engines), "ms": t * 1e3,
             "hbm_gbs": passes * 2 * (1 << n) * 16 / t / 1e9,
             "gates_amps_per_s": len(circ) * (1 << n) / t,
             "max_abs_diff_vs_unfused": float(np.max(np.abs(got - ref)))}
