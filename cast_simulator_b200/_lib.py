@@ -149,6 +149,13 @@ CAST_B200 = [
     ("cast_b200_traj_add_channel", C.c_int,
      [C.c_void_p, C.c_uint32, C.POINTER(Complex64), C.c_uint32, C.c_char_p, C.c_size_t]),
     ("cast_b200_traj_num_ops", C.c_uint32, [C.c_void_p]),
+    ("cast_b200_traj_num_qubits", C.c_uint32, [C.c_void_p]),
+    ("cast_b200_traj_build", C.c_int,
+     [C.c_void_p, C.c_uint32, c_u32p, c_u32p, c_u32p, C.POINTER(Complex64), c_u32p, c_dp, C.c_uint32,
+      c_u32p, C.c_char_p, C.c_size_t]),
+    ("cast_b200_traj_get_op", C.c_int,
+     [C.c_void_p, C.c_uint32, c_u32p, c_u32p, c_u32p, c_dp, c_u32p, c_u32p, C.POINTER(Complex64),
+      C.c_size_t]),
     ("cast_b200_gate_engine", C.c_int,
      [C.c_uint8, C.c_uint32, C.POINTER(Complex64), c_u32p, C.c_uint32, C.c_double, C.c_double,
       C.c_int, C.c_char_p, C.c_size_t]),

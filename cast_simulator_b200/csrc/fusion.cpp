@@ -18,8 +18,12 @@
 #include <cmath>
 #include <complex>
 #include <exception>
+#include <map>
 #include <memory>
 #include <set>
+#include <stdexcept>
+#include <string>
+#include <tuple>
 #include <unordered_set>
 #include <vector>
 
@@ -30,6 +34,7 @@ using cd = std::complex<double>;
 struct HGate {
   std::vector<uint32_t> q;  // ascending
   std::vector<cd> m;        // row-major 2^k x 2^k
+  std::vector<int> prov;    // source gates in application order (trajectory builder)
   uint32_t k() const { return (uint32_t)q.size(); }
 };
 using GatePtr = std::shared_ptr<const HGate>;
@@ -60,6 +65,8 @@ std::vector<cd> expand(const HGate &g, const std::vector<uint32_t> &uq) {
 // QuantumGate::matmul (unitary part): self * other on the union (gate.rs:280-284, 319)
 GatePtr matmul(const HGate &a, const HGate &b) {
   auto g = std::make_shared<HGate>();
+  g->prov = b.prov;  // b acts first
+  g->prov.insert(g->prov.end(), a.prov.begin(), a.prov.end());
   std::set_union(a.q.begin(), a.q.end(), b.q.begin(), b.q.end(), std::back_inserter(g->q));
   const size_t d = 1ull << g->q.size();
   const std::vector<cd> ea = expand(a, g->q), eb = expand(b, g->q);
@@ -329,6 +336,224 @@ size_t gate_fusion_pass(Graph &g, const Cost &cost, double margin, uint32_t cdd)
   return nf;
 }
 
+// ── trajectory-program construction ─────────────────────────────────────────
+// The host half of the batched trajectories, natively: the same program the
+// Python builder emits (and a CPU test checks exactly as a channel sequence):
+//  * unitary gates collect into a segment; a depolarizing / bit-flip /
+//    phase-flip channel marks the last gate on its qubit (an identity is
+//    inserted when there is none);
+//  * any other channel closes the segment: the segment is fused (size-only
+//    cost, width k) and every block is emitted, followed by its Pauli errors
+//    moved to the block's end as U_s P U_s^dagger (U_s: the block's gates after
+//    the error); amplitude damping on consecutive qubits with one rate merges
+//    into one mask; other one-qubit channels are emitted with their Kraus
+//    operators sqrt(p_i) K_i.
+using Mat = std::vector<cd>;
+
+Mat mat_mul(const Mat &a, const Mat &b, size_t d) {
+  Mat c(d * d, cd(0, 0));
+  for (size_t r = 0; r < d; ++r)
+    for (size_t t = 0; t < d; ++t) {
+      const cd x = a[r * d + t];
+      if (x == cd(0, 0)) continue;
+      for (size_t j = 0; j < d; ++j) c[r * d + j] += x * b[t * d + j];
+    }
+  return c;
+}
+
+Mat dagger(const Mat &a, size_t d) {
+  Mat c(d * d);
+  for (size_t r = 0; r < d; ++r)
+    for (size_t j = 0; j < d; ++j) c[j * d + r] = std::conj(a[r * d + j]);
+  return c;
+}
+
+Mat identity(size_t d) {
+  Mat m(d * d, cd(0, 0));
+  for (size_t i = 0; i < d; ++i) m[i * d + i] = 1.0;
+  return m;
+}
+
+bool close2(const cd *a, const Mat &b, double tol) {
+  for (int i = 0; i < 4; ++i)
+    if (std::abs(a[i].real() - b[i].real()) > tol || std::abs(a[i].imag() - b[i].imag()) > tol)
+      return false;
+  return true;
+}
+
+const Mat &pauli(int i) {
+  static const Mat x{0, 1, 1, 0}, y{0, cd(0, -1), cd(0, 1), 0}, z{1, 0, 0, -1};
+  return i == 0 ? x : (i == 1 ? y : z);
+}
+
+struct Channel {  // a one-qubit channel: base matrix and weighted branches
+  uint32_t q;
+  const cd *base;
+  std::vector<double> w;
+  std::vector<const cd *> k;  // 2 x 2 each
+};
+
+// (p, three matrices) for a Pauli channel on an identity base, as the Python
+// builder's _is_pauli_channel; empty when it is not one.
+bool pauli_channel(const Channel &c, double &p, std::vector<Mat> &mats) {
+  const Mat eye = identity(2);
+  if (!close2(c.base, eye, 1e-9) || c.k.empty() || !close2(c.k[0], eye, 1e-9)) return false;
+  const size_t ne = c.k.size() - 1;
+  mats.clear();
+  for (size_t i = 1; i < c.k.size(); ++i) {
+    int which = -1;
+    for (int j = 0; j < 3; ++j)
+      if (close2(c.k[i], pauli(j), 1e-9)) which = j;
+    if (which < 0) return false;
+    mats.push_back(pauli(which));
+  }
+  if (ne == 3) {
+    const double lo = std::min({c.w[1], c.w[2], c.w[3]}), hi = std::max({c.w[1], c.w[2], c.w[3]});
+    if (hi - lo > 1e-12 * std::max(1.0, std::abs(c.w[1]))) return false;
+    p = c.w[1] + c.w[2] + c.w[3];
+    return true;
+  }
+  if (ne == 1) {
+    p = c.w[1];
+    mats = {mats[0], mats[0], mats[0]};
+    return true;
+  }
+  return false;
+}
+
+// gamma of an amplitude-damping channel (weights p0, p1; K0 = diag(1, s),
+// K1 = sqrt(gamma)|0><1| after scaling by sqrt(p)), as _damping_rate; < 0 if not.
+double damping_rate(const Channel &c) {
+  if (!close2(c.base, identity(2), 1e-9) || c.k.size() != 2) return -1;
+  const double s0 = std::sqrt(c.w[0]), s1 = std::sqrt(c.w[1]);
+  const cd k00 = s0 * c.k[0][0], k01 = s0 * c.k[0][1], k10 = s0 * c.k[0][2], k11 = s0 * c.k[0][3];
+  if (std::abs(k01) > 1e-12 || std::abs(k10) > 1e-12 || std::abs(k00 - 1.0) > 1e-12) return -1;
+  const double gamma = 1.0 - std::norm(k11);
+  const Mat exp1{0, std::sqrt(std::max(gamma, 0.0)), 0, 0};
+  Mat k1(4);
+  for (int i = 0; i < 4; ++i) k1[i] = s1 * c.k[1][i];
+  if (!close2(k1.data(), exp1, 1e-12)) return -1;
+  return gamma;
+}
+
+struct TrajBuilder {
+  void *prog;
+  uint32_t n, fk;
+  char *eb;
+  size_t el;
+  uint32_t stats[4] = {0, 0, 0, 0};  // blocks, error sites, damping ops, channels
+  std::vector<GatePtr> seg;
+  std::map<int, std::vector<std::tuple<uint32_t, double, std::vector<Mat>>>> markers;
+  std::vector<int> last_on;
+  uint32_t damp_mask = 0;
+  double damp_gamma = 0;
+
+  void fail(const char *what) {
+    throw std::runtime_error(std::string(what) + ": " + (eb && el ? eb : ""));
+  }
+  void emit_gate(const HGate &g) {
+    std::vector<cast_complex64_t> m(g.m.size());
+    for (size_t e = 0; e < g.m.size(); ++e) m[e] = {g.m[e].real(), g.m[e].imag()};
+    if (cast_b200_traj_add_gate(prog, m.data(), g.q.data(), g.k(), eb, el)) fail("add_gate");
+    ++stats[0];
+  }
+  void flush_damp() {
+    if (damp_mask) {
+      if (cast_b200_traj_add_damping(prog, damp_mask, damp_gamma, eb, el)) fail("add_damping");
+      ++stats[2];
+    }
+    damp_mask = 0;
+  }
+  void flush() {
+    if (seg.empty()) return;
+    Graph g;
+    g.n = n;
+    for (const GatePtr &x : seg) g.insert(x);
+    Cost cost{0, fk, 0.0, 0.0, 0.0, 0};
+    size_two_fusion(g);
+    for (uint32_t cdd = 3; cdd <= fk; ++cdd)
+      while (gate_fusion_pass(g, cost, 0.0, cdd) > 0) {
+      }
+    for (int id : g.live_ids()) {
+      const HGate &blk = *g.gates[id];
+      emit_gate(blk);
+      bool any = false;
+      for (int j : blk.prov) any = any || markers.count(j);
+      if (!any) continue;
+      const size_t d = 1ull << blk.k();
+      std::vector<Mat> suffix(blk.prov.size());
+      Mat u = identity(d);
+      for (size_t pos = blk.prov.size(); pos-- > 0;) {
+        suffix[pos] = u;
+        u = mat_mul(u, expand(*seg[blk.prov[pos]], blk.q), d);
+      }
+      for (size_t pos = 0; pos < blk.prov.size(); ++pos) {
+        auto it = markers.find(blk.prov[pos]);
+        if (it == markers.end()) continue;
+        const Mat ud = dagger(suffix[pos], d);
+        for (const auto &mk : it->second) {
+          std::vector<cast_complex64_t> buf;
+          for (const Mat &P : std::get<2>(mk)) {
+            HGate h;
+            h.q = {std::get<0>(mk)};
+            h.m = P;
+            const Mat e = mat_mul(mat_mul(suffix[pos], expand(h, blk.q), d), ud, d);
+            for (const cd &z : e) buf.push_back({z.real(), z.imag()});
+          }
+          if (cast_b200_traj_add_pauli_error(prog, std::get<1>(mk), buf.data(), eb, el))
+            fail("add_pauli_error");
+          ++stats[1];
+        }
+      }
+    }
+    seg.clear();
+    markers.clear();
+    std::fill(last_on.begin(), last_on.end(), -1);
+  }
+  void unitary(const uint32_t *q, uint32_t k, const cast_complex64_t *m) {
+    flush_damp();
+    auto h = std::make_shared<HGate>();
+    h->q.assign(q, q + k);
+    const size_t ne = 1ull << (2 * k);
+    h->m.resize(ne);
+    for (size_t e = 0; e < ne; ++e) h->m[e] = cd(m[e].re, m[e].im);
+    const int idx = (int)seg.size();
+    h->prov = {idx};
+    seg.push_back(h);
+    for (uint32_t b = 0; b < k; ++b) last_on[q[b]] = idx;
+  }
+  void channel(const Channel &c) {
+    double p;
+    std::vector<Mat> mats;
+    if (pauli_channel(c, p, mats)) {
+      flush_damp();
+      if (last_on[c.q] < 0) {
+        const cast_complex64_t id[4] = {{1, 0}, {0, 0}, {0, 0}, {1, 0}};
+        unitary(&c.q, 1, id);
+      }
+      markers[last_on[c.q]].emplace_back(c.q, p, std::move(mats));
+      return;
+    }
+    flush();  // any other channel closes the segment
+    const double gamma = damping_rate(c);
+    if (gamma >= 0) {
+      if (damp_mask && (std::abs(gamma - damp_gamma) > 1e-15 || ((damp_mask >> c.q) & 1))) flush_damp();
+      damp_mask |= 1u << c.q;
+      damp_gamma = gamma;
+      return;
+    }
+    flush_damp();
+    if (c.k.size() > 4) throw std::runtime_error("trajectory mode supports one-qubit channels with <= 4 Kraus operators");
+    std::vector<cast_complex64_t> kr;
+    for (size_t i = 0; i < c.k.size(); ++i) {
+      const double s = std::sqrt(c.w[i]);
+      for (int e = 0; e < 4; ++e) kr.push_back({s * c.k[i][e].real(), s * c.k[i][e].imag()});
+    }
+    if (cast_b200_traj_add_channel(prog, c.q, kr.data(), (uint32_t)c.k.size(), eb, el)) fail("add_channel");
+    ++stats[3];
+  }
+};
+
 constexpr uint32_t kFusedMagic = 0xCB20F05Eu;
 struct Fused {
   uint32_t magic = kFusedMagic;
@@ -428,6 +653,61 @@ void cast_b200_fused_free(void *fused) {
   if (!f || f->magic != kFusedMagic) return;
   f->magic = 0;
   delete f;
+}
+
+int cast_b200_traj_build(void *program, uint32_t n_items, const uint32_t *kind, const uint32_t *k,
+                         const uint32_t *qubits, const cast_complex64_t *matrices,
+                         const uint32_t *n_branches, const double *weights, uint32_t fusion_k,
+                         uint32_t *out_stats, char *err_buf, size_t err_buf_len) {
+  const uint32_t n = cast_b200_traj_num_qubits(program);
+  if (!n || (n_items && (!kind || !k || !qubits || !matrices || !n_branches))) {
+    cb2::write_err(err_buf, err_buf_len, "invalid trajectory program or circuit arrays");
+    return 1;
+  }
+  if (fusion_k < 1 || fusion_k > 4) {
+    cb2::write_err(err_buf, err_buf_len, "trajectory fusion width must be 1..4");
+    return 1;
+  }
+  try {
+    TrajBuilder tb{program, n, fusion_k, err_buf, err_buf_len};
+    tb.last_on.assign(n, -1);
+    size_t qo = 0, mo = 0, wo = 0;
+    for (uint32_t i = 0; i < n_items; ++i) {
+      const uint32_t kk = k[i];
+      if (kk == 0 || kk > cb2::kMaxGateQubits) throw std::runtime_error("gate size out of range");
+      for (uint32_t b = 0; b < kk; ++b) {
+        if (qubits[qo + b] >= n) throw std::runtime_error("qubit out of range");
+        if (b && qubits[qo + b - 1] >= qubits[qo + b]) throw std::runtime_error("qubits must be ascending");
+      }
+      if (kind[i] == 0) {
+        tb.unitary(qubits + qo, kk, matrices + mo);
+        mo += 1ull << (2 * kk);
+      } else {
+        if (kk != 1 || !weights) throw std::runtime_error("trajectory mode supports one-qubit channels");
+        Channel c;
+        c.q = qubits[qo];
+        c.base = reinterpret_cast<const cd *>(matrices + mo);
+        mo += 4;
+        for (uint32_t b = 0; b < n_branches[i]; ++b) {
+          c.w.push_back(weights[wo + b]);
+          c.k.push_back(reinterpret_cast<const cd *>(matrices + mo));
+          mo += 4;
+        }
+        wo += n_branches[i];
+        tb.channel(c);
+      }
+      qo += kk;
+    }
+    tb.flush();
+    tb.flush_damp();
+    if (out_stats)
+      for (int j = 0; j < 4; ++j) out_stats[j] = tb.stats[j];
+    cb2::clear_err(err_buf, err_buf_len);
+    return 0;
+  } catch (const std::exception &e) {
+    cb2::write_err(err_buf, err_buf_len, e.what());
+    return 1;
+  }
 }
 
 }  // extern "C"

@@ -864,6 +864,41 @@ int cast_b200_traj_set_launch(void *prog, uint32_t threads, uint32_t max_ctas, c
   return 0;
 }
 
+uint32_t cast_b200_traj_num_qubits(const void *prog) {
+  const TrajProgram *p = static_cast<const TrajProgram *>(prog);
+  return p && p->magic == kTrajMagic ? p->n : 0;
+}
+
+int cast_b200_traj_get_op(const void *prog, uint32_t index, uint32_t *out_type, uint32_t *out_k,
+                          uint32_t *out_qubits, double *out_prob, uint32_t *out_mask,
+                          uint32_t *out_n_mats, cast_complex64_t *out_mats, size_t out_mats_len) {
+  const TrajProgram *p = static_cast<const TrajProgram *>(prog);
+  if (!p || p->magic != kTrajMagic || index >= p->ops.size()) return 1;
+  const TOp &o = p->ops[index];
+  size_t entries = 0;
+  uint32_t nm = 0;
+  double prob = 0;
+  switch (o.type) {
+  case T_GATE: nm = 1; entries = 1ull << (2 * o.k); break;
+  case T_ERR: nm = 3; entries = 3ull << (2 * o.k); prob = o.prob; break;
+  case T_DAMP: prob = o.gamma; break;
+  default: nm = o.nk; entries = 4ull * o.nk; break;
+  }
+  if (out_type) *out_type = o.type;
+  if (out_k) *out_k = o.k;
+  if (out_qubits)
+    for (uint32_t b = 0; b < o.k && b < kTrajMaxGate; ++b) out_qubits[b] = o.q[b];
+  if (out_prob) *out_prob = prob;
+  if (out_mask) *out_mask = o.mask;
+  if (out_n_mats) *out_n_mats = nm;
+  if (out_mats) {
+    if (out_mats_len < entries) return 1;
+    for (size_t e = 0; e < entries; ++e)
+      out_mats[e] = {p->pool[o.mat + e].x, p->pool[o.mat + e].y};
+  }
+  return 0;
+}
+
 uint32_t cast_b200_traj_num_ops(const void *prog) {
   const TrajProgram *p = static_cast<const TrajProgram *>(prog);
   return p && p->magic == kTrajMagic ? (uint32_t)p->ops.size() : 0;

@@ -88,11 +88,15 @@ class TrajectoryProgramStats:
     n_errors: int = 0
     n_damping: int = 0
     n_channels: int = 0
-    block_sizes: list = field(default_factory=list)
+    block_sizes: list = field(default_factory=list)  # filled by the Python builder
 
 
 class TrajectoryProgram:
-    def __init__(self, circuit: QuantumCircuit, fusion_k: int = 4):
+    """A noisy circuit compiled for the batched-trajectory kernel.  The program
+    is built natively (``cast_b200_traj_build``); ``native=False`` runs the
+    Python builder, which emits the same program."""
+
+    def __init__(self, circuit: QuantumCircuit, fusion_k: int = 4, native: bool = True):
         if not 1 <= fusion_k <= 4:
             raise ValueError("trajectory fusion width must be 1..4")
         self.n = circuit.n_qubits()
@@ -101,7 +105,10 @@ class TrajectoryProgram:
                                   "traj_create")
         self.stats = TrajectoryProgramStats()
         self._k = fusion_k
-        self._build(circuit)
+        if native:
+            self._build_native(circuit)
+        else:
+            self._build(circuit)
 
     def __del__(self):
         h = getattr(self, "handle", None)
@@ -223,6 +230,64 @@ class TrajectoryProgram:
 
     def __len__(self):
         return int(L.lib().cast_b200_traj_num_ops(self.handle))
+
+    def _build_native(self, circ: QuantumCircuit) -> None:
+        kind, ks, qs, mats, nb, ws = [], [], [], [], [], []
+        for g in circ.gates():
+            q = g.qubits()
+            if g.is_unitary():
+                kind.append(0)
+                nb.append(0)
+            else:
+                br = g.noise_model().branches
+                if len(q) != 1:
+                    raise ValueError("trajectory mode supports single-qubit channels with <= 4 "
+                                     "Kraus operators")
+                kind.append(1)
+                nb.append(len(br))
+            ks.append(len(q))
+            qs.extend(q)
+            mats.append(np.asarray(g.matrix(), dtype=np.complex128).ravel())
+            if not g.is_unitary():
+                for p, k in br:
+                    mats.append(np.asarray(k, dtype=np.complex128).ravel())
+                    ws.append(p)
+        u32 = lambda a: np.ascontiguousarray(a, dtype=np.uint32)
+        kind_a, ks_a, qs_a, nb_a = u32(kind), u32(ks), u32(qs), u32(nb)
+        m_a = np.ascontiguousarray(np.concatenate(mats) if mats else np.zeros(1), dtype=np.complex128)
+        w_a = np.ascontiguousarray(ws if ws else [0.0], dtype=np.float64)
+        stats = np.zeros(4, dtype=np.uint32)
+        eb = L.errbuf()
+        L.check(L.lib().cast_b200_traj_build(
+            self.handle, len(kind), kind_a.ctypes.data_as(L.c_u32p), ks_a.ctypes.data_as(L.c_u32p),
+            qs_a.ctypes.data_as(L.c_u32p), m_a.view(np.float64).ctypes.data_as(C.POINTER(L.Complex64)),
+            nb_a.ctypes.data_as(L.c_u32p), w_a.ctypes.data_as(L.c_dp), self._k,
+            stats.ctypes.data_as(L.c_u32p), eb, L.ERR_LEN), eb, "traj_build")
+        self.stats.n_blocks, self.stats.n_errors, self.stats.n_damping, self.stats.n_channels = (
+            int(x) for x in stats)
+
+    def ops(self) -> list:
+        """The program as (kind, k, qubits, probability or rate, mask, matrices)
+        tuples, kind one of gate / err / damp / chan (matrices in complex64)."""
+        out = []
+        names = ("gate", "err", "damp", "chan")
+        t, k, m = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        nm, p = C.c_uint32(), C.c_double()
+        q = np.zeros(4, dtype=np.uint32)
+        buf = np.zeros(3 * 256, dtype=np.complex128)
+        for i in range(len(self)):
+            rc = L.lib().cast_b200_traj_get_op(self.handle, i, C.byref(t), C.byref(k),
+                                               q.ctypes.data_as(L.c_u32p), C.byref(p), C.byref(m),
+                                               C.byref(nm), buf.view(np.float64).ctypes.data_as(
+                                                   C.POINTER(L.Complex64)), buf.size)
+            if rc:
+                raise RuntimeError("traj_get_op failed")
+            kind = names[t.value]
+            kk = k.value if kind != "chan" else 1
+            d = 1 << kk
+            mats = [buf[j * d * d:(j + 1) * d * d].reshape(d, d).copy() for j in range(nm.value)]
+            out.append((kind, k.value, tuple(int(x) for x in q[:k.value]), p.value, m.value, mats))
+        return out
 
     def set_launch(self, threads: int = 0, max_ctas: int = 0) -> None:
         """Launch shape of the trajectory kernel: threads per CTA (512 or 1024)

@@ -182,6 +182,26 @@ int cast_b200_traj_add_damping(void *program, uint32_t qubit_mask, double gamma,
 int cast_b200_traj_add_channel(void *program, uint32_t qubit, const cast_complex64_t *kraus,
                                uint32_t n_kraus, char *err_buf, size_t err_buf_len);
 uint32_t cast_b200_traj_num_ops(const void *program);
+uint32_t cast_b200_traj_num_qubits(const void *program);
+/* Builds the whole program from a circuit, natively (the trajectory
+ * construction: Pauli channels moved to the end of their fused block as
+ * U P U^dagger, damping merged into masks, other one-qubit channels kept).
+ * Item i is a unitary gate (kind 0: k[i] ascending qubits, 4^k matrix entries)
+ * or a one-qubit channel (kind 1: base matrix then n_branches[i] Kraus
+ * matrices, 4 entries each, and as many weights).  Qubits, matrices and
+ * weights are consumed in item order.  out_stats (4 entries, may be NULL):
+ * fused blocks, Pauli error sites, damping ops, general channels. */
+int cast_b200_traj_build(void *program, uint32_t n_items, const uint32_t *kind, const uint32_t *k,
+                         const uint32_t *qubits, const cast_complex64_t *matrices,
+                         const uint32_t *n_branches, const double *weights, uint32_t fusion_k,
+                         uint32_t *out_stats, char *err_buf, size_t err_buf_len);
+/* Reads op `index` back: type (0 gate, 1 Pauli error, 2 damping, 3 channel),
+ * k and qubits, probability (error) or rate (damping), qubit mask (damping),
+ * and its matrices (gate: 1, error: 3 on the block's qubits, channel: the
+ * Kraus operators; complex64 precision) when out_mats holds enough entries. */
+int cast_b200_traj_get_op(const void *program, uint32_t index, uint32_t *out_type, uint32_t *out_k,
+                          uint32_t *out_qubits, double *out_prob, uint32_t *out_mask,
+                          uint32_t *out_n_mats, cast_complex64_t *out_mats, size_t out_mats_len);
 /* Launch shape of the trajectory kernel, a tuning knob with no counterpart in
  * the reference.  threads: threads per CTA, 512 or 1024, or 0 (the default) to
  * choose by state size.  max_ctas: CTAs, i.e. trajectories in flight (each owns

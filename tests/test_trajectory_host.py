@@ -67,7 +67,7 @@ def _record(monkeypatch):
 def test_program_equals_circuit_as_channels(monkeypatch, oracle, cblib, fusion_k):
     ops = _record(monkeypatch)
     circ = _circuit()
-    TR.TrajectoryProgram(circ, fusion_k)
+    TR.TrajectoryProgram(circ, fusion_k, native=False)  # the Python builder, recorded
     n = circ.n_qubits()
     # the reference: every gate / channel of the circuit, in order
     ref = oracle.dm_zero(n)
@@ -105,3 +105,71 @@ def test_program_equals_circuit_as_channels(monkeypatch, oracle, cblib, fusion_k
     assert [o for o in ops if o[0] == "damp"] == [("damp", 0b1111, pytest.approx(0.1))]
     assert kinds.count("chan") == 1
     assert kinds.count("err") == 6  # one per Pauli site
+
+
+def _dm_of_ops(oracle, n, ops):
+    """Density matrix of a trajectory program read as a channel sequence
+    (ops as TrajectoryProgram.ops() returns them)."""
+    rho = oracle.dm_zero(n)
+    block_q = None
+    for kind, k, q, p, mask, mats in ops:
+        if kind == "gate":
+            block_q = q
+            oracle.dm_apply_channel(rho, n, mats, [1.0], q)
+        elif kind == "err":
+            d = 1 << len(block_q)
+            oracle.dm_apply_channel(rho, n, [np.eye(d)] + mats, [1 - p] + [p / 3] * 3, block_q)
+        elif kind == "damp":
+            k0 = np.diag([1.0, math.sqrt(1 - p)])
+            k1 = np.array([[0.0, math.sqrt(p)], [0.0, 0.0]])
+            for qq in range(n):
+                if (mask >> qq) & 1:
+                    oracle.dm_apply_channel(rho, n, [k0, k1], [1.0, 1.0], (qq,))
+        else:
+            oracle.dm_apply_channel(rho, n, mats, [1.0] * len(mats), q)
+    return rho
+
+
+@pytest.mark.parametrize("fusion_k", [1, 2, 3, 4])
+def test_native_builder_equals_python_builder(oracle, cblib, fusion_k):
+    """The native builder (cast_b200_traj_build) emits the Python builder's
+    program: same op sequence, qubits and probabilities, matrices equal to the
+    complex64 storage precision; read as channels it reproduces the circuit's
+    density matrix."""
+    circ = _circuit()
+    n = circ.n_qubits()
+    nat = TR.TrajectoryProgram(circ, fusion_k, native=True)
+    py = TR.TrajectoryProgram(circ, fusion_k, native=False)
+    a, b = nat.ops(), py.ops()
+    assert [(o[0], o[1], o[2], o[4]) for o in a] == [(o[0], o[1], o[2], o[4]) for o in b]
+    for x, y in zip(a, b):
+        assert x[3] == pytest.approx(y[3], abs=1e-7)
+        assert all(np.max(np.abs(mx - my)) < 1e-6 for mx, my in zip(x[5], y[5]))
+    assert (nat.stats.n_blocks, nat.stats.n_errors, nat.stats.n_damping, nat.stats.n_channels) == \
+        (py.stats.n_blocks, py.stats.n_errors, py.stats.n_damping, py.stats.n_channels)
+    ref = oracle.dm_zero(n)
+    for g in circ.gates():
+        if g.is_unitary():
+            oracle.dm_apply_channel(ref, n, [g.matrix()], [1.0], g.qubits())
+        else:
+            br = g.noise_model().branches
+            oracle.dm_apply_channel(ref, n, [k for _, k in br], [p for p, _ in br], g.qubits())
+    assert np.max(np.abs(_dm_of_ops(oracle, n, a) - ref)) < 1e-5
+
+
+def test_native_builder_brickwork_matches_python(cblib):
+    """The trajectory configuration's construction (brickwork, depolarizing after
+    every gate, damping every layer) at 12 qubits builds the same program both ways."""
+    circ = QuantumCircuit.brickwork(12, 6, 5, depolarizing=1e-3, damping=5e-4)
+    a = TR.TrajectoryProgram(circ, 3, native=True).ops()
+    b = TR.TrajectoryProgram(circ, 3, native=False).ops()
+    assert len(a) == len(b) > 0
+    assert [(o[0], o[2], o[4]) for o in a] == [(o[0], o[2], o[4]) for o in b]
+    assert max(np.max(np.abs(mx - my)) for x, y in zip(a, b) for mx, my in zip(x[5], y[5])) < 1e-6
+
+
+def test_native_builder_rejects_wide_channels(cblib):
+    c = QuantumCircuit(3)
+    c.add(QuantumGate.cx(0, 1).with_noise([(0.99, np.eye(4)), (0.01, np.kron(mat_x(), np.eye(2)))]))
+    with pytest.raises(ValueError, match="single-qubit channels"):
+        TR.TrajectoryProgram(c, 3)
