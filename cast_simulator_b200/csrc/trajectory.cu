@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <cmath>
 #include <exception>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -628,6 +629,44 @@ cudaError_t launch_trajectories(unsigned grid, unsigned threads, cudaStream_t s,
   return cudaLaunchKernelEx(&cfg, k_trajectories<512>, ops, n_ops, pool, ws, n, run, z, sample);
 }
 
+// Device buffers of trajectory programs come from a process-wide cache keyed by
+// exact size.  cudaFree synchronises the whole device, and a serving loop
+// creates and drops one program per noisy request while other requests run on
+// other streams.  A dropped program's buffers are idle (cast_b200_traj_run
+// returns only after its work completes), so they wait here for reuse, up to
+// 8 GiB in all; beyond that they are freed.
+std::mutex g_buf_mu;
+std::multimap<size_t, void *> g_buf_cache;
+size_t g_buf_cached = 0;
+constexpr size_t kBufCacheMax = 8ull << 30;
+
+cudaError_t buf_alloc(void **p, size_t bytes) {
+  {
+    std::lock_guard<std::mutex> lock(g_buf_mu);
+    auto it = g_buf_cache.find(bytes);
+    if (it != g_buf_cache.end()) {
+      *p = it->second;
+      g_buf_cache.erase(it);
+      g_buf_cached -= bytes;
+      return cudaSuccess;
+    }
+  }
+  return cudaMalloc(p, bytes);
+}
+
+void buf_free(void *p, size_t bytes) {
+  if (!p) return;
+  {
+    std::lock_guard<std::mutex> lock(g_buf_mu);
+    if (g_buf_cached + bytes <= kBufCacheMax) {
+      g_buf_cache.emplace(bytes, p);
+      g_buf_cached += bytes;
+      return;
+    }
+  }
+  cudaFree(p);
+}
+
 struct TrajProgram {
   uint32_t magic = kTrajMagic;
   uint32_t n = 0;
@@ -638,6 +677,7 @@ struct TrajProgram {
   float2 *d_pool = nullptr;
   float2 *d_ws = nullptr;
   size_t ws_ctas = 0;
+  size_t ops_bytes = 0, pool_bytes = 0, ws_bytes = 0, z_bytes = 0, sample_bytes = 0;
   TRun *d_run = nullptr;
   double *d_z = nullptr;
   uint32_t *d_sample = nullptr;
@@ -652,12 +692,12 @@ struct TrajProgram {
 
   ~TrajProgram() {
     if (graph) cudaGraphExecDestroy(graph);
-    cudaFree(d_ops);
-    cudaFree(d_pool);
-    cudaFree(d_ws);
-    cudaFree(d_run);
-    cudaFree(d_z);
-    cudaFree(d_sample);
+    buf_free(d_ops, ops_bytes);
+    buf_free(d_pool, pool_bytes);
+    buf_free(d_ws, ws_bytes);
+    buf_free(d_run, sizeof(TRun));
+    buf_free(d_z, z_bytes);
+    buf_free(d_sample, sample_bytes);
   }
 
   uint32_t push_matrix(const cast_complex64_t *m, size_t entries) {
@@ -693,15 +733,19 @@ struct TrajProgram {
       cudaGraphExecDestroy(graph);
       graph = nullptr;
     }
-    cudaFree(d_ops);
-    cudaFree(d_pool);
+    buf_free(d_ops, ops_bytes);
+    buf_free(d_pool, pool_bytes);
     d_ops = nullptr;
     d_pool = nullptr;
+    ops_bytes = pool_bytes = 0;
     const size_t ob = sizeof(TOp) * std::max<size_t>(1, ops.size());
     const size_t pb = sizeof(float2) * std::max<size_t>(1, pool.size());
-    if (!cuda_ok(cudaMalloc(&d_ops, ob), "cudaMalloc (trajectory ops)", err) ||
-        !cuda_ok(cudaMalloc(&d_pool, pb), "cudaMalloc (trajectory matrices)", err))
+    if (!cuda_ok(buf_alloc(reinterpret_cast<void **>(&d_ops), ob), "cudaMalloc (trajectory ops)", err))
       return false;
+    ops_bytes = ob;
+    if (!cuda_ok(buf_alloc(reinterpret_cast<void **>(&d_pool), pb), "cudaMalloc (trajectory matrices)", err))
+      return false;
+    pool_bytes = pb;
     if (!ops.empty() &&
         !cuda_ok(cudaMemcpy(d_ops, ops.data(), sizeof(TOp) * ops.size(), cudaMemcpyHostToDevice),
                  "cudaMemcpy (trajectory ops)", err))
@@ -935,34 +979,44 @@ int cast_b200_traj_run_range(void *prog, uint32_t first, uint32_t n_traj, uint64
     const unsigned grid = (unsigned)std::min<uint64_t>(n_traj, ctas);
     const unsigned threads = p->threads ? p->threads : auto_threads(p->n);
     if (p->ws_ctas < grid) {
-      cudaFree(p->d_ws);
+      buf_free(p->d_ws, p->ws_bytes);
       p->d_ws = nullptr;
-      if (!cuda_ok(cudaMalloc(&p->d_ws, (sizeof(float2) << p->n) * grid),
+      p->ws_bytes = 0;
+      if (!cuda_ok(buf_alloc(reinterpret_cast<void **>(&p->d_ws), (sizeof(float2) << p->n) * grid),
                    "cudaMalloc (trajectory workspace)", err)) {
         cb2::write_err(err_buf, err_buf_len, err);
         return 1;
       }
       p->ws_ctas = grid;
+      p->ws_bytes = (sizeof(float2) << p->n) * grid;
       if (p->graph) {
         cudaGraphExecDestroy(p->graph);
         p->graph = nullptr;
       }
     }
-    if (!p->d_run && !cuda_ok(cudaMalloc(&p->d_run, sizeof(TRun)), "cudaMalloc (run)", err)) {
+    if (!p->d_run &&
+        !cuda_ok(buf_alloc(reinterpret_cast<void **>(&p->d_run), sizeof(TRun)), "cudaMalloc (run)", err)) {
       cb2::write_err(err_buf, err_buf_len, err);
       return 1;
     }
     if (p->out_cap < n_traj) {
-      cudaFree(p->d_z);
-      cudaFree(p->d_sample);
+      buf_free(p->d_z, p->z_bytes);
+      buf_free(p->d_sample, p->sample_bytes);
       p->d_z = nullptr;
       p->d_sample = nullptr;
-      if (!cuda_ok(cudaMalloc(&p->d_z, sizeof(double) * n_traj * p->n), "cudaMalloc (z)", err) ||
-          !cuda_ok(cudaMalloc(&p->d_sample, sizeof(uint32_t) * n_traj), "cudaMalloc (samples)",
-                   err)) {
+      p->z_bytes = p->sample_bytes = 0;
+      if (!cuda_ok(buf_alloc(reinterpret_cast<void **>(&p->d_z), sizeof(double) * n_traj * p->n),
+                   "cudaMalloc (z)", err)) {
         cb2::write_err(err_buf, err_buf_len, err);
         return 1;
       }
+      p->z_bytes = sizeof(double) * n_traj * p->n;
+      if (!cuda_ok(buf_alloc(reinterpret_cast<void **>(&p->d_sample), sizeof(uint32_t) * n_traj),
+                   "cudaMalloc (samples)", err)) {
+        cb2::write_err(err_buf, err_buf_len, err);
+        return 1;
+      }
+      p->sample_bytes = sizeof(uint32_t) * n_traj;
       p->out_cap = n_traj;
       if (p->graph) {
         cudaGraphExecDestroy(p->graph);
