@@ -630,20 +630,25 @@ cudaError_t launch_trajectories(unsigned grid, unsigned threads, cudaStream_t s,
 }
 
 // Device buffers of trajectory programs come from a process-wide cache keyed by
-// exact size.  cudaFree synchronises the whole device, and a serving loop
-// creates and drops one program per noisy request while other requests run on
-// other streams.  A dropped program's buffers are idle (cast_b200_traj_run
+// (device, exact size).  cudaFree synchronises the whole device, and a serving
+// loop creates and drops one program per noisy request while other requests
+// run on other streams.  A dropped program's buffers are idle (cast_b200_traj_run
 // returns only after its work completes), so they wait here for reuse, up to
-// 8 GiB in all; beyond that they are freed.
+// 8 GiB in all; beyond that they are freed.  The device of a returned buffer is
+// read from the pointer itself, so a process that switches devices with
+// cast_b200_set_device never receives another device's memory.
 std::mutex g_buf_mu;
-std::multimap<size_t, void *> g_buf_cache;
+std::multimap<std::pair<int, size_t>, void *> g_buf_cache;
 size_t g_buf_cached = 0;
 constexpr size_t kBufCacheMax = 8ull << 30;
 
 cudaError_t buf_alloc(void **p, size_t bytes) {
+  int dev = 0;
+  const cudaError_t rc = cudaGetDevice(&dev);
+  if (rc != cudaSuccess) return rc;
   {
     std::lock_guard<std::mutex> lock(g_buf_mu);
-    auto it = g_buf_cache.find(bytes);
+    auto it = g_buf_cache.find({dev, bytes});
     if (it != g_buf_cache.end()) {
       *p = it->second;
       g_buf_cache.erase(it);
@@ -656,10 +661,11 @@ cudaError_t buf_alloc(void **p, size_t bytes) {
 
 void buf_free(void *p, size_t bytes) {
   if (!p) return;
-  {
+  cudaPointerAttributes attr{};
+  if (cudaPointerGetAttributes(&attr, p) == cudaSuccess && attr.type == cudaMemoryTypeDevice) {
     std::lock_guard<std::mutex> lock(g_buf_mu);
     if (g_buf_cached + bytes <= kBufCacheMax) {
-      g_buf_cache.emplace(bytes, p);
+      g_buf_cache.emplace(std::make_pair(attr.device, bytes), p);
       g_buf_cached += bytes;
       return;
     }
