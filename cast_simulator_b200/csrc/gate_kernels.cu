@@ -50,9 +50,65 @@ struct Targets {
   uint64_t stride[kMaxGateQubits];   // 1 << q_b (amplitude units)
 };
 
+// 4-qubit gates use three real products per complex multiply-add (the 3M
+// method, Higham, "Accuracy and Stability of Numerical Algorithms", 2nd ed.,
+// sec. 23.2.4): for M = c + i d and x = a + i b,
+//   S1 += c (a + b),  S2 += a (d - c),  S3 += b (c + d),
+//   Re(Mx) = S1 - S3,  Im(Mx) = S1 + S2,
+// with a + b formed once per amplitude and c, d - c, c + d formed on the host.
+// That is 48 FMAs and 3 adds per row against 64 FMAs.  At k = 4 the FP64 pass
+// is FMA-bound at the power-capped SM clock (about 1.35 GHz); the rounding
+// error stays within a small multiple of the 4-product form's (Higham,
+// Lemma 3.7 and sec. 23.2.4), and an exact zero entry still contributes exact
+// zeros to all three sums.  Entry e of the matrix is stored as
+// m[3e], m[3e+1], m[3e+2] = c, d - c, c + d; every other k keeps (re, im) pairs.
+template <int K> struct ThreeMult { static constexpr bool on = K == 4; };
+
 template <typename T, int K> struct MatParam {
-  T m[2 * (1 << K) * (1 << K)];
+  T m[(ThreeMult<K>::on ? 3 : 2) * (1 << K) * (1 << K)];
 };
+
+// Row r of M times the D amplitudes x, for the register and tile kernels.
+template <typename T, int K, typename V>
+__device__ __forceinline__ V gate_row(const MatParam<T, K> &M, int r, const V (&x)[1 << K],
+                                      const T (&sx)[1 << K]) {
+  constexpr int D = 1 << K;
+  V o;
+  if constexpr (ThreeMult<K>::on) {
+    T s1 = T(0), s2 = T(0), s3 = T(0);
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+      s1 = fma(M.m[3 * (r * D + c)], sx[c], s1);
+      s2 = fma(M.m[3 * (r * D + c) + 1], x[c].x, s2);
+      s3 = fma(M.m[3 * (r * D + c) + 2], x[c].y, s3);
+    }
+    o.x = s1 - s3;
+    o.y = s1 + s2;
+  } else {
+    T re = T(0), im = T(0);
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+      const T mr = M.m[2 * (r * D + c)];
+      const T mi = M.m[2 * (r * D + c) + 1];
+      re = fma(mr, x[c].x, re);
+      re = fma(-mi, x[c].y, re);
+      im = fma(mr, x[c].y, im);
+      im = fma(mi, x[c].x, im);
+    }
+    o.x = re;
+    o.y = im;
+  }
+  return o;
+}
+
+// a + b of each amplitude, the shared operand of S1 (3M form only).
+template <typename T, int K, typename V>
+__device__ __forceinline__ void row_sums(const V (&x)[1 << K], T (&sx)[1 << K]) {
+  if constexpr (ThreeMult<K>::on) {
+#pragma unroll
+    for (int c = 0; c < (1 << K); ++c) sx[c] = x[c].x + x[c].y;
+  }
+}
 
 // Group index -> amplitude index of the group's first member: insert a zero
 // bit at every target position, lowest first (the PDEP of cuda_gen.cpp:174-211).
@@ -101,23 +157,10 @@ __global__ void __launch_bounds__(kRegThreads) k_gate_reg(T *__restrict__ sv, ui
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     if (g0 + (uint64_t)u * kRegThreads >= n_groups) break;
+    T sx[D];
+    row_sums<T, K>(x[u], sx);
 #pragma unroll
-    for (int r = 0; r < D; ++r) {
-      T re = T(0), im = T(0);
-#pragma unroll
-      for (int c = 0; c < D; ++c) {
-        const T mr = M.m[2 * (r * D + c)];
-        const T mi = M.m[2 * (r * D + c) + 1];
-        re = fma(mr, x[u][c].x, re);
-        re = fma(-mi, x[u][c].y, re);
-        im = fma(mr, x[u][c].y, im);
-        im = fma(mi, x[u][c].x, im);
-      }
-      V o;
-      o.x = re;
-      o.y = im;
-      psi[base[u] + member_offset<K>(r, t)] = o;
-    }
+    for (int r = 0; r < D; ++r) psi[base[u] + member_offset<K>(r, t)] = gate_row<T, K>(M, r, x[u], sx);
   }
 }
 
@@ -195,21 +238,11 @@ __global__ void __launch_bounds__(TileThreads<K>::N) k_gate_tile(T *__restrict__
           if ((m >> b) & 1) o += a.loc_lo_mask[b] + 1;
         x[m] = s[swz<LOGE>(o)];
       }
+      T sx[D];
+      row_sums<T, K>(x, sx);
 #pragma unroll
       for (int r = 0; r < D; ++r) {
-        T re = T(0), im = T(0);
-#pragma unroll
-        for (int c = 0; c < D; ++c) {
-          const T mr = M.m[2 * (r * D + c)];
-          const T mi = M.m[2 * (r * D + c) + 1];
-          re = fma(mr, x[c].x, re);
-          re = fma(-mi, x[c].y, re);
-          im = fma(mr, x[c].y, im);
-          im = fma(mi, x[c].x, im);
-        }
-        V o;
-        o.x = re;
-        o.y = im;
+        const V o = gate_row<T, K>(M, r, x, sx);
         uint32_t po = base;
 #pragma unroll
         for (int b = 0; b < K; ++b)
@@ -525,6 +558,30 @@ template <typename F> int max_blocks_per_sm(F kernel, int threads, size_t smem) 
   return b;
 }
 
+// The kernel-parameter copy of the matrix: the snapped (re, im) pairs as they
+// are, or for the 3M form (c, d - c, c + d) per entry, formed in FP64 from the
+// snapped matrix and rounded once to T.  The launch copies the parameters, so
+// `scratch` only has to outlive the launch call.
+template <typename T, int K>
+const MatParam<T, K> *mat_param(const GateData &g, MatParam<T, K> &scratch) {
+  if constexpr (ThreeMult<K>::on) {
+    constexpr size_t E = size_t(1) << (2 * K);
+    const bool wide = g.m64.size() == 2 * E;
+    for (size_t e = 0; e < E; ++e) {
+      const double c = wide ? g.m64[2 * e] : (double)g.m32[2 * e];
+      const double d = wide ? g.m64[2 * e + 1] : (double)g.m32[2 * e + 1];
+      scratch.m[3 * e] = (T)c;
+      scratch.m[3 * e + 1] = (T)(d - c);
+      scratch.m[3 * e + 2] = (T)(c + d);
+    }
+    return &scratch;
+  } else {
+    (void)scratch;
+    if constexpr (sizeof(T) == 8) return reinterpret_cast<const MatParam<T, K> *>(g.m64.data());
+    else return reinterpret_cast<const MatParam<T, K> *>(g.m32.data());
+  }
+}
+
 template <typename T, int K>
 bool launch_reg(const GateData &g, void *sv, uint32_t n, const Targets &t, cudaStream_t s,
                 std::string &err) {
@@ -535,9 +592,8 @@ bool launch_reg(const GateData &g, void *sv, uint32_t n, const Targets &t, cudaS
     err = "statevector too large for the gate kernel grid";
     return false;
   }
-  const MatParam<T, K> *mp;
-  if constexpr (sizeof(T) == 8) mp = reinterpret_cast<const MatParam<T, K> *>(g.m64.data());
-  else mp = reinterpret_cast<const MatParam<T, K> *>(g.m32.data());
+  MatParam<T, K> scratch;
+  const MatParam<T, K> *mp = mat_param<T, K>(g, scratch);
   T *p = static_cast<T *>(sv);
   void *args[] = {&p, const_cast<uint64_t *>(&n_groups), const_cast<Targets *>(&t),
                   const_cast<MatParam<T, K> *>(mp)};
@@ -693,9 +749,8 @@ bool launch_tile(const GateData &g, void *sv, uint32_t n, const TileArgs &a, cud
   if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(tile gate kernel)", err)) return false;
   const uint64_t n_tiles = 1ull << (n - tile_bits(K));
   const size_t smem = sizeof(V) << tile_bits(K);
-  const MatParam<T, K> *mp;
-  if constexpr (sizeof(T) == 8) mp = reinterpret_cast<const MatParam<T, K> *>(g.m64.data());
-  else mp = reinterpret_cast<const MatParam<T, K> *>(g.m32.data());
+  MatParam<T, K> scratch;
+  const MatParam<T, K> *mp = mat_param<T, K>(g, scratch);
   T *p = static_cast<T *>(sv);
   void *args[] = {&p, const_cast<TileArgs *>(&a), const_cast<MatParam<T, K> *>(mp)};
   return cuda_ok(cudaLaunchKernel((const void *)k_gate_tile<T, K>, dim3((unsigned)n_tiles),
