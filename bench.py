@@ -218,18 +218,20 @@ def run_reference(args):
     samples = []
     for _ in range(args.warmup):
         cpu_baseline_run(n_cpu, gates, args.precision, args.cpu_budget / 4, threads)
-    passes_tot = 0
+    passes_tot, el_tot = 0, 0.0
     for _ in range(args.steps):
         gbs, passes, el = cpu_baseline_run(n_cpu, gates, args.precision, args.cpu_budget, threads)
         samples.append(gbs)
         passes_tot += passes
+        el_tot += el
     v = float(np.mean(samples))
     sample = (f"{n_cpu}-qubit brickwork depth {args.depth} fused k={args.k}, "
-              f"{passes_tot} fused-gate passes over {args.steps} steps of ~{args.cpu_budget:.0f} s")
+              f"{passes_tot} fused-gate passes over {args.steps} steps of ~{args.cpu_budget:g} s")
     line = {
         "impl": "reference", "metric": "HBM GB/s (fused-gate statevector passes)", "value": v,
         "unit": "GB/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "higher_is_better": True, "dtype": args.precision, "data": "synthetic",
+        "ms_per_step": el_tot / max(args.steps, 1) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "dtype": args.precision, "data": "synthetic",
         "config": {"workload": f"brickwork-{args.n}q-d{args.depth}-{'c128' if args.precision == 'f64' else 'c64'}"
                    f"-k{args.k}", "cpu_sample_qubits": n_cpu},
         "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "port",
