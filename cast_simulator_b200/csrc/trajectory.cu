@@ -1083,6 +1083,9 @@ int cast_b200_traj_run_range(void *prog, uint32_t first, uint32_t n_traj, uint64
                                   cudaMemcpyDeviceToHost, s),
                   "cudaMemcpyAsync (samples)", err)) ||
         !cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize (trajectories)", err)) {
+      // The kernel may already be queued: let it finish before returning, so
+      // that no buffer of this program is handed on (buffer cache) in use.
+      cudaStreamSynchronize(s);
       cb2::write_err(err_buf, err_buf_len, err);
       return 1;
     }
