@@ -122,12 +122,12 @@ class ServingEngine:
         self._t0 = time.perf_counter()
         self._work: collections.deque = collections.deque()
         self._work_cv = threading.Condition()
+        self.max_concurrent = 0
         self._workers = [threading.Thread(target=self._worker, daemon=True) for _ in range(max_slots)]
         self._dispatcher = threading.Thread(target=self._dispatch, daemon=True)
         for t in self._workers:
             t.start()
         self._dispatcher.start()
-        self.max_concurrent = 0
 
     # -- public API
     def now(self) -> float:
@@ -139,6 +139,8 @@ class ServingEngine:
             raise ValueError(f"request needs {need} bytes, above the device-memory budget {self.budget}")
         fut: Future = Future()
         with self._cv:
+            if self._stop:
+                raise RuntimeError("the serving engine has been shut down")
             self._pending.append((req, fut, self.now()))
             self._cv.notify_all()
         return fut
@@ -155,9 +157,15 @@ class ServingEngine:
         return [f.result() for f in futs]
 
     def shutdown(self) -> None:
+        """Stop admitting: requests already admitted run to completion, requests
+        still waiting for admission fail with RuntimeError."""
         with self._cv:
             self._stop = True
+            pending = list(self._pending)
+            self._pending.clear()
             self._cv.notify_all()
+        for _, fut, _ in pending:
+            fut.set_exception(RuntimeError("the serving engine was shut down before admission"))
         with self._work_cv:
             self._work_cv.notify_all()
         self._dispatcher.join(timeout=30)
@@ -227,12 +235,21 @@ class ServingEngine:
         L.check(L.lib().cast_b200_program_add_fused(prog.handle, fused.handle, eb, L.ERR_LEN), eb,
                 "program_add_fused")
         sv = self._pool.get(n, req.precision)
+        ok = False
         try:
             sv.zero(stream)
             prog.run(sv, stream, self.use_graph)
             p1, nrm = qubit_populations(sv, stream)
+            ok = True
             return (nrm - 2.0 * p1) / nrm
         finally:
+            if not ok:
+                # work of a failed request may still be queued on this stream:
+                # let it drain before another worker can take the statevector
+                try:
+                    stream.sync()
+                except Exception:
+                    pass
             self._pool.put(sv)
 
 

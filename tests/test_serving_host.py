@@ -1,6 +1,8 @@
 """Host-side logic of the serving loop, without a GPU: the arrival stream the
 bench draws, the admission charge of a request, and the single-server FIFO
-model the sequential plain-path baseline uses."""
+model the sequential plain-path baseline uses, and the scheduler (admission by
+memory and slots in arrival order, failure isolation, shutdown) with the
+device work replaced by a host fake."""
 import numpy as np
 import pytest
 
@@ -48,3 +50,117 @@ def test_sequential_fifo_model():
     summ = S.latency_summary([0.010, 0.020, 0.030, 0.040])
     assert summ["n"] == 4 and summ["p50_ms"] == pytest.approx(25.0)
     assert summ["mean_ms"] == pytest.approx(25.0) and summ["p99_ms"] <= 40.0
+
+
+# ── the scheduler, with the device work replaced by a fake ──────────────────
+
+
+class _FakeStream:
+    def sync(self):
+        pass
+
+
+@pytest.fixture
+def fake_engine(monkeypatch):
+    """A ServingEngine whose per-request work is a short sleep on the host: it
+    records the order requests start in and the largest number running at once,
+    and raises for requests whose seed is negative."""
+    import threading
+    import time
+
+    state = {"running": 0, "peak": 0, "order": [], "lock": threading.Lock()}
+
+    def execute(self, req, stream):
+        with state["lock"]:
+            state["running"] += 1
+            state["peak"] = max(state["peak"], state["running"])
+            state["order"].append(req.rid)
+        try:
+            time.sleep(0.02)
+            if req.seed < 0:
+                raise RuntimeError(f"request {req.rid} failed")
+            return np.full(req.circuit.n_qubits(), float(req.rid))
+        finally:
+            with state["lock"]:
+                state["running"] -= 1
+
+    monkeypatch.setattr(S, "Stream", _FakeStream)
+    monkeypatch.setattr(S.ServingEngine, "_execute", execute)
+    engines = []
+
+    def make(**kw):
+        eng = S.ServingEngine(**kw)
+        engines.append(eng)
+        return eng
+
+    yield make, state
+    for eng in engines:
+        eng.shutdown()
+
+
+def _reqs(n_qubits, count, prec=CudaPrecision.F64, seeds=None):
+    c = QuantumCircuit.brickwork(n_qubits, 2, 1)
+    return [S.Request(c, prec, 0, (seeds or {}).get(i, i), 0.0, i) for i in range(count)]
+
+
+def test_admission_is_bounded_by_the_memory_budget(fake_engine):
+    make, state = fake_engine
+    one = 16 << 20  # a 20-qubit complex128 statevector
+    eng = make(max_slots=8, mem_budget_bytes=int(2.5 * one))
+    res = [f.result(timeout=30) for f in [eng.submit(r) for r in _reqs(20, 8)]]
+    assert [r.rid for r in res] == list(range(8))
+    assert all(np.all(r.z == r.rid) for r in res)
+    assert state["peak"] <= 2 and eng.max_concurrent <= 2
+    assert all(r.admitted >= r.arrival and r.finished >= r.admitted for r in res)
+    assert eng._in_use == 0 and eng._active == 0
+
+
+def test_admission_is_bounded_by_slots_and_keeps_arrival_order(fake_engine):
+    make, state = fake_engine
+    eng = make(max_slots=3, mem_budget_bytes=1 << 40)
+    futs = [eng.submit(r) for r in _reqs(12, 12)]
+    for f in futs:
+        f.result(timeout=30)
+    assert state["peak"] <= 3 and eng.max_concurrent == 3
+    # admission never reorders: with one slot, requests start in submission order
+    make2, state2 = fake_engine
+    state["order"].clear()
+    eng1 = make2(max_slots=1, mem_budget_bytes=1 << 40)
+    for f in [eng1.submit(r) for r in _reqs(10, 6)]:
+        f.result(timeout=30)
+    assert state["order"] == list(range(6))
+
+
+def test_a_failing_request_does_not_stop_the_engine(fake_engine):
+    make, state = fake_engine
+    eng = make(max_slots=2, mem_budget_bytes=1 << 40)
+    futs = [eng.submit(r) for r in _reqs(10, 6, seeds={2: -1})]
+    for i, f in enumerate(futs):
+        if i == 2:
+            with pytest.raises(RuntimeError, match="request 2 failed"):
+                f.result(timeout=30)
+        else:
+            assert f.result(timeout=30).rid == i
+    assert eng._in_use == 0 and eng._active == 0
+
+
+def test_oversized_requests_and_shutdown(fake_engine):
+    make, state = fake_engine
+    eng = make(max_slots=1, mem_budget_bytes=(16 << 20) + 1)
+    with pytest.raises(ValueError, match="budget"):
+        eng.submit(_reqs(21, 1)[0])
+    futs = [eng.submit(r) for r in _reqs(20, 5)]
+    futs[0].result(timeout=30)
+    eng.shutdown()
+    done = failed = 0
+    for f in futs:
+        try:
+            f.result(timeout=30)
+            done += 1
+        except RuntimeError as e:
+            assert "shut down" in str(e)
+            failed += 1
+    # admitted requests finish, the rest fail instead of waiting for ever
+    assert done >= 1 and done + failed == 5
+    with pytest.raises(RuntimeError, match="shut down"):
+        eng.submit(_reqs(20, 1)[0])
