@@ -151,7 +151,7 @@ class ShardedStatevector:
         """<Z_q> for every logical qubit, every rank (FP64 all-reduce)."""
         import torch
 
-        p = (self.shard.abs() ** 2).to(torch.float64)
+        p = torch.view_as_real(self.shard).to(torch.float64).square().sum(-1)  # |psi|^2 in FP64
         ones = torch.zeros(self.n + 1, dtype=torch.float64, device=p.device)
         idx = torch.arange(1 << self.n_local, device=p.device)
         for pos in range(self.n_local):
