@@ -250,7 +250,9 @@ def test_trajectories_leave_gate_throughput_alone(mods):
     TR.TrajectoryProgram(T.QuantumCircuit.brickwork(16, 10, 1, depolarizing=1e-3, damping=5e-4), 3).run(
         1024, 1, st)
     after = best_time()
-    assert after < 1.3 * before, (before, after)
+    # the slowdown this guards against was 2x or more; the margin leaves room
+    # for SM clock changes under the power cap between the two measurements
+    assert after < 1.5 * before, (before, after)
 
 
 @pytest.mark.parametrize("n", [12, 16])
