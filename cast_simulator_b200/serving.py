@@ -24,7 +24,6 @@ steady-state admission does not call cudaMalloc.
 from __future__ import annotations
 
 import collections
-import math
 import threading
 import time
 from concurrent.futures import Future

@@ -3,7 +3,6 @@
 Tolerances are the reference's (tests/cpu_cuda_compare.rs:27, 397): 1e-10 per
 amplitude for FP64, 1e-5 for FP32; 1e-9 for sequential circuits
 (tests/circuit_execution_order.rs:34)."""
-import json
 import os
 
 import numpy as np

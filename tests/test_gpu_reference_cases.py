@@ -10,7 +10,6 @@
   * tests/circuit_execution_order.rs: random 1q/2q Haar circuits with syncs split
     through the sequence (:238-325), 1e-9;
   * tests/density_matrix.rs: depolarizing with p = 0 is the identity (:115-129)."""
-import math
 
 import numpy as np
 import pytest

@@ -1,5 +1,4 @@
 """Host-side gate algebra and circuit builders of the product vs the oracle."""
-import math
 
 import numpy as np
 import pytest
