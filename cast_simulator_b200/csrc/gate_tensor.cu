@@ -73,7 +73,6 @@ bool tma_enabled() { return g_tensor_loader.load() != 1; }
 template <int K, bool kStage> struct UmCfg {
   static constexpr int D = 1 << K;
   static constexpr int R = 2 * D;                          // reals per group: MMA N and K extent
-  static constexpr int CH = D / 4;                         // 16-byte chunks (4 members) per group
   static constexpr int KH = D / kStageMembers;             // stages (K atoms) per tile
   static constexpr int LG = kStages;                       // loader groups: one per stage
   static constexpr int GS = kLoadThreads / LG;             // threads per loader group: one per group row
