@@ -46,8 +46,8 @@ def measured_peak_hbm():
 
 
 def measured_peak_bf16():
-    """Dense BF16 TFLOP/s (burst) from the driver's measurement, else the pool's
-    earlier measurement."""
+    """Dense BF16 TFLOP/s (burst) from MEASURED_PEAKS.json, else an earlier
+    cuBLAS measurement on a B200 (1590)."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             return float(json.load(f)["bf16_tflops"])
@@ -122,7 +122,8 @@ def build_fused(n: int, depth: int, k: int, seed: int = 2024):
 
 def _cpu_baseline_lib():
     """The threaded SIMD CPU restatement of CAST's CPU kernels (oracle/), built
-    on first use: the timed CPU baseline and the checker of the GPU result."""
+    on first use: the timed CPU baseline, and the FP64 result the GPU output is
+    compared with."""
     import ctypes as C
 
     from oracle import oracle as O

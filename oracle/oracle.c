@@ -2,7 +2,7 @@
  * CPU parity oracle for the gate-application path.  TEST INFRASTRUCTURE ONLY:
  * this file is a scalar FP64 restatement of the reference simulator's CPU
  * semantics (narix10yc/cast_simulator, a Rust crate) and is only ever loaded by
- * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg as the checker.
+ * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg, to check results.
  * The product (cast_simulator_b200) never links, imports or calls it.
  *
  * Every routine cites the reference code it restates (path:line inside the

@@ -1,6 +1,6 @@
 """ctypes front end of the CPU parity oracle (oracle/oracle.c).
 
-TEST INFRASTRUCTURE ONLY.  This module is the checker: tests/,
+TEST INFRASTRUCTURE ONLY.  This module checks results: tests/,
 ``__graft_entry__.smoke()`` and the ``cpu_baseline`` leg of ``bench.py`` may
 import it; the product package ``cast_simulator_b200`` never does.
 
@@ -217,7 +217,7 @@ def inner(a: np.ndarray, b: np.ndarray) -> complex:
 
 
 def fidelity_report(ref: np.ndarray, got: np.ndarray) -> dict:
-    """1-|<ref|got>| (the north-star form), 1-|<ref|got>|^2 (the reference's
+    """1-|<ref|got>| (the form every result reports), 1-|<ref|got>|^2 (the reference's
     fidelity, cpu/statevector.rs:363-374) and the max amplitude error."""
     ov = inner(ref, got)
     return {
