@@ -157,3 +157,47 @@ def test_gate_engine_routing(cblib):
     assert gate_engine(mono(6), (15, 10, 11, 12, 13, 14), 20, F64) == "sparse"
     with pytest.raises(RuntimeError, match="outside"):
         gate_engine(haar(2), (0, 25), 20, F64)
+
+
+def test_compile_is_reentrant(cblib):
+    """The reference compiles gates from several worker threads at once
+    (cuda/kernel.rs:1078-1096): concurrent calls give exactly the descriptors
+    that serial calls give (ctypes drops the GIL around each call)."""
+    import threading
+
+    rng = np.random.default_rng(11)
+    jobs = []
+    for _ in range(160):
+        k = int(rng.integers(1, 5))
+        q = np.sort(rng.choice(20, size=k, replace=False))
+        d = 1 << k
+        jobs.append((rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d)), q,
+                     int(rng.integers(0, 2))))
+
+    def descriptor(job):
+        m, q, prec = job
+        rc, err, ptx, fn, k, pr = _compile(cblib, m, q, prec)
+        assert rc == 0, err
+        text = C.string_at(ptx.value)
+        cblib.cast_cuda_str_free(ptx)
+        cblib.cast_cuda_str_free(fn)
+        return text, k, pr
+
+    serial = [descriptor(j) for j in jobs]
+    out = [None] * len(jobs)
+    errors = []
+
+    def worker(t):
+        try:
+            for i in range(t, len(jobs), 8):
+                out[i] = descriptor(jobs[i])
+        except Exception as e:  # reported below, on the test's thread
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(t,)) for t in range(8)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    assert out == serial
