@@ -290,6 +290,13 @@ int cast_b200_program_run(void *program, uint64_t sv_dptr, void *stream, int use
     write_err(err_buf, err_buf_len, "invalid program handle or statevector");
     return 1;
   }
+  {
+    std::string err;
+    if (!cb2::aligned16(sv_dptr, "statevector pointer", err)) {
+      write_err(err_buf, err_buf_len, err);
+      return 1;
+    }
+  }
   try {
     std::lock_guard<std::mutex> lock(p->mu);
     std::string err;

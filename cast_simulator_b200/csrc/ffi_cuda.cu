@@ -376,6 +376,13 @@ void *cast_cuda_cubin_load(const uint8_t *cubin_data, size_t cubin_len, char *er
     write_err(err_buf, err_buf_len, "cubinData must not be null");
     return nullptr;
   }
+  // The caller passes the blob's full length (the reference's Rust caller hands
+  // over cubin.len(), cuda/kernel.rs:313-319); nothing is read beyond it, so a
+  // length of 0 or one shorter than the header is refused before any read.
+  if (cubin_len < sizeof(BlobHeader)) {
+    write_err(err_buf, err_buf_len, "gate module is truncated (shorter than its header)");
+    return nullptr;
+  }
   try {
     BlobHeader h;
     std::memcpy(&h, cubin_data, sizeof(h));
@@ -384,7 +391,7 @@ void *cast_cuda_cubin_load(const uint8_t *cubin_data, size_t cubin_len, char *er
       write_err(err_buf, err_buf_len, "not a cast_b200 gate module");
       return nullptr;
     }
-    if (cubin_len != 0 && cubin_len < sizeof(h) + h.n_scalars * sizeof(double)) {
+    if (cubin_len < sizeof(h) + h.n_scalars * sizeof(double)) {
       write_err(err_buf, err_buf_len, "gate module is truncated");
       return nullptr;
     }

@@ -913,6 +913,7 @@ bool launch_gate(const GateData &g, void *sv, uint32_t n, cudaStream_t stream, s
     err = "statevector pointer must not be null";
     return false;
   }
+  if (!aligned16(reinterpret_cast<uint64_t>(sv), "statevector pointer", err)) return false;
   if (g.d_tc) return launch_gate_tensor(g, sv, n, stream, err);
   Targets t;
   for (uint32_t b = 0; b < kMaxGateQubits; ++b) {

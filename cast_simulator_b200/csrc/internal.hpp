@@ -44,6 +44,18 @@ inline void clear_err(char *buf, size_t len) {
   if (buf && len) buf[0] = '\0';
 }
 
+// Every kernel reads amplitudes as 16-byte vectors (double2 / float4), so a
+// device pointer handed in through the C ABI must be 16-byte aligned (every
+// cudaMalloc result is 256-byte aligned; an interior pointer may not be).
+// Returns false and fills `err` for a misaligned pointer; null passes (the
+// callers check for null with their own messages).
+inline bool aligned16(uint64_t dptr, const char *what, std::string &err) {
+  if ((dptr & 15u) == 0) return true;
+  err = std::string(what) + " must be 16-byte aligned (got an address ending in 0x" +
+        "0123456789abcdef"[dptr & 15u] + ")";
+  return false;
+}
+
 // Validates the gate against an n-qubit statevector.
 bool check_gate(const GateData &g, uint32_t n, std::string &err);
 

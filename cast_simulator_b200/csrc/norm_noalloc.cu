@@ -2,15 +2,16 @@
 //
 // cast_cuda_norm_squared keeps its per-block partial sums in a device buffer
 // that the library allocates with cudaMalloc on first use.  Some callers
-// cannot let a library allocate device memory: code running inside a CUDA
-// stream capture (where cudaMalloc is not allowed), applications whose
-// device memory is owned by a pool or arena that must account for every byte,
-// and hosts that forbid hidden allocations after start-up.  This entry point
-// serves them: its scratch is a file-scope __device__ array of fixed size,
-// created when the library is loaded onto a device and held until the process
-// exits (kNoAllocPartials + 1 doubles, about 1 MiB, on every GPU that loads
-// the library).  It calls no cudaMalloc / cudaFree and no allocating library
-// routine.
+// cannot let a library allocate device memory: applications whose device
+// memory is owned by a pool or arena that must account for every byte (an
+// allocation behind its back can push the pool past its budget), and hosts
+// that forbid allocations once they are running (cudaMalloc and cudaFree may
+// synchronise the whole device, which stalls every other stream of a
+// latency-bound service).  This entry point serves them: its scratch is a
+// file-scope __device__ array of fixed size, created when the library is
+// loaded onto a device and held until the process exits (kNoAllocPartials + 1
+// doubles, about 1 MiB, on every GPU that loads the library).  It calls no
+// cudaMalloc / cudaFree and no allocating library routine.
 //
 // Each block of the first pass reduces a fixed chunk of 256 threads x 64
 // 128-bit vectors and writes one partial; the second pass folds the partials
@@ -21,6 +22,8 @@
 // overlap on the GPU (different streams, no ordering between them) race on it.
 #include "../../include/cast_b200.h"
 #include "internal.hpp"
+
+#include <cuda.h>
 
 #include <mutex>
 
@@ -91,10 +94,38 @@ __global__ void __launch_bounds__(1024) k_na_pass2(double *__restrict__ partials
   if (threadIdx.x == 0) partials[kNoAllocPartials] = acc;
 }
 
-// Device address of g_noalloc_scratch, resolved once per device with that
-// device current (in host code the symbol itself is only a host-side handle).
+// Device address of g_noalloc_scratch.  In host code the symbol is only a
+// host-side handle, so the address is looked up with cudaGetSymbolAddress, with
+// the device current, once per device: the set-up step, taken by the first
+// call on each device.  The address belongs to the device's context; a
+// cudaDeviceReset destroys that context and the next one may load the array
+// elsewhere.  So each entry also records the unique ID of the context it was
+// resolved in, and a call that finds a different context (after a reset)
+// resolves the address again.  The driver calls go through
+// cudaGetDriverEntryPoint, so the library needs no link against libcuda.
+using PfnCtxGetCurrent = CUresult (*)(CUcontext *);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long *);
+
+struct ScratchEntry {
+  double *addr = nullptr;
+  unsigned long long ctx_id = 0;
+};
+
 std::mutex g_na_mu;
-double *g_na_addr[kMaxDevices] = {nullptr};
+ScratchEntry g_na_table[kMaxDevices];
+PfnCtxGetCurrent g_ctx_get_current = nullptr;
+PfnCtxGetId g_ctx_get_id = nullptr;
+
+// The unique ID of the calling thread's current context, or 0 when there is
+// none (or the driver cannot tell).
+unsigned long long current_context_id() {
+  if (!g_ctx_get_current || !g_ctx_get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (g_ctx_get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 bool scratch_address(double **out, std::string &err) {
   int dev = 0;
@@ -104,14 +135,32 @@ bool scratch_address(double **out, std::string &err) {
     return false;
   }
   std::lock_guard<std::mutex> lock(g_na_mu);
-  if (!g_na_addr[dev]) {
-    void *p = nullptr;
-    if (!cb2::cuda_ok(cudaGetSymbolAddress(&p, g_noalloc_scratch),
-                      "cudaGetSymbolAddress (allocation-free scratch)", err))
-      return false;
-    g_na_addr[dev] = static_cast<double *>(p);
+  if (!g_ctx_get_current || !g_ctx_get_id) {
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSuccess, q2 = q1;
+    void *f1 = nullptr, *f2 = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+        q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+      g_ctx_get_current = reinterpret_cast<PfnCtxGetCurrent>(f1);
+      g_ctx_get_id = reinterpret_cast<PfnCtxGetId>(f2);
+    }
+    (void)cudaGetLastError();
   }
-  *out = g_na_addr[dev];
+  ScratchEntry &e = g_na_table[dev];
+  if (e.addr) {
+    const unsigned long long id = current_context_id();
+    if (id != 0 && id == e.ctx_id) {
+      *out = e.addr;
+      return true;
+    }
+  }
+  void *p = nullptr;
+  if (!cb2::cuda_ok(cudaGetSymbolAddress(&p, g_noalloc_scratch),
+                    "cudaGetSymbolAddress (allocation-free scratch)", err))
+    return false;
+  e.addr = static_cast<double *>(p);
+  e.ctx_id = current_context_id();  // 0 (never matches): resolve again on every call
+  *out = e.addr;
   return true;
 }
 
@@ -152,6 +201,10 @@ extern "C" int cast_b200_norm_squared_noalloc(uint64_t dptr, size_t n_elements, 
     return 1;
   }
   std::string err;
+  if (!cb2::aligned16(dptr, "dptr", err)) {
+    cb2::write_err(err_buf, err_buf_len, err);
+    return 1;
+  }
   const bool ok =
       precision == 0
           ? norm_noalloc<float>(reinterpret_cast<const void *>(dptr), n_elements, out_norm_sq,

@@ -357,24 +357,30 @@ bool dm_impl(const void *rho, uint32_t n, double *out, cudaStream_t s, std::stri
 
 bool norm_squared(const void *x, uint64_t n_scalars, uint8_t precision, double *out,
                   cudaStream_t s, std::string &err) {
+  if (!aligned16(reinterpret_cast<uint64_t>(x), "statevector pointer", err)) return false;
   return precision == 0 ? norm_sq_impl<float>(x, n_scalars, out, s, err)
                         : norm_sq_impl<double>(x, n_scalars, out, s, err);
 }
 
 bool scale(void *x, uint64_t n_scalars, uint8_t precision, double factor, cudaStream_t s,
            std::string &err) {
+  if (!aligned16(reinterpret_cast<uint64_t>(x), "statevector pointer", err)) return false;
   return precision == 0 ? scale_impl<float>(x, n_scalars, factor, s, err)
                         : scale_impl<double>(x, n_scalars, factor, s, err);
 }
 
 bool inner_product(const void *a, const void *b, uint32_t n, uint8_t precision, double *re,
                    double *im, cudaStream_t s, std::string &err) {
+  if (!aligned16(reinterpret_cast<uint64_t>(a), "first statevector pointer", err) ||
+      !aligned16(reinterpret_cast<uint64_t>(b), "second statevector pointer", err))
+    return false;
   return precision == 0 ? inner_impl<float>(a, b, n, re, im, s, err)
                         : inner_impl<double>(a, b, n, re, im, s, err);
 }
 
 bool qubit_populations(const void *x, uint32_t n, uint8_t precision, double *p1, double *norm,
                        cudaStream_t s, std::string &err) {
+  if (!aligned16(reinterpret_cast<uint64_t>(x), "statevector pointer", err)) return false;
   if (n > kMaxPopQubits) {
     err = "populations support at most 40 qubits";
     return false;
@@ -385,6 +391,7 @@ bool qubit_populations(const void *x, uint32_t n, uint8_t precision, double *p1,
 
 bool marginal_probabilities(const void *x, uint32_t n, uint8_t precision, const uint32_t *measured,
                             uint32_t m, double *out, cudaStream_t s, std::string &err) {
+  if (!aligned16(reinterpret_cast<uint64_t>(x), "statevector pointer", err)) return false;
   if (m == 0 || m > 12) {
     err = "between 1 and 12 measured qubits are supported";
     return false;
@@ -400,6 +407,7 @@ bool marginal_probabilities(const void *x, uint32_t n, uint8_t precision, const 
 
 bool dm_populations(const void *rho, uint32_t n, uint8_t precision, double *out, cudaStream_t s,
                     std::string &err) {
+  if (!aligned16(reinterpret_cast<uint64_t>(rho), "density-matrix pointer", err)) return false;
   if (2 * n > kMaxSvQubits) {
     err = "density matrix too large";
     return false;

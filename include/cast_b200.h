@@ -221,17 +221,20 @@ int cast_b200_traj_run_range(void *program, uint32_t first, uint32_t n_traj, uin
 
 /* -- Allocation-free norm^2 -------------------------------------------------------
  * No counterpart in the reference: an extra variant of cast_cuda_norm_squared
- * for callers that cannot let a library allocate device memory (work recorded
- * inside a CUDA stream capture, memory owned by a pool or arena that accounts
- * for every byte, hosts that forbid allocations after start-up).  Same result
+ * for callers that cannot let a library allocate device memory: applications
+ * whose device memory is owned by a pool or arena that accounts for every byte,
+ * and hosts that forbid allocations once running (cudaMalloc / cudaFree may
+ * synchronise the whole device and stall their other streams).  Same result
  * (sum of squares of n_elements scalars, FP64 accumulation, written to the host
- * double *out_norm_sq; synchronous on `stream`, NULL = legacy default stream),
- * but the scratch is a fixed array inside the library (about 1 MiB per GPU,
- * held until the process exits) and no memory is allocated.  Limit:
+ * double *out_norm_sq; the call waits for it on `stream`, NULL = legacy default
+ * stream), but the scratch is a fixed array inside the library (about 1 MiB per
+ * GPU, held until the process exits) and no memory is allocated.  Limit:
  * n_elements <= 2^32 (F64) / 2^33 (F32), i.e. 32 GiB of amplitudes; larger
- * inputs are rejected with an error.  The first call on each device resolves
- * the array's device address (do it before any stream capture).  Calls whose
- * kernels may overlap on the GPU share the array and race; order them. */
+ * inputs are rejected with an error.  dptr must be 16-byte aligned.  The first
+ * call on each device (and the first after a cudaDeviceReset) looks up the
+ * array's device address; make that first call before any stream capture.
+ * Calls whose kernels may overlap on the GPU share the array and race; order
+ * them. */
 int cast_b200_norm_squared_noalloc(uint64_t dptr, size_t n_elements, uint8_t precision,
                                    double *out_norm_sq, void *stream, char *err_buf,
                                    size_t err_buf_len);

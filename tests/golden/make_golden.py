@@ -2,7 +2,7 @@
 
 Run in a container where the reference checkout is mounted:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path to the reference checkout>
 
 It reads ``tests/assets/qft_14.qasm`` of narix10yc/cast_simulator (the QFT with
 each controlled phase decomposed into CX + u3 phases, qft_14.qasm:3-8), runs it
@@ -127,4 +127,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path to the reference checkout>")
+    main(sys.argv[1])

@@ -91,6 +91,29 @@ def test_bad_descriptor_rejected(cblib):
     assert b"must not be null" in eb.value
 
 
+def test_truncated_blob_rejected_before_any_read(cblib):
+    """cubin_load never reads past the length it is given: a length of 0, one
+    shorter than the header, and one that cuts the matrix short are refused
+    (these return before the device is touched, so they run without a GPU)."""
+    from cast_simulator_b200 import _lib as L
+
+    rc, _, ptx, fn, *_ = _compile(cblib, np.eye(4), [0, 1])
+    assert rc == 0
+    blob, ln = C.c_void_p(), C.c_size_t()
+    eb = L.errbuf()
+    assert cblib.cast_cuda_ptx_to_cubin(C.string_at(ptx.value), C.byref(blob), C.byref(ln), eb,
+                                        L.ERR_LEN) == 0
+    raw = C.string_at(blob.value, ln.value)
+    for n in (0, 16, ln.value - 1):
+        buf = C.create_string_buffer(raw[:n], max(n, 1))
+        eb = L.errbuf()
+        assert cblib.cast_cuda_cubin_load(buf, n, eb, L.ERR_LEN) is None
+        assert b"truncated" in eb.value, (n, eb.value)
+    cblib.cast_cuda_cubin_free(blob)
+    cblib.cast_cuda_str_free(ptx)
+    cblib.cast_cuda_str_free(fn)
+
+
 def test_trajectory_threads_setting(cblib):
     """Trajectory programs are built on the host; the launch-shape knob accepts
     512, 1024 and 0 (by state size) threads and any CTA count."""
@@ -201,3 +224,35 @@ def test_compile_is_reentrant(cblib):
         t.join()
     assert not errors, errors
     assert out == serial
+
+
+def test_misaligned_pointers_rejected_without_touching_the_device(cblib):
+    """Every kernel reads amplitudes as 16-byte vectors, so an interior pointer
+    that is not 16-byte aligned is refused with an error instead of reaching a
+    kernel.  The check comes before any CUDA call, so this runs without a GPU;
+    the fake address is never dereferenced."""
+    from cast_simulator_b200 import _lib as L
+
+    bad = 0x10000008
+    eb = L.errbuf()
+    m = np.ascontiguousarray(np.eye(2, dtype=np.complex128))
+    q = np.zeros(1, dtype=np.uint32)
+    out = (C.c_double * 64)()
+    re, im = C.c_double(), C.c_double()
+    calls = [
+        lambda: cblib.cast_b200_apply_gate(bad, 4, 1, m.view(np.float64).ctypes.data_as(
+            C.POINTER(L.Complex64)), q.ctypes.data_as(L.c_u32p), 1, 1e-12, 1e-12, None, eb, L.ERR_LEN),
+        lambda: cblib.cast_cuda_norm_squared(bad, 32, 1, out, eb, L.ERR_LEN),
+        lambda: cblib.cast_cuda_scale(bad, 32, 0, 2.0, eb, L.ERR_LEN),
+        lambda: cblib.cast_b200_inner_product(0x10000000, bad, 4, 1, C.byref(re), C.byref(im), None,
+                                              eb, L.ERR_LEN),
+        lambda: cblib.cast_b200_qubit_populations(bad, 4, 1, out, None, None, eb, L.ERR_LEN),
+        lambda: cblib.cast_b200_marginal_probabilities(bad, 4, 1, q.ctypes.data_as(L.c_u32p), 1, out,
+                                                       None, eb, L.ERR_LEN),
+        lambda: cblib.cast_b200_dm_populations(bad, 2, 1, out, None, eb, L.ERR_LEN),
+        lambda: cblib.cast_b200_norm_squared_noalloc(bad, 32, 1, out, None, eb, L.ERR_LEN),
+    ]
+    for i, call in enumerate(calls):
+        eb.value = b""
+        assert call() == 1, i
+        assert b"16-byte aligned" in eb.value, (i, eb.value)
