@@ -15,6 +15,14 @@ reference's size-only fusion at width k (default 4), complex128 statevector
            matrices uploaded from host, run, <Z_q> for every qubit read back.
   roofline / cpu_baseline / clocks: see the JSON keys.
 
+Keys beside the headline (rank 0, one GPU): c2_complex64 (the same 30-qubit
+circuit in complex64, with its own roofline), qft (22-qubit QFT-CX), fusion_sweep
+(k = 2..7, both precisions, tensor cores at k = 5, 6), tensor_path, largest_fit
+(34-qubit complex64 / 33-qubit complex128, fidelity of a 28-qubit prefix against
+the FP64 CPU restatement run in the same process), trajectories (persistent
+kernel vs host-driven plain path vs exact density matrix) and serving (Poisson
+streams at swept rates vs the same engine one request at a time).
+
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
        [--precision f64|f32] [--k 4] [--n 30] [--depth 20]
 """
@@ -120,16 +128,32 @@ def build_fused(n: int, depth: int, k: int, seed: int = 2024):
     return circ, g.gates_in_row_order()
 
 
+_CB_LIB = None
+
+
 def _cpu_baseline_lib():
     """The threaded SIMD CPU restatement of CAST's CPU kernels (oracle/), built
     on first use: the timed CPU baseline, and the FP64 result the GPU output is
-    compared with."""
+    compared with.  It is compiled here with -march=native for the host cores
+    that run it; if that build fails, the portable x86-64-v3 build is used.
+    Returns (library, compiler flags)."""
+    global _CB_LIB
+    if _CB_LIB is not None:
+        return _CB_LIB
     import ctypes as C
 
     from oracle import oracle as O
 
     O.build()
-    lib = C.CDLL(os.path.join(ROOT, "oracle", "build", "libcpu_baseline.so"))
+    flags, path = "-O3 -march=x86-64-v3", os.path.join(ROOT, "oracle", "build", "libcpu_baseline.so")
+    try:
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "native"], check=True,
+                       capture_output=True, timeout=300)
+        flags, path = "-O3 -march=native", os.path.join(ROOT, "oracle", "build",
+                                                         "libcpu_baseline_native.so")
+    except Exception:
+        pass
+    lib = C.CDLL(path)
     lib.cb_alloc.restype = C.c_void_p
     lib.cb_alloc.argtypes = [C.c_uint32, C.c_int]
     lib.cb_free.argtypes = [C.c_void_p]
@@ -137,23 +161,19 @@ def _cpu_baseline_lib():
     lib.cb_store.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     lib.cb_apply.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint32), C.c_uint32,
                              C.c_int]
-    return lib
+    _CB_LIB = (lib, flags)
+    return _CB_LIB
 
 
-def cpu_parity(n: int, depth: int, k: int, precision: str, threads: int) -> dict:
-    """Parity of the GPU result against CAST's FP64 CPU statevector path (its
-    restatement in oracle/): the benchmark's brickwork construction at n qubits,
-    fused at width k, run once from |0> on the CPU in FP64 and on the GPU in the
-    benchmark's precision through the public gate-program API."""
+def cpu_reference_state(n: int, gates, threads: int) -> np.ndarray:
+    """Final amplitudes (complex128) of a gate list applied to |0...0> by the FP64
+    CPU restatement of CAST's statevector path, with `threads` host threads."""
     import ctypes as C
 
-    from cast_simulator_b200 import cuda as cu
-
-    lib = _cpu_baseline_lib()
-    _, gates = build_fused(n, depth, k)
+    lib, _ = _cpu_baseline_lib()
     sv = lib.cb_alloc(n, 0)
     if not sv:
-        raise MemoryError("cpu parity allocation failed")
+        raise MemoryError("cpu reference allocation failed")
     try:
         lib.cb_zero(sv)
         for g in gates:
@@ -165,14 +185,33 @@ def cpu_parity(n: int, depth: int, k: int, precision: str, threads: int) -> dict
         lib.cb_store(sv, ref.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
     finally:
         lib.cb_free(sv)
+    return ref
+
+
+def fidelity_vs(ref: np.ndarray, psi: np.ndarray) -> dict:
+    """1 - |<ref|psi>| (psi renormalised), max amplitude error and norm drift."""
+    nrm = float(np.linalg.norm(psi))
+    ov = abs(np.vdot(ref, psi)) / (float(np.linalg.norm(ref)) * nrm)
+    return {"one_minus_abs_overlap": float(1.0 - ov), "max_abs_err": float(np.max(np.abs(ref - psi))),
+            "norm_drift": float(1.0 - nrm)}
+
+
+def cpu_parity(n: int, depth: int, k: int, precision: str, threads: int) -> dict:
+    """Parity of the GPU result against CAST's FP64 CPU statevector path (its
+    restatement in oracle/): the benchmark's brickwork construction at n qubits,
+    fused at width k, run once from |0> on the CPU in FP64 and on the GPU in the
+    benchmark's precision through the public gate-program API."""
+    from cast_simulator_b200 import cuda as cu
+
+    _, gates = build_fused(n, depth, k)
+    ref = cpu_reference_state(n, gates, threads)
     prec = cu.CudaPrecision.F64 if precision == "f64" else cu.CudaPrecision.F32
     _, gsv = _run_fused(n, gates, prec, reps=1)
     psi = gsv.download()
-    ov = abs(np.vdot(ref, psi)) / (np.linalg.norm(ref) * np.linalg.norm(psi))
+    rep = fidelity_vs(ref, psi)
     return {"workload": f"brickwork-{n}q-d{depth} fused k={k} ({len(gates)} passes), from |0>",
             "reference": "FP64 CPU restatement of CAST's statevector path",
-            "one_minus_abs_overlap": float(1.0 - ov),
-            "max_abs_err": float(np.max(np.abs(ref - psi)))}
+            "one_minus_abs_overlap": rep["one_minus_abs_overlap"], "max_abs_err": rep["max_abs_err"]}
 
 
 def cpu_baseline_run(n: int, gates, precision: str, budget_s: float, threads: int):
@@ -181,7 +220,7 @@ def cpu_baseline_run(n: int, gates, precision: str, budget_s: float, threads: in
     (GB/s, passes, seconds)."""
     import ctypes as C
 
-    lib = _cpu_baseline_lib()
+    lib, _ = _cpu_baseline_lib()
     f32 = precision == "f32"
     sv = lib.cb_alloc(n, int(f32))
     if not sv:
@@ -209,13 +248,15 @@ def cpu_baseline_run(n: int, gates, precision: str, budget_s: float, threads: in
 
 def run_reference(args):
     """--impl reference: the reference's CPU path (threaded C++ restatement of
-    CAST's CPU SIMD kernels; CAST itself cannot be built here) on the host cores."""
+    CAST's CPU SIMD kernels; CAST itself cannot be built here) on the host cores,
+    on the same 30-qubit configuration as the GPU arm."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
     n_cpu = min(args.n, args.cpu_n)
     _, gates = build_fused(n_cpu, args.depth, args.k)
+    _, flags = _cpu_baseline_lib()
     samples = []
     for _ in range(args.warmup):
         cpu_baseline_run(n_cpu, gates, args.precision, args.cpu_budget / 4, threads)
@@ -236,7 +277,8 @@ def run_reference(args):
         "config": {"workload": f"brickwork-{args.n}q-d{args.depth}-{'c128' if args.precision == 'f64' else 'c64'}"
                    f"-k{args.k}", "cpu_sample_qubits": n_cpu},
         "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "port",
-                         "sample": sample},
+                         "sample": sample, "build": flags,
+                         "stddev": float(np.std(samples, ddof=1)) if len(samples) > 1 else 0.0},
         "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "vs_baseline": None,
     }
@@ -251,9 +293,12 @@ def _random_state(n: int, seed: int) -> np.ndarray:
     return v / np.linalg.norm(v)
 
 
-def _run_fused(n: int, gates, precision, split: bool = False, initial=None, reps: int = 3):
+def _run_fused(n: int, gates, precision, split: bool = False, initial=None, reps: int = 3,
+               warm: bool = True, use_graph: bool = True):
     """Device time (median of reps, CUDA events) of a fused gate list as one
-    gate program, and the final statevector object."""
+    gate program, and the final statevector object.  With `warm`, one untimed
+    run first (graph capture, first launches); every timed run starts from the
+    same initial state."""
     from cast_simulator_b200 import cuda as cu
     from cast_simulator_b200.simulator import Event, GateProgram, Stream
 
@@ -265,16 +310,17 @@ def _run_fused(n: int, gates, precision, split: bool = False, initial=None, reps
     st = Stream()
     e0, e1 = Event(), Event()
     ts = []
-    for _ in range(reps):
+    for rep in range(reps + (1 if warm else 0)):
         if initial is None:
             sv.zero(st)
         else:
             sv.upload(initial)
         e0.record(st)
-        prog.run(sv, st, use_graph=True)
+        prog.run(sv, st, use_graph=use_graph)
         e1.record(st)
         e1.sync()
-        ts.append(e1.elapsed_s(e0))
+        if rep or not warm:
+            ts.append(e1.elapsed_s(e0))
     return float(np.median(ts)), sv
 
 
@@ -306,56 +352,78 @@ def qft_leg(n: int = 22, seed: int = 7):
             "max_abs_diff_vs_unfused": float(np.max(np.abs(got - ref)))}
 
 
-def largest_leg(depth: int = 10, n64: int = 34, n128: int = 33, n_prefix: int = 28):
+def largest_leg(threads: int, depth: int = 10, n64: int = 34, n128: int = 33, n_prefix: int = 28):
     """Largest single-GPU fit: 34-qubit complex64 and 33-qubit complex128 (128 GiB
-    each), brickwork (depth 10) and QFT-CX; plain CUDA-core path at k = 4 vs the
-    split-BF16 tensor path at k = 5, 6 for complex64.  Fidelity on a 28-qubit
-    prefix of the same constructions against the complex128 plain path."""
+    each), random brickwork (depth 10) and QFT-CX; the plain CUDA-core path at
+    k = 4 against split-precision programs (dense 5- and 6-qubit gates on the
+    tensor cores) at k = 5, 6 for complex64.  Each run is one timed pass of the
+    whole circuit after the state is reset (seconds-long, eager launches).
+    Fidelity: the same constructions on a 28-qubit prefix, run once on the FP64
+    CPU restatement of CAST's statevector path in this process and on the GPU in
+    every variant."""
     from cast_simulator_b200 import cuda as cu
     from cast_simulator_b200.fusion import FusionConfig, optimize_native
     from cast_simulator_b200.types import QuantumCircuit
 
-    out = {"runs": []}
+    peak = measured_peak_hbm()[0]
+    out = {"runs": [], "no_k7_tensor_form": "a 7-qubit gate's split operand (256 KB) does not fit in "
+           "shared memory beside the tiles; k = 7 runs on the CUDA cores only"}
     for n, prec, label in ((n64, cu.CudaPrecision.F32, "c64"), (n128, cu.CudaPrecision.F64, "c128")):
         amp = 8 if label == "c64" else 16
         for name, circ in (("brickwork", QuantumCircuit.brickwork(n, depth, 2024)),
                            ("qft-cx", QuantumCircuit.qft_cx(n))):
             variants = [(4, False)] + ([(5, True), (6, True)] if label == "c64" else [])
+            base = None
             for k, split in variants:
                 fused = optimize_native(n, circ.gates(), FusionConfig.size_only(k)).gates()
-                t, sv = _run_fused(n, fused, prec, split, reps=2)
+                t, sv = _run_fused(n, fused, prec, split, reps=1, warm=False, use_graph=False)
                 del sv
-                out["runs"].append({"workload": f"{name}-{n}q-{label}", "fusion_k": k,
-                                    "tensor_cores": split, "fused_gates": len(fused),
-                                    "ms": t * 1e3,
-                                    "hbm_gbs": len(fused) * 2 * (1 << n) * amp / t / 1e9})
+                gbs = len(fused) * 2 * (1 << n) * amp / t / 1e9
+                base = base or t
+                wl = f"{name}-{n}q" + (f"-d{depth}" if name == "brickwork" else "") + f"-{label}"
+                out["runs"].append({"workload": wl, "fusion_k": k,
+                                    "tensor_cores": split, "fused_gates": len(fused), "ms": t * 1e3,
+                                    "hbm_gbs": gbs, "hbm_frac": gbs / peak,
+                                    "speedup_vs_plain_k4": base / t})
     fid = {}
+    t0 = time.perf_counter()
     for name, circ in (("brickwork", QuantumCircuit.brickwork(n_prefix, depth, 2024)),
                        ("qft-cx", QuantumCircuit.qft_cx(n_prefix))):
         g4 = optimize_native(n_prefix, circ.gates(), FusionConfig.size_only(4)).gates()
-        _, ref_sv = _run_fused(n_prefix, g4, cu.CudaPrecision.F64, reps=1)
-        ref = ref_sv.download()
-        del ref_sv
-        for k, split in ((4, False), (6, True)):
-            gk = optimize_native(n_prefix, circ.gates(), FusionConfig.size_only(k)).gates()
-            _, sv = _run_fused(n_prefix, gk, cu.CudaPrecision.F32, split, reps=1)
+        ref = cpu_reference_state(n_prefix, g4, threads)
+        for label, prec, k, split in (("c128-k4", cu.CudaPrecision.F64, 4, False),
+                                      ("c64-k4", cu.CudaPrecision.F32, 4, False),
+                                      ("c64-k5-tensor", cu.CudaPrecision.F32, 5, True),
+                                      ("c64-k6-tensor", cu.CudaPrecision.F32, 6, True)):
+            gk = g4 if k == 4 else optimize_native(n_prefix, circ.gates(), FusionConfig.size_only(k)).gates()
+            _, sv = _run_fused(n_prefix, gk, prec, split, reps=1, warm=False, use_graph=False)
             psi = sv.download()
             del sv
-            nrm = float(np.linalg.norm(psi))
-            fid[f"{name}-k{k}{'-tensor' if split else ''}"] = {
-                "one_minus_abs_overlap_renormalised": float(1 - abs(np.vdot(ref, psi / nrm))),
-                "max_abs_err": float(np.max(np.abs(ref - psi)))}
-    out["fidelity_28q_prefix_vs_c128"] = fid
+            fid[f"{name}-{label}"] = fidelity_vs(ref, psi)
+            del psi
+        del ref
+    out["fidelity_28q_prefix_vs_cpu_fp64"] = fid
+    out["fidelity_reference"] = (f"FP64 CPU restatement of CAST's statevector path, {threads} host "
+                                 f"threads, {time.perf_counter() - t0:.1f} s for both prefix circuits "
+                                 "with the GPU runs")
     return out
 
 
-def trajectory_leg(n: int = 16, depth: int = 30, n_traj: int = 4096, k: int = 3):
+def trajectory_leg(n: int = 16, depth: int = 30, n_traj: int = 4096, k: int = 3, n_plain: int = 48):
     """Noisy-trajectory configuration: brickwork depth 30 with depolarizing 1e-3
-    after every gate and amplitude damping 5e-4 per qubit per layer; 4096
-    trajectories in one persistent launch (CUDA graph) vs the plain per-gate
-    path with host-side noise decisions on a few trajectories."""
-    from cast_simulator_b200.simulator import Stream
-    from cast_simulator_b200.trajectory import TrajectoryProgram, run_plain
+    after every gate and amplitude damping 5e-4 per qubit per layer, 4096
+    trajectories in one persistent launch (CUDA graph).  Time to solution for
+    <Z_q> on the same GPU against
+      * the plain path one trajectory at a time (fused segments replayed as CUDA
+        graphs, host draws, one masked FP64 reduction per damping layer), timed
+        on n_plain trajectories;
+      * the exact density matrix on the plain kernels (2n = 32 virtual qubits,
+        complex64, 32 GiB), which has no statistical error.
+    The trajectory mean is also checked against that exact <Z_q>."""
+    from cast_simulator_b200 import cuda as cu
+    from cast_simulator_b200.fusion import FusionConfig, optimize_native
+    from cast_simulator_b200.simulator import GateProgram, Stream
+    from cast_simulator_b200.trajectory import TrajectoryProgram, run_plain_fused
     from cast_simulator_b200.types import QuantumCircuit
 
     circ = QuantumCircuit.brickwork(n, depth, 31337, depolarizing=1e-3, damping=5e-4)
@@ -363,84 +431,131 @@ def trajectory_leg(n: int = 16, depth: int = 30, n_traj: int = 4096, k: int = 3)
     st = Stream()
     prog.run(n_traj, 1, st)
     times = []
+    z = None
     for r in range(3):
         t0 = time.perf_counter()
         z, _ = prog.run(n_traj, 2 + r, st)
         times.append(time.perf_counter() - t0)
     t = float(np.median(times))
-    n_plain = 4
-    t0 = time.perf_counter()
-    run_plain(circ, n_plain, 5)
-    tp = (time.perf_counter() - t0) / n_plain
+    mean = z.mean(axis=0)
+    sig = z.std(axis=0, ddof=1)
+    se = sig / np.sqrt(n_traj)
+    rate = n_traj / t
     # every fused block is one pass over the trajectory's 2^n complex64 amplitudes
     # (read + write); the passes run out of L2, so this is an equivalent rate
     equiv = n_traj * prog.stats.n_blocks * 2 * (1 << n) * 8 / t / 1e9
-    return {"config": f"brickwork-{n}q-d{depth}, depolarizing 1e-3, damping 5e-4, c64, k={k}",
-            "n_traj": n_traj, "seconds": t, "traj_per_s": n_traj / t,
-            "pass_equivalent_gbs": equiv,
-            "plain_traj_per_s": 1.0 / tp, "speedup_vs_plain": (n_traj / t) * tp,
-            "blocks": prog.stats.n_blocks, "error_sites": prog.stats.n_errors,
-            "z_mean_first4": [float(x) for x in z.mean(axis=0)[:4]]}
+    out = {"config": f"brickwork-{n}q-d{depth}, depolarizing 1e-3, damping 5e-4, c64, k={k}",
+           "n_traj": n_traj, "seconds": t, "traj_per_s": rate, "pass_equivalent_gbs": equiv,
+           "blocks": prog.stats.n_blocks, "error_sites": prog.stats.n_errors,
+           "z_stderr_max": float(se.max()), "z_mean_first4": [float(x) for x in mean[:4]]}
+
+    # plain path, one trajectory at a time
+    run_plain_fused(circ, 2, 3, fusion_k=4, stream=st)  # warm: segment graphs, first launches
+    t0 = time.perf_counter()
+    zp = run_plain_fused(circ, n_plain, 5, fusion_k=4, stream=st)
+    tp = (time.perf_counter() - t0) / n_plain
+    out["plain_per_trajectory"] = {
+        "method": "plain gate kernels, one trajectory at a time: fused unitary segments (k=4) "
+                  "replayed as CUDA graphs, host Pauli draws, one FP64 masked reduction per "
+                  "damping layer",
+        "n_traj": n_plain, "traj_per_s": 1.0 / tp, "seconds_for_4096": 4096 * tp,
+        "persistent_speedup": rate * tp,
+        "z_mean_first4": [float(x) for x in zp.mean(axis=0)[:4]]}
+
+    # exact density matrix on the plain kernels
+    sup = [g.to_density_matrix_gate(n) for g in circ.gates()]
+    fused = optimize_native(2 * n, sup, FusionConfig.size_only(4))
+    gp = GateProgram(cu.CudaPrecision.F32, 2 * n, 1e-6, 1e-6)
+    from cast_simulator_b200 import _lib as L
+
+    eb = L.errbuf()
+    L.check(L.lib().cast_b200_program_add_fused(gp.handle, fused.handle, eb, L.ERR_LEN), eb,
+            "program_add_fused")
+    rho = cu.CudaStatevector(2 * n, cu.CudaPrecision.F32)
+    from cast_simulator_b200.simulator import Event
+
+    e0, e1 = Event(), Event()
+    rho.zero(st)
+    e0.record(st)
+    gp.run(rho, st, use_graph=False)
+    e1.record(st)
+    e1.sync()
+    t_dm = e1.elapsed_s(e0)
+    pops = np.zeros(1 << n)
+    L.check(L.lib().cast_b200_dm_populations(rho.dptr, n, 0, pops.ctypes.data_as(L.c_dp), st.handle,
+                                             eb, L.ERR_LEN), eb, "dm_populations")
+    del rho
+    idx = np.arange(1 << n)
+    z_dm = np.array([1 - 2 * pops[(idx >> q) & 1 == 1].sum() for q in range(n)]) / pops.sum()
+    dev = np.abs(mean - z_dm)
+    dm_passes = len(fused)
+    out["density_matrix_exact"] = {
+        "method": f"2n = {2 * n} virtual qubits, complex64 ({(8 << (2 * n)) / 2**30:.0f} GiB), "
+                  "superoperators fused at k=4 on the plain kernels",
+        "fused_passes": dm_passes, "seconds": t_dm,
+        "hbm_gbs": dm_passes * 2 * (8 << (2 * n)) / t_dm / 1e9,
+        "trajectory_mean_max_dev": float(dev.max()),
+        "trajectory_mean_max_dev_in_stderr": float((dev / se).max())}
+    # time to solution at a target standard error eps of every <Z_q>:
+    # trajectories need max_q sigma_q^2 / eps^2 runs; the density matrix is exact
+    eps = float(se.max())
+    out["time_to_solution"] = {
+        "target_stderr": eps,
+        "persistent_kernel_s": t, "plain_per_trajectory_s": 4096 * tp, "density_matrix_s": t_dm,
+        "stderr_where_persistent_equals_dm": float(sig.max() / np.sqrt(rate * t_dm))}
+    return out
 
 
-def serving_leg(n_req: int):
-    """Serving stream (bounded sample): Poisson arrivals of random brickwork
-    circuits, 10..24 qubits (noisy: 10..16 with 256 trajectories), depth 5..40,
-    half complex64 / half complex128, 20% noisy; p50/p99 latency and circuits/s
-    at two arrival rates, against a sequential FIFO of plain-path service times
-    (per-gate C-ABI launches; noisy requests scaled from 8 host-driven
-    trajectories).  One engine serves an unmeasured pass of each rate's stream
-    and then the measured ones, as a long-running server would: first-use costs
-    (kernel module loading on first launch, the first allocation of each
-    statevector size, which then stays pooled) do not land on the measured
-    requests."""
+def serving_leg(n_req: int, rates=(20.0, 80.0, 320.0)):
+    """Serving stream (bounded sample of the 10,000-request configuration, same
+    distributions): Poisson arrivals of random brickwork circuits, 10..28 qubits,
+    depth 5..40, half complex64 / half complex128, 20% noisy (depolarizing 1e-3,
+    256 trajectories; noisy circuits have at most 20 qubits, the trajectory
+    kernel's range).  At each swept rate: p50/p99 latency and circuits/s of the
+    continuous-batching engine, and of the same engine with one request at a time
+    (max_slots = 1: sequential execution, measured on the same arrivals).  An
+    unmeasured pass of the fastest stream warms each engine first (kernel module
+    loads, first allocation of each pooled statevector size)."""
     from cast_simulator_b200 import serving as S
 
-    rates = (40.0, 160.0)
-    out = {"requests": n_req, "rates": [],
-           "warmup": "one unmeasured pass of each rate's stream on the same engine"}
-    eng = S.ServingEngine(max_slots=8)
-    try:
-        for rate in rates:
-            eng.run_stream(S.make_stream(n_req, rate, 7, n_range=(10, 24)))
-        for rate in rates:
-            reqs = S.make_stream(n_req, rate, 7, n_range=(10, 24))
-            eng.max_concurrent = 0
-            t0 = time.perf_counter()
-            res = eng.run_stream(reqs)
-            wall = time.perf_counter() - t0
-            lat = [r.latency for r in res]
-            out["rates"].append({"rate_hz": rate, **S.latency_summary(lat),
-                                 "circuits_per_s": n_req / wall, "max_concurrent": eng.max_concurrent})
-    finally:
-        eng.shutdown()
-    # plain sequential baseline on the same requests (service times measured alone)
-    reqs = S.make_stream(n_req, 40.0, 7, n_range=(10, 24))
-    svc = []
-    for r in reqs:
-        if r.n_traj:
-            sub = S.Request(r.circuit, r.precision, 8, r.seed, r.arrival, r.rid)
-            svc.append(S.plain_service_time(sub) * r.n_traj / 8)
-        else:
-            svc.append(S.plain_service_time(r))
-    for entry in out["rates"]:
-        arr = [r.arrival * 40.0 / entry["rate_hz"] for r in reqs]
-        seq = S.sequential_latencies(arr, svc)
-        entry["plain_sequential"] = {**S.latency_summary(seq),
-                                     "circuits_per_s": n_req / max(arr[-1], float(np.sum(svc)))}
-    out["plain_service_s_total"] = float(np.sum(svc))
+    def stream(rate):
+        return S.make_stream(n_req, rate, 7, n_range=(10, 28), noisy_max_qubits=20)
+
+    out = {"requests_per_rate": n_req, "n_range": [10, 28], "noisy_max_qubits": 20,
+           "sample": f"{n_req} requests per rate of the 10,000-request stream's distributions",
+           "rates": []}
+    for label, slots in (("engine", 8), ("sequential", 1)):
+        eng = S.ServingEngine(max_slots=slots)
+        try:
+            eng.run_stream(stream(max(rates)))
+            for i, rate in enumerate(rates):
+                eng.max_concurrent = 0
+                t0 = time.perf_counter()
+                res = eng.run_stream(stream(rate))
+                wall = time.perf_counter() - t0
+                entry = {**S.latency_summary([r.latency for r in res]),
+                         "circuits_per_s": n_req / wall, "max_concurrent": eng.max_concurrent,
+                         "wall_s": wall}
+                if label == "engine":
+                    out["rates"].append({"rate_hz": rate, **entry})
+                else:
+                    out["rates"][i]["sequential"] = entry
+                    out["rates"][i]["p99_speedup_vs_sequential"] = entry["p99_ms"] / out["rates"][i]["p99_ms"]
+        finally:
+            eng.shutdown()
     return out
 
 
 def fusion_sweep_leg(n: int, depth: int):
     """The brickwork with fusion width k = 2..7 on the CUDA-core path in complex128
     and complex64, and on the split-BF16 tensor cores for k = 5, 6 (complex64):
-    device time per circuit (median of 2 after a warm-up), fused passes, and the
-    HBM rate those passes imply."""
+    device time per circuit (median of 2 after a warm-up run), fused passes, and
+    the HBM rate those passes imply."""
     from cast_simulator_b200 import cuda as cu
     from cast_simulator_b200.fusion import FusionConfig, optimize_native
     from cast_simulator_b200.types import QuantumCircuit
 
+    peak = measured_peak_hbm()[0]
     circ = QuantumCircuit.brickwork(n, depth, 2024)
     out = {"workload": f"brickwork-{n}q-d{depth}", "runs": []}
     cases = [(cu.CudaPrecision.F64, "c128", False, k) for k in range(2, 8)]
@@ -449,82 +564,18 @@ def fusion_sweep_leg(n: int, depth: int):
     fused = {k: optimize_native(n, circ.gates(), FusionConfig.size_only(k)).gates() for k in range(2, 8)}
     for prec, label, split, k in cases:
         gates = fused[k]
-        t, sv = _run_fused(n, gates, prec, split, reps=3)
+        t, sv = _run_fused(n, gates, prec, split, reps=2)
         b_amp = 16 if label == "c128" else 8
+        gbs = len(gates) * 2 * (1 << n) * b_amp / t / 1e9
         out["runs"].append({"precision": label, "tensor_cores": split, "fusion_k": k,
                             "fused_gates": len(gates), "ms_per_circuit": t * 1e3,
-                            "hbm_gbs": len(gates) * 2 * (1 << n) * b_amp / t / 1e9})
+                            "hbm_gbs": gbs, "hbm_frac": gbs / peak})
         del sv
     for label in ("c128", "c64"):
         best = min((r for r in out["runs"] if r["precision"] == label),
                    key=lambda r: r["ms_per_circuit"])
         out[f"best_{label}"] = {"fusion_k": best["fusion_k"], "tensor_cores": best["tensor_cores"],
                                 "ms_per_circuit": best["ms_per_circuit"]}
-    return out
-
-
-def tensor_leg(n: int, depth: int):
-    """Tensor-core fused path (complex64, split BF16, k = 5 and 6) vs the plain
-    CUDA-core path at its best width (k = 4): time per circuit on the full
-    30-qubit brickwork, and 1-|<psi_64|psi>| against the complex128 plain path on
-    a 24-qubit brickwork of the same construction."""
-    from cast_simulator_b200 import cuda as cu
-    from cast_simulator_b200.fusion import CircuitGraph, FusionConfig, optimize_native
-    from cast_simulator_b200.simulator import Event, GateProgram, Simulator, Stream
-    from cast_simulator_b200.types import QuantumCircuit
-
-    out = {"workload": f"brickwork-{n}q-d{depth}-c64", "runs": []}
-    circ = QuantumCircuit.brickwork(n, depth, 2024)
-    st = Stream()
-    for k, split in ((4, False), (5, True), (6, True)):
-        gates = optimize_native(n, circ.gates(), FusionConfig.size_only(k)).gates()
-        prog = GateProgram(cu.CudaPrecision.F32, n, 1e-6, 1e-6, split)
-        for g in gates:
-            prog.add(g.matrix(), g.qubits())
-        sv = cu.CudaStatevector(n, cu.CudaPrecision.F32)
-        e0, e1 = Event(), Event()
-        ts = []
-        for rep in range(4):
-            sv.zero(st)
-            e0.record(st)
-            prog.run(sv, st, use_graph=True)
-            e1.record(st)
-            e1.sync()
-            if rep:
-                ts.append(e1.elapsed_s(e0))
-        t = float(np.median(ts))
-        run = {"fusion_k": k, "tensor_cores": split, "fused_gates": len(gates),
-               "ms_per_circuit": t * 1e3, "hbm_gbs": len(gates) * 2 * (1 << n) * 8 / t / 1e9,
-               "hbm_frac": len(gates) * 2 * (1 << n) * 8 / t / 1e9 / measured_peak_hbm()[0]}
-        if split:
-            # tensor-pipe work of the passes that ran there: 3 split products of the
-            # real (2D x 2D) GEMM per group, D = 2^kg
-            flops = sum(3 * 2 * (2 << g.n_qubits()) ** 2 * (1 << (n - g.n_qubits()))
-                        for g in gates if g.n_qubits() in (5, 6))
-            peak = measured_peak_bf16()
-            run["tensor_tflops"] = flops / t / 1e12
-            run["tensor_frac"] = flops / t / 1e12 / peak if peak else None
-        out["runs"].append(run)
-        del sv, prog
-    base = out["runs"][0]["ms_per_circuit"]
-    for r in out["runs"]:
-        r["speedup_vs_plain_k4"] = base / r["ms_per_circuit"]
-    # fidelity on a 24-qubit instance against complex128
-    nf = 24
-    small = QuantumCircuit.brickwork(nf, depth, 2024)
-    ref = Simulator(cu.CudaKernelGenSpec.f64()).simulate(
-        CircuitGraph.from_gates(nf, optimize_native(nf, small.gates(), FusionConfig.size_only(4)).gates())
-    ).download_amplitudes()
-    fid = {}
-    for k in (5, 6):
-        g = CircuitGraph.from_gates(nf, optimize_native(nf, small.gates(), FusionConfig.size_only(k)).gates())
-        psi = Simulator(cu.CudaKernelGenSpec.f32(), split_precision=True).simulate(g).download_amplitudes()
-        nrm = float(np.linalg.norm(psi))
-        ov = np.vdot(ref, psi / nrm)
-        fid[f"k{k}"] = {"one_minus_abs_overlap_renormalised": float(1 - abs(ov)),
-                        "norm_drift": 1.0 - nrm,
-                        "max_abs_err": float(np.max(np.abs(ref - psi / nrm)))}
-    out["fidelity_24q_vs_c128"] = fid
     return out
 
 
@@ -541,6 +592,76 @@ def traffic_from_profile(n: int, precision: str, k: int):
         return None
 
 
+def plain_line(n: int, depth: int, k: int, precision: str, steps: int, warmup: int, local: int,
+               pg=None) -> dict:
+    """The fused brickwork through the drop-in C ABI (compile_gate_ptx ->
+    cubin_load -> kernel_launch per fused gate, the reference's execution path)
+    on a device-resident statevector: `warmup` untimed steps, then `steps` timed
+    steps bracketed by a barrier and CUDA events on the launching stream, with
+    the SM clocks sampled meanwhile.  One step = reset to |0...0> + every fused
+    gate once.  Returns the device time (max over ranks), per-kernel event times
+    by gate size, and the fused circuit."""
+    from cast_simulator_b200 import cuda as cu
+    from cast_simulator_b200.simulator import Event
+
+    prec = cu.CudaPrecision.F64 if precision == "f64" else cu.CudaPrecision.F32
+    spec = cu.CudaKernelGenSpec.f64() if prec == cu.CudaPrecision.F64 else cu.CudaKernelGenSpec.f32()
+    circ, gates = build_fused(n, depth, k)
+    mgr = cu.CudaKernelManager(spec, timing=True)
+    kids = [mgr.generate(g) for g in gates]
+    sv = cu.CudaStatevector(n, prec)
+
+    def step():
+        sv.zero()
+        for kid in kids:
+            mgr.apply(kid, sv)
+        return mgr.sync()
+
+    for _ in range(warmup):
+        step()
+    stream = mgr.stream  # the launching stream: events bracket the kernels themselves
+    if pg:
+        pg.barrier()
+    e_start, e_end = Event(), Event()
+    per_kernel = {}
+    with ClockSampler(local) as clk:
+        e_start.record(stream)
+        wall0 = time.perf_counter()
+        for _ in range(steps):
+            st = step()
+            for kt in st.kernels:
+                per_kernel.setdefault(kt.n_gate_qubits, []).append(kt.gpu_time)
+        e_end.record(stream)
+        e_end.sync()
+        wall = time.perf_counter() - wall0
+    t = max(e_end.elapsed_s(e_start), 1e-12)
+    if pg:
+        import torch
+
+        tt = torch.tensor([t], device=f"cuda:{local}", dtype=torch.float64)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t = float(tt.item())
+    del sv
+    return {"t": t, "per_kernel": per_kernel, "circ": circ, "gates": gates, "clocks": clk.summary(),
+            "wall": wall, "n_launch": steps * len(gates)}
+
+
+def roofline_of(run: dict, n: int, precision: str) -> dict:
+    """The dominant kernel (the gate size with the largest summed device time):
+    algorithmic bytes per launch / its average CUDA-event duration, against the
+    measured HBM copy peak."""
+    amp_bytes = 16 if precision == "f64" else 8
+    per_kernel = run["per_kernel"]
+    dom_k = max(per_kernel, key=lambda kk: sum(per_kernel[kk]))
+    dom_avg = float(np.mean(per_kernel[dom_k]))
+    achieved = 2 * (1 << n) * amp_bytes / dom_avg / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic_from_profile(n, precision, dom_k), "kernel": f"k_gate k={dom_k}",
+            "kernel_time_share": sum(per_kernel[dom_k]) / sum(sum(v) for v in per_kernel.values()),
+            "peak_kind": peak_kind}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -551,15 +672,15 @@ def main(argv=None):
     ap.add_argument("--k", type=int, default=4)
     ap.add_argument("--n", type=int, default=30)
     ap.add_argument("--depth", type=int, default=20)
-    ap.add_argument("--cpu-n", type=int, default=28)
+    ap.add_argument("--cpu-n", type=int, default=30)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip trajectory and serving legs")
-    ap.add_argument("--sweep", action="store_true",
-                    help="add the fusion-width sweep k = 2..7 (complex128, complex64, tensor cores)")
-    ap.add_argument("--serve-requests", type=int, default=60)
-    ap.add_argument("--largest", action="store_true",
-                    help="add the 34q complex64 / 33q complex128 largest-fit leg (minutes)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip every leg beside the headline (and the CPU baseline)")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the fusion-width sweep k = 2..7")
+    ap.add_argument("--no-largest", action="store_true",
+                    help="skip the 34q complex64 / 33q complex128 largest-fit leg")
+    ap.add_argument("--serve-requests", type=int, default=200)
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
@@ -576,7 +697,7 @@ def main(argv=None):
 
     from cast_simulator_b200 import _lib as L
     from cast_simulator_b200 import cuda as cu
-    from cast_simulator_b200.simulator import Event, Simulator
+    from cast_simulator_b200.simulator import Simulator
 
     eb = L.errbuf()
     L.check(L.lib().cast_b200_set_device(local, eb, L.ERR_LEN), eb, "set_device")
@@ -584,56 +705,12 @@ def main(argv=None):
     spec = cu.CudaKernelGenSpec.f64() if prec == cu.CudaPrecision.F64 else cu.CudaKernelGenSpec.f32()
     amp_bytes = 16 if prec == cu.CudaPrecision.F64 else 8
     n = args.n
-    circ, gates = build_fused(n, args.depth, args.k)
     bytes_per_pass = 2 * (1 << n) * amp_bytes
 
     # ---- value: drop-in C ABI path, device-resident statevector ----
-    mgr = cu.CudaKernelManager(spec, timing=True)
-    kids = [mgr.generate(g) for g in gates]
-    sv = cu.CudaStatevector(n, prec)
-
-    def step():
-        sv.zero()
-        for kid in kids:
-            mgr.apply(kid, sv)
-        return mgr.sync()
-
-    for _ in range(args.warmup):
-        step()
-    stream = mgr.stream  # the launching stream: events bracket the kernels themselves
-    if pg:
-        pg.barrier()
-    e_start, e_end = Event(), Event()
-    per_kernel = {}
-    with ClockSampler(local) as clk:
-        e_start.record(stream)
-        wall0 = time.perf_counter()
-        for _ in range(args.steps):
-            st = step()
-            for kt in st.kernels:
-                per_kernel.setdefault(kt.n_gate_qubits, []).append(kt.gpu_time)
-        e_end.record(stream)
-        e_end.sync()
-        wall = time.perf_counter() - wall0
-    t_dev = e_end.elapsed_s(e_start)
-    t = max(t_dev, 1e-12)
-    if pg:
-        import torch
-
-        tt = torch.tensor([t], device=f"cuda:{local}", dtype=torch.float64)
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        t = float(tt.item())
-    total_bytes = ws * args.steps * len(gates) * bytes_per_pass
-    value = total_bytes / t / 1e9
-    n_launch = args.steps * len(gates)
-
-    # dominant kernel = the gate size with the largest summed device time
-    dom_k = max(per_kernel, key=lambda kk: sum(per_kernel[kk]))
-    dom_avg = float(np.mean(per_kernel[dom_k]))
-    achieved = bytes_per_pass / dom_avg / 1e9
-    peak, peak_kind = measured_peak_hbm()
-    traffic = traffic_from_profile(n, args.precision, dom_k)
-    kernel_share = sum(per_kernel[dom_k]) / sum(sum(v) for v in per_kernel.values())
+    run = plain_line(n, args.depth, args.k, args.precision, args.steps, args.warmup, local, pg)
+    t, gates, circ = run["t"], run["gates"], run["circ"]
+    value = ws * args.steps * len(gates) * bytes_per_pass / t / 1e9
 
     # ---- e2e: public Simulator API, gates from host, <Z> read back ----
     from cast_simulator_b200.fusion import CircuitGraph
@@ -642,9 +719,7 @@ def main(argv=None):
     fused_graph = CircuitGraph.from_gates(n, gates)
     h2d = sum(16 * g.matrix().size for g in gates)
     d2h = 8 * (n + 1)
-    del sv  # free the device-resident state before the e2e state is allocated
-    for _ in range(1):
-        sim.simulate(fused_graph).expectation_z()
+    sim.simulate(fused_graph).expectation_z()
     e0 = time.perf_counter()
     zs = None
     for _ in range(args.steps):
@@ -652,6 +727,7 @@ def main(argv=None):
         zs = state.expectation_z()
         del state
     e2e_t = time.perf_counter() - e0
+    sim.release_memory()
     if pg:
         import torch
 
@@ -682,16 +758,12 @@ def main(argv=None):
             "parallelism": f"replicas{ws}",
         },
         "gates_amps_per_s": ws * args.steps * len(gates) * (1 << n) / t,
-        "roofline": {
-            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic, "kernel": f"k_gate k={dom_k}",
-            "kernel_time_share": kernel_share, "peak_kind": peak_kind,
-        },
+        "roofline": roofline_of(run, n, args.precision),
         "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "gpu_launches": n_launch,
-        "clocks": clk.summary(),
-        "wall_s_timed": wall,
+        "gpu_launches": run["n_launch"],
+        "clocks": run["clocks"],
+        "wall_s_timed": run["wall"],
         "z_expectation_sample": [float(x) for x in zs[:4]] if zs is not None else None,
     }
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -701,19 +773,29 @@ def main(argv=None):
         gbs, passes, el = cpu_baseline_run(n_cpu, cgates, args.precision, args.cpu_budget, threads)
         line["cpu_baseline"] = {
             "value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
+            "build": _cpu_baseline_lib()[1],
             "sample": f"{passes} fused-gate passes of the {n_cpu}-qubit brickwork (k={args.k}) in {el:.1f} s",
             "parity": cpu_parity(min(n, 22), args.depth, args.k, args.precision, threads)}
     # the extra legs run on one GPU only: under torchrun the other ranks would sit
     # in the closing barrier for the minutes they take
     if rank == 0 and ws == 1 and not args.no_extras:
+        threads = os.cpu_count() or 1
+        other = "f32" if args.precision == "f64" else "f64"
+        orun = plain_line(n, args.depth, args.k, other, min(args.steps, 10), 3, local)
+        ob = 2 * (1 << n) * (16 if other == "f64" else 8)
+        line["c2_" + ("complex64" if other == "f32" else "complex128")] = {
+            "workload": f"brickwork-{n}q-d{args.depth}-{'c64' if other == 'f32' else 'c128'}-k{args.k}",
+            "value": min(args.steps, 10) * len(orun["gates"]) * ob / orun["t"] / 1e9, "unit": "GB/s",
+            "ms_per_step": orun["t"] / min(args.steps, 10) * 1e3, "dtype": other,
+            "roofline": roofline_of(orun, n, other), "clocks": orun["clocks"]}
         line["qft"] = qft_leg()
-        line["tensor_path"] = tensor_leg(n, args.depth)
+        if not args.no_sweep:
+            line["fusion_sweep"] = fusion_sweep_leg(n, args.depth)
+            line["tensor_path"] = tensor_leg(n, args.depth, line["fusion_sweep"])
         line["trajectories"] = trajectory_leg()
         line["serving"] = serving_leg(args.serve_requests)
-    if rank == 0 and ws == 1 and args.sweep:
-        line["fusion_sweep"] = fusion_sweep_leg(n, args.depth)
-    if rank == 0 and ws == 1 and args.largest:
-        line["largest_fit"] = largest_leg()
+        if not args.no_largest:
+            line["largest_fit"] = largest_leg(threads)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg:

@@ -131,6 +131,12 @@ CAST_B200 = [
       C.c_size_t]),
     ("cast_b200_dm_populations", C.c_int,
      [C.c_uint64, C.c_uint32, C.c_uint8, c_dp, C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("cast_b200_damping_sums", C.c_int,
+     [C.c_uint64, C.c_uint32, C.c_uint8, C.c_uint64, C.c_double, c_dp, c_dp, C.c_void_p, C.c_char_p,
+      C.c_size_t]),
+    ("cast_b200_scale_popc", C.c_int,
+     [C.c_uint64, C.c_uint32, C.c_uint8, C.c_uint64, C.c_double, C.c_double, C.c_void_p, C.c_char_p,
+      C.c_size_t]),
     ("cast_b200_fuse", C.c_void_p,
      [C.c_uint32, C.c_uint32, c_u32p, c_u32p, C.POINTER(Complex64), C.POINTER(FusionConfigC),
       C.c_char_p, C.c_size_t]),

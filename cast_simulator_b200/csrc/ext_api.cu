@@ -403,6 +403,40 @@ int cast_b200_marginal_probabilities(uint64_t sv_dptr, uint32_t n_qubits, uint8_
   return 0;
 }
 
+int cast_b200_damping_sums(uint64_t sv_dptr, uint32_t n_qubits, uint8_t precision, uint64_t mask,
+                           double gamma, double *out_total, double *out_weighted, void *stream,
+                           char *err_buf, size_t err_buf_len) {
+  std::string err;
+  if (!sv_dptr || !out_total || !out_weighted) {
+    write_err(err_buf, err_buf_len, "arguments must not be null");
+    return 1;
+  }
+  if (!cb2::damping_sums(reinterpret_cast<const void *>(sv_dptr), n_qubits, precision, mask, gamma,
+                         out_total, out_weighted, static_cast<cudaStream_t>(stream), err)) {
+    write_err(err_buf, err_buf_len, err);
+    return 1;
+  }
+  clear_err(err_buf, err_buf_len);
+  return 0;
+}
+
+int cast_b200_scale_popc(uint64_t sv_dptr, uint32_t n_qubits, uint8_t precision, uint64_t mask,
+                         double factor, double scale, void *stream, char *err_buf,
+                         size_t err_buf_len) {
+  std::string err;
+  if (!sv_dptr) {
+    write_err(err_buf, err_buf_len, "statevector must not be null");
+    return 1;
+  }
+  if (!cb2::scale_popc(reinterpret_cast<void *>(sv_dptr), n_qubits, precision, mask, factor, scale,
+                       static_cast<cudaStream_t>(stream), err)) {
+    write_err(err_buf, err_buf_len, err);
+    return 1;
+  }
+  clear_err(err_buf, err_buf_len);
+  return 0;
+}
+
 int cast_b200_dm_populations(uint64_t rho_dptr, uint32_t n_physical, uint8_t precision,
                              double *out, void *stream, char *err_buf, size_t err_buf_len) {
   std::string err;

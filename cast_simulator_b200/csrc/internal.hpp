@@ -111,5 +111,13 @@ bool marginal_probabilities(const void *x, uint32_t n, uint8_t precision, const 
                             uint32_t m, double *out, cudaStream_t s, std::string &err);
 bool dm_populations(const void *rho, uint32_t n, uint8_t precision, double *out, cudaStream_t s,
                     std::string &err);
+// Amplitude damping on a qubit mask, for host-driven quantum-jump trajectories:
+// tot = sum |a_i|^2, wsum = sum |a_i|^2 (1 - gamma)^popc(i & mask) (FP64,
+// synchronous); scale_popc multiplies a_i by scale * sfac^popc(i & mask)
+// (enqueued on `s`).
+bool damping_sums(const void *x, uint32_t n, uint8_t precision, uint64_t mask, double gamma,
+                  double *tot, double *wsum, cudaStream_t s, std::string &err);
+bool scale_popc(void *x, uint32_t n, uint8_t precision, uint64_t mask, double sfac, double scale,
+                cudaStream_t s, std::string &err);
 
 }  // namespace cb2

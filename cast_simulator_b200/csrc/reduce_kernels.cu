@@ -263,6 +263,58 @@ __global__ void __launch_bounds__(kRedThreads) k_marginal(const T *__restrict__ 
     partial[(size_t)blockIdx.x * nb + i] = bins[i];
 }
 
+// A table of powers indexed by a popcount (0 .. kMaxPopQubits), passed to the
+// kernels by value (328 bytes of kernel parameters).
+struct PopcTable {
+  double v[kMaxPopQubits + 1];
+};
+
+// Amplitude-damping sums on a qubit mask: per block (T, D) with
+// T = sum |a_i|^2 and D = sum |a_i|^2 * w^popc(i & mask), w = 1 - gamma
+// (the probability weight of "no jump on any masked qubit"); tab.v[c] = w^c.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_damp_sums(const T *__restrict__ x, uint32_t n,
+                                                          uint64_t mask, const PopcTable tab,
+                                                          double *__restrict__ partial) {
+  using V = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+  const V *xv = reinterpret_cast<const V *>(x);
+  const uint64_t n_amps = 1ull << n;
+  const uint64_t stride = (uint64_t)gridDim.x * kRedThreads;
+  double t = 0, d = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * kRedThreads + threadIdx.x; i < n_amps; i += stride) {
+    const V v = xv[i];
+    const double p = (double)v.x * v.x + (double)v.y * v.y;
+    t += p;
+    d += p * tab.v[__popcll(i & mask)];
+  }
+  t = block_sum(t);
+  __syncthreads();
+  d = block_sum(d);
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = t;
+    partial[2 * blockIdx.x + 1] = d;
+  }
+}
+
+// x_i *= scale * s^popc(i & mask): the no-jump branch of amplitude damping on
+// the masked qubits (s = sqrt(1 - gamma)) with its renormalisation folded in.
+// tab.v[c] = scale * s^c, computed in FP64 on the host.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_scale_popc(T *__restrict__ x, uint32_t n, uint64_t mask,
+                                                           const PopcTable tab) {
+  using V = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+  V *xv = reinterpret_cast<V *>(x);
+  const uint64_t n_amps = 1ull << n;
+  const uint64_t stride = (uint64_t)gridDim.x * kRedThreads;
+  for (uint64_t i = (uint64_t)blockIdx.x * kRedThreads + threadIdx.x; i < n_amps; i += stride) {
+    V v = xv[i];
+    const T f = (T)tab.v[__popcll(i & mask)];
+    v.x *= f;
+    v.y *= f;
+    xv[i] = v;
+  }
+}
+
 template <typename T>
 __global__ void k_dm_diag(const T *__restrict__ rho, uint32_t n, double *__restrict__ out) {
   const uint64_t dim = 1ull << n;
@@ -338,6 +390,44 @@ bool marg_impl(const void *x, uint32_t n, const uint32_t *measured, uint32_t m, 
          cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize (marginal)", err);
 }
 
+PopcTable powers(double base, double first) {
+  PopcTable t;
+  double f = first;
+  for (int c = 0; c <= kMaxPopQubits; ++c) {
+    t.v[c] = f;
+    f *= base;
+  }
+  return t;
+}
+
+template <typename T>
+bool damp_sums_impl(const void *x, uint32_t n, uint64_t mask, double gamma, double *tot, double *wsum,
+                    cudaStream_t s, std::string &err) {
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  const unsigned grid = red_grid(1ull << n);
+  if (!ensure_scratch(2 * (int)grid + 2, err)) return false;
+  double res[2];
+  k_damp_sums<T><<<grid, kRedThreads, 0, s>>>(static_cast<const T *>(x), n, mask,
+                                               powers(1.0 - gamma, 1.0), g_scratch);
+  k_sum_columns<<<2, kRedThreads, 0, s>>>(g_scratch, (int)grid, 2, g_scratch + 2 * grid);
+  if (!cuda_ok(cudaGetLastError(), "damping sums launch", err) ||
+      !cuda_ok(cudaMemcpyAsync(res, g_scratch + 2 * grid, 16, cudaMemcpyDeviceToHost, s),
+               "cudaMemcpyAsync (damping sums)", err) ||
+      !cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize (damping sums)", err))
+    return false;
+  *tot = res[0];
+  *wsum = res[1];
+  return true;
+}
+
+template <typename T>
+bool scale_popc_impl(void *x, uint32_t n, uint64_t mask, double sfac, double scale, cudaStream_t s,
+                     std::string &err) {
+  k_scale_popc<T><<<red_grid(1ull << n), kRedThreads, 0, s>>>(static_cast<T *>(x), n, mask,
+                                                               powers(sfac, scale));
+  return cuda_ok(cudaGetLastError(), "popcount scale launch", err);
+}
+
 template <typename T>
 bool dm_impl(const void *rho, uint32_t n, double *out, cudaStream_t s, std::string &err) {
   double *d = nullptr;
@@ -354,6 +444,28 @@ bool dm_impl(const void *rho, uint32_t n, double *out, cudaStream_t s, std::stri
 }
 
 }  // namespace
+
+bool damping_sums(const void *x, uint32_t n, uint8_t precision, uint64_t mask, double gamma,
+                  double *tot, double *wsum, cudaStream_t s, std::string &err) {
+  if (!aligned16(reinterpret_cast<uint64_t>(x), "statevector pointer", err)) return false;
+  if (n == 0 || n > kMaxSvQubits || precision > 1 || !(gamma >= 0.0 && gamma <= 1.0)) {
+    err = "damping sums: invalid statevector size, precision or gamma";
+    return false;
+  }
+  return precision == 0 ? damp_sums_impl<float>(x, n, mask, gamma, tot, wsum, s, err)
+                        : damp_sums_impl<double>(x, n, mask, gamma, tot, wsum, s, err);
+}
+
+bool scale_popc(void *x, uint32_t n, uint8_t precision, uint64_t mask, double sfac, double scale,
+                cudaStream_t s, std::string &err) {
+  if (!aligned16(reinterpret_cast<uint64_t>(x), "statevector pointer", err)) return false;
+  if (n == 0 || n > kMaxSvQubits || precision > 1) {
+    err = "popcount scale: invalid statevector size or precision";
+    return false;
+  }
+  return precision == 0 ? scale_popc_impl<float>(x, n, mask, sfac, scale, s, err)
+                        : scale_popc_impl<double>(x, n, mask, sfac, scale, s, err);
+}
 
 bool norm_squared(const void *x, uint64_t n_scalars, uint8_t precision, double *out,
                   cudaStream_t s, std::string &err) {

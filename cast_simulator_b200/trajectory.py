@@ -410,6 +410,166 @@ def run_plain(circuit: QuantumCircuit, n_traj: int, seed: int, precision=None) -
     return out
 
 
+def run_plain_fused(circuit: QuantumCircuit, n_traj: int, seed: int, precision=None,
+                    fusion_k: int = 4, stream=None) -> np.ndarray:
+    """Quantum-jump trajectories one at a time on the plain gate kernels, with
+    host-side draws: the fair plain-path counterpart of the persistent kernel.
+
+    Each run of unitary gates between two damping layers is fused at width
+    ``fusion_k`` once and replayed per trajectory as a CUDA graph (GateProgram).
+    Pauli errors (depolarizing) are state-independent, so the host draws them
+    per trajectory up front; a segment where one fires runs its gates one by
+    one with the Pauli inserted.  A layer of amplitude damping on a qubit mask
+    takes one FP64 device reduction (T, D) and one host draw: no jump with
+    probability D/T, applied as one renormalised diagonal pass; otherwise the
+    jump pattern is sampled qubit by qubit, conditioned on at least one jump
+    (populations and masked sums re-read after each step).  Other one-qubit
+    channels sample their Kraus branch from the qubit's FP64 populations.
+    Returns <Z_q> per trajectory (n_traj x n)."""
+    from .cuda import CudaPrecision, CudaStatevector
+    from .fusion import optimize_native
+    from .simulator import GateProgram, Stream, qubit_populations
+    from .types import SplitMix64
+
+    prec = CudaPrecision.F32 if precision is None else precision
+    lib = L.lib()
+    n = circuit.n_qubits()
+    tol = 1e-6 if prec == CudaPrecision.F32 else 1e-12
+    st = stream if stream is not None else Stream()
+    h = st.handle
+
+    # items: ("seg", gates, sites, program) | ("damp", mask, gamma) | ("chan", gate)
+    items: list = []
+    seg: list = []
+    sites: list = []  # (position after which it acts, qubit, p, [X, Y, Z])
+
+    def close_seg():
+        nonlocal seg, sites
+        if seg or sites:
+            prog = None
+            if seg:
+                fused = optimize_native(n, seg, FusionConfig.size_only(fusion_k))
+                prog = GateProgram(prec, n, tol, tol)
+                eb = L.errbuf()
+                L.check(lib.cast_b200_program_add_fused(prog.handle, fused.handle, eb, L.ERR_LEN), eb,
+                        "program_add_fused")
+            items.append(("seg", seg, sites, prog))
+        seg, sites = [], []
+
+    for g in circuit.gates():
+        if g.is_unitary():
+            seg.append(g)
+            continue
+        pc = _is_pauli_channel(g)
+        if pc is not None:
+            sites.append((len(seg), g.qubits()[0], pc[0], pc[1]))
+            continue
+        close_seg()
+        gam = _damping_rate(g)
+        if gam is not None:
+            q = g.qubits()[0]
+            last = items[-1] if items else None
+            if last is not None and last[0] == "damp" and last[2] == gam and not (last[1] >> q) & 1:
+                items[-1] = ("damp", last[1] | (1 << q), gam)
+            else:
+                items.append(("damp", 1 << q, gam))
+        else:
+            items.append(("chan", g))
+    close_seg()
+
+    def apply(sv, m, q):
+        mm = np.ascontiguousarray(m, dtype=np.complex128)
+        qq = np.ascontiguousarray(q, dtype=np.uint32)
+        eb = L.errbuf()
+        L.check(lib.cast_b200_apply_gate(sv.dptr, n, int(prec), mm.view(np.float64).ctypes.data_as(
+            C.POINTER(L.Complex64)), qq.ctypes.data_as(L.c_u32p), qq.size, tol, tol, h, eb,
+            L.ERR_LEN), eb, "apply_gate")
+
+    def sums(sv, mask, gam):
+        t, d = C.c_double(), C.c_double()
+        eb = L.errbuf()
+        L.check(lib.cast_b200_damping_sums(sv.dptr, n, int(prec), mask, gam, C.byref(t), C.byref(d), h,
+                                           eb, L.ERR_LEN), eb, "damping_sums")
+        return t.value, d.value
+
+    def scale_popc(sv, mask, factor, scale):
+        eb = L.errbuf()
+        L.check(lib.cast_b200_scale_popc(sv.dptr, n, int(prec), mask, factor, scale, h, eb, L.ERR_LEN),
+                eb, "scale_popc")
+
+    k1_of = lambda gam: np.array([[0, math.sqrt(gam)], [0, 0]], dtype=np.complex128)  # noqa: E731
+    rng = SplitMix64(seed)
+    out = np.zeros((n_traj, n))
+    sv = CudaStatevector(n, prec)
+    for t in range(n_traj):
+        sv.zero(st)
+        for it in items:
+            if it[0] == "seg":
+                _, gates, ssites, prog = it
+                fired = []
+                for pos, q, p, mats in ssites:
+                    u = rng.uniform()
+                    if u < p:
+                        fired.append((pos, q, mats[min(2, int(u / p * 3))]))
+                if not fired:
+                    if prog is not None:
+                        prog.run(sv, st, True)
+                    continue
+                for pos in range(len(gates) + 1):
+                    for fp, q, m in fired:
+                        if fp == pos:
+                            apply(sv, m, (q,))
+                    if pos < len(gates):
+                        apply(sv, gates[pos].matrix(), gates[pos].qubits())
+            elif it[0] == "damp":
+                _, mask, gam = it
+                tot, w = sums(sv, mask, gam)
+                if rng.uniform() * tot < w:  # no jump on any masked qubit
+                    scale_popc(sv, mask, math.sqrt(1.0 - gam), 1.0 / math.sqrt(w))
+                    continue
+                # at least one jump: qubit by qubit, conditioned while none has jumped yet
+                rest, jumped = mask, False
+                for q in range(n):
+                    if not (rest >> q) & 1:
+                        continue
+                    p1, nrm = qubit_populations(sv, st)
+                    pj = gam * p1[q] / nrm
+                    if not jumped:
+                        tot, w = sums(sv, rest, gam)
+                        pj = pj / max(1.0 - w / tot, 1e-300)
+                    rest &= ~(1 << q)
+                    if rng.uniform() < pj:
+                        apply(sv, k1_of(gam) / math.sqrt(gam * p1[q] / nrm), (q,))
+                        jumped = True
+                    else:
+                        scale_popc(sv, 1 << q, math.sqrt(1.0 - gam),
+                                   1.0 / math.sqrt(1.0 - gam * p1[q] / nrm))
+            else:
+                g = it[1]
+                q = g.qubits()[0]
+                p1, nrm = qubit_populations(sv, st)
+                kraus = [math.sqrt(p) * k for p, k in g.noise_model().branches]
+                probs = []
+                for k in kraus:
+                    w0 = abs(k[0, 0]) ** 2 + abs(k[1, 0]) ** 2
+                    w1 = abs(k[0, 1]) ** 2 + abs(k[1, 1]) ** 2
+                    if abs(np.vdot(k[:, 0], k[:, 1])) >= 1e-15:
+                        raise ValueError("plain trajectories support channels with orthogonal Kraus "
+                                         "columns")
+                    probs.append((w0 * (nrm - p1[q]) + w1 * p1[q]) / nrm)
+                u = rng.uniform() * sum(probs)
+                acc, pick = 0.0, len(kraus) - 1
+                for i, pr in enumerate(probs):
+                    acc += pr
+                    if u < acc:
+                        pick = i
+                        break
+                apply(sv, kraus[pick] / math.sqrt(probs[pick]), (q,))
+        p1, nrm = qubit_populations(sv, st)
+        out[t] = 1.0 - 2.0 * p1 / nrm
+    return out
+
+
 def _main(argv=None) -> None:
     """Time one batch of trajectories of the noisy brickwork construction:
 

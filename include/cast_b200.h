@@ -123,6 +123,21 @@ int cast_b200_marginal_probabilities(uint64_t sv_dptr, uint32_t n_qubits, uint8_
  * 2n-qubit state (QuantumState::populations / trace, src/simulator/mod.rs:387-413). */
 int cast_b200_dm_populations(uint64_t rho_dptr, uint32_t n_physical, uint8_t precision,
                              double *out, void *stream, char *err_buf, size_t err_buf_len);
+/* Amplitude damping on the qubits of `mask` for host-driven quantum-jump
+ * trajectories on the plain path (no counterpart in the reference, whose
+ * ensemble loop weights branches by fixed probabilities,
+ * src/simulator/trajectory.rs:180-265).  damping_sums: *out_total = sum |a_i|^2
+ * and *out_weighted = sum |a_i|^2 (1 - gamma)^popc(i & mask), both FP64, so the
+ * no-jump branch has probability weighted / total; synchronous on `stream`.
+ * scale_popc: a_i *= scale * factor^popc(i & mask) (with factor = sqrt(1 - gamma)
+ * and scale = 1 / sqrt(weighted) it applies the no-jump branch renormalised to
+ * norm 1); enqueued on `stream`. */
+int cast_b200_damping_sums(uint64_t sv_dptr, uint32_t n_qubits, uint8_t precision, uint64_t mask,
+                           double gamma, double *out_total, double *out_weighted, void *stream,
+                           char *err_buf, size_t err_buf_len);
+int cast_b200_scale_popc(uint64_t sv_dptr, uint32_t n_qubits, uint8_t precision, uint64_t mask,
+                         double factor, double scale, void *stream, char *err_buf,
+                         size_t err_buf_len);
 
 /* -- Native fusion planner -----------------------------------------------------------
  * Runs the reference's optimiser - phase 1 size-2 canonicalisation and phase 2

@@ -271,6 +271,25 @@ void cb_store(void *p, double *amps) {
   }
 }
 
+// Amplitudes [first, first + count) as interleaved complex128, for comparing a
+// large state chunk by chunk without a second full copy on the host.
+int cb_store_range(void *p, uint64_t first, uint64_t count, double *amps) {
+  Sv *sv = static_cast<Sv *>(p);
+  const int S = sv->f32 ? Lanes<float>::S : Lanes<double>::S;
+  if (first > (1ull << sv->n) || count > (1ull << sv->n) - first) return 1;
+  for (uint64_t j = 0; j < count; ++j) {
+    const uint64_t b = insert_zero(first + j, S);
+    if (sv->f32) {
+      amps[2 * j] = static_cast<float *>(sv->data)[b];
+      amps[2 * j + 1] = static_cast<float *>(sv->data)[b | (1ull << S)];
+    } else {
+      amps[2 * j] = static_cast<double *>(sv->data)[b];
+      amps[2 * j + 1] = static_cast<double *>(sv->data)[b | (1ull << S)];
+    }
+  }
+  return 0;
+}
+
 // Initialise |0...0>: statevector.rs:439-442 (initialize).
 void cb_zero(void *p) {
   Sv *sv = static_cast<Sv *>(p);

@@ -28,9 +28,13 @@ _lib = None
 
 def build(force: bool = False) -> str:
     """Compile oracle.c (and the threaded CPU baseline) with the committed Makefile."""
-    if force or not os.path.exists(_LIB_PATH) or (
-        os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "oracle.c"))
-    ):
+    stale = False
+    for lib_name, src in (("liboracle.so", "oracle.c"), ("libcpu_baseline.so", "cpu_baseline.cpp")):
+        lib_path = os.path.join(_BUILD, lib_name)
+        if not os.path.exists(lib_path) or (
+                os.path.getmtime(lib_path) < os.path.getmtime(os.path.join(_HERE, src))):
+            stale = True
+    if force or stale:
         subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
 
@@ -251,3 +255,57 @@ def dm_populations(rho: np.ndarray, n: int) -> np.ndarray:
     out = np.zeros(1 << n)
     lib().or_dm_populations(_dp(_cplx_view(rho)), n, _dp(out))
     return out
+
+
+class ThreadedState:
+    """A statevector held by the threaded split-layout CPU restatement
+    (cpu_baseline.cpp, FP64 with CAST's CPU zero/+-1 semantics): the oracle for
+    sizes the scalar one cannot finish in seconds (a 30-qubit complex128 state
+    is 16 GiB of host memory).  Use as a context manager; ``apply`` runs a gate
+    list from |0...0> on `threads` host threads, ``chunk`` reads amplitudes
+    [first, first + count) as complex128."""
+
+    def __init__(self, n: int, threads: int | None = None):
+        build()
+        lib = C.CDLL(os.path.join(_BUILD, "libcpu_baseline.so"))
+        lib.cb_alloc.restype = C.c_void_p
+        lib.cb_alloc.argtypes = [C.c_uint32, C.c_int]
+        lib.cb_free.argtypes = [C.c_void_p]
+        lib.cb_zero.argtypes = [C.c_void_p]
+        lib.cb_apply.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint32), C.c_uint32,
+                                 C.c_int]
+        lib.cb_apply.restype = C.c_int
+        lib.cb_store_range.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.POINTER(C.c_double)]
+        lib.cb_store_range.restype = C.c_int
+        self._lib, self.n = lib, n
+        self.threads = threads or os.cpu_count() or 1
+        self._p = lib.cb_alloc(n, 0)
+        if not self._p:
+            raise MemoryError(f"cannot allocate a {n}-qubit state on the host")
+        lib.cb_zero(self._p)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def close(self):
+        if self._p:
+            self._lib.cb_free(self._p)
+            self._p = None
+
+    def apply(self, gates) -> None:
+        for m, q in gates:
+            mm = np.ascontiguousarray(m, dtype=np.complex128).view(np.float64)
+            qq = np.ascontiguousarray(q, dtype=np.uint32)
+            if self._lib.cb_apply(self._p, mm.ctypes.data_as(C.POINTER(C.c_double)),
+                                  qq.ctypes.data_as(C.POINTER(C.c_uint32)), qq.size, self.threads):
+                raise ValueError(f"cb_apply rejected qubits {tuple(q)}")
+
+    def chunk(self, first: int, count: int) -> np.ndarray:
+        out = np.empty(count, dtype=np.complex128)
+        if self._lib.cb_store_range(self._p, first, count,
+                                    out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double))):
+            raise IndexError("amplitude range out of bounds")
+        return out

@@ -251,6 +251,9 @@ def test_misaligned_pointers_rejected_without_touching_the_device(cblib):
                                                        None, eb, L.ERR_LEN),
         lambda: cblib.cast_b200_dm_populations(bad, 2, 1, out, None, eb, L.ERR_LEN),
         lambda: cblib.cast_b200_norm_squared_noalloc(bad, 32, 1, out, None, eb, L.ERR_LEN),
+        lambda: cblib.cast_b200_damping_sums(bad, 4, 1, 3, 0.1, C.byref(re), C.byref(im), None, eb,
+                                             L.ERR_LEN),
+        lambda: cblib.cast_b200_scale_popc(bad, 4, 0, 3, 0.5, 1.0, None, eb, L.ERR_LEN),
     ]
     for i, call in enumerate(calls):
         eb.value = b""

@@ -39,6 +39,7 @@ def test_reference_arm_line_keeps_the_contract():
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1
     assert "12-qubit brickwork" in cb["sample"]
+    assert cb["build"] in ("-O3 -march=native", "-O3 -march=x86-64-v3")
     assert d["e2e"] == {"value": d["value"], "unit": "GB/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
 

@@ -274,3 +274,82 @@ def test_ranges_reproduce_the_batch(mods, n):
     mean, rows, first = D.run_trajectories_sharded(prog, 300, 5, st)
     assert first == 0 and np.array_equal(rows, z)
     assert np.allclose(mean, z.mean(axis=0), atol=1e-14)
+
+
+def test_plain_fused_trajectories_match_dm(mods, oracle):
+    """The host-driven plain-path trajectories (fused graph segments, host
+    Pauli draws, one masked FP64 reduction per damping layer) against the DM
+    oracle: strong noise so that every branch kind is taken."""
+    T, TR, S = mods
+    n = 5
+    circ = T.QuantumCircuit.brickwork(n, 4, 17, depolarizing=0.04, damping=0.08)
+    z_ref = dm_reference(oracle, circ)
+    n_traj = 3000
+    z = TR.run_plain_fused(circ, n_traj, 11, fusion_k=3)
+    se = z.std(axis=0, ddof=1) / math.sqrt(n_traj)
+    assert np.all(np.abs(z.mean(axis=0) - z_ref) < 5 * se + 2e-3), (z.mean(axis=0), z_ref, se)
+
+
+def test_plain_fused_conditioned_jump_path(mods):
+    """Every qubit in |1>, damping 0.3 on all: the no-jump branch has
+    probability 0.7^n, so the conditioned qubit-by-qubit path dominates;
+    each qubit decays independently, <Z> = -0.4."""
+    T, TR, S = mods
+    n = 6
+    circ = T.QuantumCircuit(n)
+    for q in range(n):
+        circ.add(T.QuantumGate.x(q))
+    for q in range(n):
+        circ.add(T.QuantumGate.amplitude_damping(q, 0.3))
+    n_traj = 3000
+    z = TR.run_plain_fused(circ, n_traj, 5, fusion_k=2)
+    se = z.std(axis=0, ddof=1) / math.sqrt(n_traj)
+    assert np.all(np.abs(z.mean(axis=0) + 0.4) < 5 * se + 1e-3), z.mean(axis=0)
+
+
+def test_plain_fused_general_channel(mods, oracle):
+    T, TR, S = mods
+    n = 4
+    circ = T.QuantumCircuit.brickwork(n, 2, 8)
+    circ.add(T.QuantumGate.pauli_channel(1, 0.1, 0.05, 0.2))
+    circ.add(T.QuantumGate.u3(0.7, 0.1, 0.3, 1))
+    z_ref = dm_reference(oracle, circ)
+    n_traj = 3000
+    z = TR.run_plain_fused(circ, n_traj, 3, fusion_k=3)
+    se = z.std(axis=0, ddof=1) / math.sqrt(n_traj)
+    assert np.all(np.abs(z.mean(axis=0) - z_ref) < 5 * se + 1e-3)
+
+
+@pytest.mark.parametrize("prec", [1, 0])
+def test_damping_sums_and_popcount_scale(mods, oracle, prec):
+    """cast_b200_damping_sums / cast_b200_scale_popc against numpy on a random
+    state: FP64 sums (1e-12 relative for complex128, 1e-6 for complex64) and the
+    masked diagonal pass."""
+    import ctypes as C
+
+    from cast_simulator_b200 import _lib as L
+    from cast_simulator_b200 import cuda as cu
+
+    n, mask, gam = 13, 0b1010010110011, 0.23
+    psi = oracle.random_state(n, 4)
+    sv = cu.CudaStatevector(n, cu.CudaPrecision(prec))
+    sv.upload(psi)
+    psi = sv.download()  # the values the device holds (complex64-rounded for prec 0)
+    idx = np.arange(1 << n)
+    pc = np.array([bin(int(i & mask)).count("1") for i in idx])
+    p = np.abs(psi) ** 2
+    t, d = C.c_double(), C.c_double()
+    eb = L.errbuf()
+    lib = L.lib()
+    L.check(lib.cast_b200_damping_sums(sv.dptr, n, prec, mask, gam, C.byref(t), C.byref(d), None, eb,
+                                       L.ERR_LEN), eb, "damping_sums")
+    rel = 1e-12 if prec == 1 else 1e-6
+    assert abs(t.value - p.sum()) <= rel * p.sum()
+    assert abs(d.value - (p * (1 - gam) ** pc).sum()) <= rel * p.sum()
+    f, sc = math.sqrt(1 - gam), 1.0 / math.sqrt(d.value)
+    L.check(lib.cast_b200_scale_popc(sv.dptr, n, prec, mask, f, sc, None, eb, L.ERR_LEN), eb,
+            "scale_popc")
+    got = sv.download()
+    want = psi * sc * f ** pc
+    assert np.max(np.abs(got - want)) < (1e-14 if prec == 1 else 1e-6)
+    assert abs(np.sum(np.abs(got) ** 2) - 1.0) < (1e-12 if prec == 1 else 1e-5)
