@@ -506,16 +506,65 @@ def trajectory_leg(n: int = 16, depth: int = 30, n_traj: int = 4096, k: int = 3,
     return out
 
 
+def sampling_leg(n: int = 30, depth: int = 20, n_shots: int = 1_000_000, k: int = 4):
+    """On-device shot sampling of the 30-qubit brickwork state (complex128, 16 GiB):
+    n_shots full bitstrings by the inverse CDF (cast_b200_sample), against the
+    reference's method on the same state - download the statevector, build the
+    FP64 CDF on the host, binary-search it per shot (src/simulator/mod.rs:282-291,
+    measure.rs:49-76), timed here with numpy.  The device reads the state once
+    for the chunk totals and once more for the chunks that receive shots."""
+    from cast_simulator_b200 import cuda as cu
+    from cast_simulator_b200.simulator import Event, Stream, sample
+
+    _, gates = build_fused(n, depth, k)
+    _, sv = _run_fused(n, gates, cu.CudaPrecision.F64, reps=1, warm=False, use_graph=False)
+    st = Stream()
+    sample(sv, 1000, seed=1, stream=st)  # first launches
+    e0, e1 = Event(), Event()
+    ts = []
+    keys = None
+    for r in range(3):
+        e0.record(st)
+        keys = sample(sv, n_shots, seed=10 + r, stream=st)
+        e1.record(st)
+        e1.sync()
+        ts.append(e1.elapsed_s(e0))
+    t = float(np.median(ts))
+    state_bytes = (1 << n) * 16
+    out = {"workload": f"brickwork-{n}q-d{depth}-c128 final state, {n_shots} shots",
+           "ms": t * 1e3, "shots_per_s": n_shots / t,
+           "state_reads_gbs": 2 * state_bytes / t / 1e9,
+           "distinct_outcomes": int(np.unique(keys).size)}
+    t0 = time.perf_counter()
+    psi = sv.download()
+    t_dl = time.perf_counter() - t0
+    del sv
+    u = np.random.default_rng(3).random(n_shots)
+    t1 = time.perf_counter()
+    cdf = np.cumsum(psi.real * psi.real + psi.imag * psi.imag)
+    del psi
+    idx = np.minimum(np.searchsorted(cdf, u, side="right"), cdf.size - 1)
+    t_host = time.perf_counter() - t1
+    del cdf, idx
+    out["host_inverse_cdf"] = {"method": "download + numpy FP64 cumsum + searchsorted (one thread)",
+                               "download_s": t_dl, "cdf_and_search_s": t_host,
+                               "total_s": t_dl + t_host, "device_speedup": (t_dl + t_host) / t}
+    return out
+
+
 def serving_leg(n_req: int, rates=(20.0, 80.0, 320.0)):
     """Serving stream (bounded sample of the 10,000-request configuration, same
     distributions): Poisson arrivals of random brickwork circuits, 10..28 qubits,
     depth 5..40, half complex64 / half complex128, 20% noisy (depolarizing 1e-3,
     256 trajectories; noisy circuits have at most 20 qubits, the trajectory
-    kernel's range).  At each swept rate: p50/p99 latency and circuits/s of the
-    continuous-batching engine, and of the same engine with one request at a time
-    (max_slots = 1: sequential execution, measured on the same arrivals).  An
-    unmeasured pass of the fastest stream warms each engine first (kernel module
-    loads, first allocation of each pooled statevector size)."""
+    kernel's range).  At each swept rate: p50/p99 latency and circuits/s of
+      * the engine: continuous batching, small pure requests (<= 16 qubits) run
+        together in the circuit-batch kernel, the rest on worker streams;
+      * the same engine with the circuit-batch kernel off;
+      * sequential execution: the same engine one request at a time
+        (max_slots = 1, no batching), measured on the same arrivals.
+    An unmeasured pass of the fastest stream warms each engine first (kernel
+    module loads, first allocation of each pooled statevector size)."""
     from cast_simulator_b200 import serving as S
 
     def stream(rate):
@@ -523,27 +572,102 @@ def serving_leg(n_req: int, rates=(20.0, 80.0, 320.0)):
 
     out = {"requests_per_rate": n_req, "n_range": [10, 28], "noisy_max_qubits": 20,
            "sample": f"{n_req} requests per rate of the 10,000-request stream's distributions",
-           "rates": []}
-    for label, slots in (("engine", 8), ("sequential", 1)):
-        eng = S.ServingEngine(max_slots=slots)
+           "rates": [{"rate_hz": r} for r in rates]}
+    for label, kw in (("engine", {"max_slots": 8}),
+                      ("engine_no_batch_kernel", {"max_slots": 8, "batch_max_qubits": 0}),
+                      ("sequential", {"max_slots": 1, "batch_max_qubits": 0})):
+        eng = S.ServingEngine(**kw)
         try:
             eng.run_stream(stream(max(rates)))
             for i, rate in enumerate(rates):
                 eng.max_concurrent = 0
+                b0, r0 = eng.batches_run, eng.batched_requests
                 t0 = time.perf_counter()
                 res = eng.run_stream(stream(rate))
                 wall = time.perf_counter() - t0
                 entry = {**S.latency_summary([r.latency for r in res]),
                          "circuits_per_s": n_req / wall, "max_concurrent": eng.max_concurrent,
                          "wall_s": wall}
+                if eng.batches_run > b0:
+                    entry["batch_launches"] = eng.batches_run - b0
+                    entry["batched_requests"] = eng.batched_requests - r0
                 if label == "engine":
-                    out["rates"].append({"rate_hz": rate, **entry})
+                    out["rates"][i].update(entry)
                 else:
-                    out["rates"][i]["sequential"] = entry
-                    out["rates"][i]["p99_speedup_vs_sequential"] = entry["p99_ms"] / out["rates"][i]["p99_ms"]
+                    out["rates"][i][label] = entry
         finally:
             eng.shutdown()
+    for r in out["rates"]:
+        r["p99_speedup_vs_sequential"] = r["sequential"]["p99_ms"] / r["p99_ms"]
+        r["p99_speedup_vs_no_batch_kernel"] = r["engine_no_batch_kernel"]["p99_ms"] / r["p99_ms"]
     return out
+
+
+def circuit_batch_leg(n_circ: int = 2048, n_range=(10, 16), depth_range=(5, 40), seed: int = 5):
+    """Many small circuits (random brickwork, 10..16 qubits, depth 5..40, half
+    complex64 / half complex128) in ONE persistent launch of the circuit-batch
+    kernel (fusion k = 3, one CTA a circuit) against the plain path run circuit
+    after circuit (each fused at k = 4 into a gate program replayed as a CUDA
+    graph, <Z_q> by the FP64 device reduction): time to <Z_q> of every circuit,
+    host fusion excluded on both sides."""
+    from cast_simulator_b200 import _lib as L
+    from cast_simulator_b200 import cuda as cu
+    from cast_simulator_b200.fusion import FusionConfig, optimize_native
+    from cast_simulator_b200.simulator import CircuitBatch, GateProgram, Stream, qubit_populations
+    from cast_simulator_b200.types import QuantumCircuit
+
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_circ):
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        d = int(rng.integers(depth_range[0], depth_range[1] + 1))
+        prec = cu.CudaPrecision.F64 if i % 2 else cu.CudaPrecision.F32
+        specs.append((n, prec, QuantumCircuit.brickwork(n, d, 9000 + i)))
+    st = Stream()
+    fused3 = [optimize_native(n, c.gates(), FusionConfig.size_only(3)) for n, _, c in specs]
+    svs = [cu.CudaStatevector(n, p) for n, p, _ in specs]
+    batch = CircuitBatch()
+    for sv, f in zip(svs, fused3):
+        batch.add(sv, f)
+    batch.run(st)  # warm: buffers, first launch
+    ts = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        zb = batch.run(st)
+        ts.append(time.perf_counter() - t0)
+    t_batch = float(np.median(ts))
+    amps = sum(1 << n for n, _, _ in specs)
+    # plain path, one circuit after another on the whole GPU
+    progs = []
+    for (n, prec, c), sv in zip(specs, svs):
+        f4 = optimize_native(n, c.gates(), FusionConfig.size_only(4))
+        tol = 1e-12 if prec == cu.CudaPrecision.F64 else 1e-6
+        gp = GateProgram(prec, n, tol, tol)
+        eb = L.errbuf()
+        L.check(L.lib().cast_b200_program_add_fused(gp.handle, f4.handle, eb, L.ERR_LEN), eb,
+                "program_add_fused")
+        progs.append(gp)
+
+    def plain_all():
+        zs = []
+        for gp, sv in zip(progs, svs):
+            sv.zero(st)
+            gp.run(sv, st, use_graph=True)
+            p1, nrm = qubit_populations(sv, st)
+            zs.append((nrm - 2 * p1) / nrm)
+        return zs
+
+    plain_all()  # graph capture
+    t0 = time.perf_counter()
+    zp = plain_all()
+    t_plain = time.perf_counter() - t0
+    dev = max(float(np.max(np.abs(a - b))) for a, b in zip(zb, zp))
+    return {"workload": f"{n_circ} random brickwork circuits, {n_range[0]}..{n_range[1]} qubits, "
+                        f"depth {depth_range[0]}..{depth_range[1]}, half complex64 / half complex128",
+            "batch_kernel_s": t_batch, "circuits_per_s": n_circ / t_batch,
+            "amplitudes_per_s": amps / t_batch,
+            "plain_sequential_s": t_plain, "plain_circuits_per_s": n_circ / t_plain,
+            "speedup": t_plain / t_batch, "max_abs_z_diff_batch_vs_plain": dev}
 
 
 def fusion_sweep_leg(n: int, depth: int):
@@ -792,6 +916,8 @@ def main(argv=None):
         if not args.no_sweep:
             line["fusion_sweep"] = fusion_sweep_leg(n, args.depth)
             line["tensor_path"] = tensor_leg(n, args.depth, line["fusion_sweep"])
+        line["sampling"] = sampling_leg(n, args.depth)
+        line["circuit_batch"] = circuit_batch_leg()
         line["trajectories"] = trajectory_leg()
         line["serving"] = serving_leg(args.serve_requests)
         if not args.no_largest:

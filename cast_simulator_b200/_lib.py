@@ -131,6 +131,12 @@ CAST_B200 = [
       C.c_size_t]),
     ("cast_b200_dm_populations", C.c_int,
      [C.c_uint64, C.c_uint32, C.c_uint8, c_dp, C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("cast_b200_sample", C.c_int,
+     [C.c_uint64, C.c_uint32, C.c_uint8, C.c_uint64, C.c_uint64, c_u32p, C.c_uint32, c_u64p,
+      C.c_void_p, C.c_char_p, C.c_size_t]),
+    ("cast_b200_sample_at", C.c_int,
+     [C.c_uint64, C.c_uint32, C.c_uint8, c_dp, C.c_uint64, c_u32p, C.c_uint32, c_u64p, C.c_void_p,
+      C.c_char_p, C.c_size_t]),
     ("cast_b200_damping_sums", C.c_int,
      [C.c_uint64, C.c_uint32, C.c_uint8, C.c_uint64, C.c_double, c_dp, c_dp, C.c_void_p, C.c_char_p,
       C.c_size_t]),
@@ -173,6 +179,18 @@ CAST_B200 = [
     ("cast_b200_traj_run_range", C.c_int,
      [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, c_dp, c_u32p, C.c_void_p, C.c_int,
       C.c_char_p, C.c_size_t]),
+    ("cast_b200_batch_create", C.c_void_p, [C.c_char_p, C.c_size_t]),
+    ("cast_b200_batch_destroy", None, [C.c_void_p]),
+    ("cast_b200_batch_add", C.c_int,
+     [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint8, C.c_uint32, c_u32p, c_u32p,
+      C.POINTER(Complex64), C.c_int, C.c_double, C.c_double, C.c_char_p, C.c_size_t]),
+    ("cast_b200_batch_add_fused", C.c_int,
+     [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint8, C.c_void_p, C.c_int, C.c_double, C.c_double,
+      C.c_char_p, C.c_size_t]),
+    ("cast_b200_batch_num_circuits", C.c_uint32, [C.c_void_p]),
+    ("cast_b200_batch_num_z", C.c_uint32, [C.c_void_p]),
+    ("cast_b200_batch_clear", None, [C.c_void_p]),
+    ("cast_b200_batch_run", C.c_int, [C.c_void_p, c_dp, C.c_void_p, C.c_char_p, C.c_size_t]),
     ("cast_b200_norm_squared_noalloc", C.c_int,
      [C.c_uint64, C.c_size_t, C.c_uint8, c_dp, C.c_void_p, C.c_char_p, C.c_size_t]),
 ]

@@ -26,6 +26,7 @@
 // final reductions are FP64; amplitudes and gate arithmetic are FP32.
 #include "../../include/cast_b200.h"
 #include "internal.hpp"
+#include "philox.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -66,24 +67,12 @@ struct TRun {  // device-resident, rewritten before each launch
   uint64_t seed;
 };
 
-// ── Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) ──────────────────────
+// Philox-4x32-10 (philox.cuh): counter (event, 0, trajectory, 0x5eed5eed),
+// key = the 64-bit seed.
 __device__ __forceinline__ double philox_uniform(uint64_t seed, uint32_t traj, uint32_t event) {
-  uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-  uint32_t x0 = event, x1 = 0, x2 = traj, x3 = 0x5eed5eedu;
-#pragma unroll
-  for (int r = 0; r < 10; ++r) {
-    const uint32_t lo0 = 0xD2511F53u * x0, hi0 = __umulhi(0xD2511F53u, x0);
-    const uint32_t lo1 = 0xCD9E8D57u * x2, hi1 = __umulhi(0xCD9E8D57u, x2);
-    const uint32_t y0 = hi1 ^ x1 ^ k0, y2 = hi0 ^ x3 ^ k1;
-    x0 = y0;
-    x1 = lo1;
-    x2 = y2;
-    x3 = lo0;
-    k0 += 0x9E3779B9u;
-    k1 += 0xBB67AE85u;
-  }
-  const uint64_t bits = ((uint64_t)x0 << 32) | x1;
-  return (double)(bits >> 11) * 0x1.0p-53;
+  uint32_t x[4] = {event, 0u, traj, 0x5eed5eedu};
+  cb2::philox4x32_10(x, (uint32_t)seed, (uint32_t)(seed >> 32));
+  return cb2::philox_unit(x);
 }
 
 struct Shared {

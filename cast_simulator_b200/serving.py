@@ -10,10 +10,15 @@ this engine keeps many requests in flight:
     device-memory budget covers its footprint (16 * 2^n bytes for complex128,
     8 * 2^n for complex64, the trajectory workspace for noisy requests);
     admission never reorders requests;
-  * each admitted request runs on its own CUDA stream in a worker thread: its
-    gates are fused by the native planner and uploaded as a gate program that is
-    launched on that stream (noisy requests run the persistent trajectory
-    kernel from a CUDA graph); work of different requests overlaps on the device;
+  * a small pure request (at most ``batch_max_qubits`` qubits) goes to the
+    batcher: every small request admitted while the previous batch ran is fused
+    by the native planner and executed with the others in ONE persistent launch
+    of the circuit-batch kernel (one CTA a circuit, <Z_q> reduced on the device);
+  * any other admitted request runs on its own CUDA stream in a worker thread:
+    its gates are fused by the native planner and uploaded as a gate program
+    that is launched on that stream (noisy requests run the persistent
+    trajectory kernel from a CUDA graph); work of different requests overlaps on
+    the device;
   * when a request finishes, its <Z_q> vector is read back (FP64 device
     reduction), its memory returns to the budget and the next requests are
     admitted - the batch composition changes continuously.
@@ -34,7 +39,7 @@ import numpy as np
 from . import _lib as L
 from .cuda import CudaPrecision, CudaStatevector, cuda_free_memory_bytes
 from .fusion import FusionConfig, optimize_native
-from .simulator import GateProgram, Stream, qubit_populations
+from .simulator import CircuitBatch, GateProgram, Stream, qubit_populations
 from .trajectory import TrajectoryProgram
 from .types import QuantumCircuit
 
@@ -103,15 +108,31 @@ class _SvPool:
 
 class ServingEngine:
     def __init__(self, max_slots: int = 8, mem_budget_bytes: int | None = None, fusion_k: int = 4,
-                 traj_fusion_k: int = 3, use_graph: bool = False):
+                 traj_fusion_k: int = 3, use_graph: bool = False, batch_max_qubits: int = 16,
+                 batch_fusion_k: int = 3, max_batch: int = 1024):
+        """max_slots: requests running at once on the worker streams.
+        batch_max_qubits: pure requests of at most this many qubits run batched
+        in the circuit-batch kernel (0 turns batching off); batch_fusion_k: their
+        fusion width (<= 4); max_batch: circuits a batch launch takes at most
+        (batched requests do not use worker slots)."""
         if mem_budget_bytes is None:
             free, _ = cuda_free_memory_bytes()
             mem_budget_bytes = int(free * 0.8)
+        if not 0 <= batch_max_qubits <= 20 or not 1 <= batch_fusion_k <= 4:
+            raise ValueError("batch_max_qubits must be 0..20 and batch_fusion_k 1..4")
         self.max_slots = max_slots
         self.budget = mem_budget_bytes
         self.fusion_k = fusion_k
         self.traj_fusion_k = traj_fusion_k
         self.use_graph = use_graph
+        self.batch_max_qubits = batch_max_qubits
+        self.batch_fusion_k = batch_fusion_k
+        self.max_batch = max_batch
+        self._bwork: collections.deque = collections.deque()
+        self._bcv = threading.Condition()
+        self._batched_active = 0
+        self.batches_run = 0
+        self.batched_requests = 0
         self._pool = _SvPool()
         self._pending: collections.deque = collections.deque()
         self._cv = threading.Condition()
@@ -124,9 +145,11 @@ class ServingEngine:
         self.max_concurrent = 0
         self._workers = [threading.Thread(target=self._worker, daemon=True) for _ in range(max_slots)]
         self._dispatcher = threading.Thread(target=self._dispatch, daemon=True)
+        self._batcher = threading.Thread(target=self._batch_loop, daemon=True)
         for t in self._workers:
             t.start()
         self._dispatcher.start()
+        self._batcher.start()
 
     # -- public API
     def now(self) -> float:
@@ -167,9 +190,12 @@ class ServingEngine:
             fut.set_exception(RuntimeError("the serving engine was shut down before admission"))
         with self._work_cv:
             self._work_cv.notify_all()
+        with self._bcv:
+            self._bcv.notify_all()
         self._dispatcher.join(timeout=30)
         for t in self._workers:
             t.join(timeout=30)
+        self._batcher.join(timeout=30)
         self._pool.drop_all()
 
     # -- internals
@@ -183,14 +209,31 @@ class ServingEngine:
                 req, fut, t_arr = self._pending.popleft()
                 need = request_bytes(req)
                 self._in_use += need
-                self._active += 1
-                self.max_concurrent = max(self.max_concurrent, self._active)
-            with self._work_cv:
-                self._work.append((req, fut, t_arr, need, self.now()))
-                self._work_cv.notify()
+                batched = self._batchable(req)
+                if batched:
+                    self._batched_active += 1
+                else:
+                    self._active += 1
+                self.max_concurrent = max(self.max_concurrent, self._active + self._batched_active)
+            if batched:
+                with self._bcv:
+                    self._bwork.append((req, fut, t_arr, need, self.now()))
+                    self._bcv.notify()
+            else:
+                with self._work_cv:
+                    self._work.append((req, fut, t_arr, need, self.now()))
+                    self._work_cv.notify()
+
+    def _batchable(self, req: Request) -> bool:
+        return not req.n_traj and req.circuit.n_qubits() <= self.batch_max_qubits
 
     def _can_admit_head(self) -> bool:
-        if not self._pending or self._active >= self.max_slots:
+        if not self._pending:
+            return False
+        if self._batchable(self._pending[0][0]):
+            if self._batched_active >= self.max_batch:
+                return False
+        elif self._active >= self.max_slots:
             return False
         need = request_bytes(self._pending[0][0])
         if self._in_use + need > self.budget:
@@ -219,6 +262,52 @@ class ServingEngine:
                 with self._cv:
                     self._in_use -= need
                     self._active -= 1
+                    self._cv.notify_all()
+
+    def _batch_loop(self) -> None:
+        """Runs every small request admitted since the last batch in one launch
+        of the circuit-batch kernel, then completes them together."""
+        stream = Stream()
+        batch = CircuitBatch()
+        while True:
+            with self._bcv:
+                while not self._bwork and not self._stop:
+                    self._bcv.wait(timeout=0.1)
+                if self._stop and not self._bwork:
+                    return
+                items = [self._bwork.popleft() for _ in range(min(len(self._bwork), self.max_batch))]
+            batch.clear()
+            svs = []
+            try:
+                for req, *_ in items:
+                    n = req.circuit.n_qubits()
+                    fused = optimize_native(n, req.circuit.gates(),
+                                            FusionConfig.size_only(self.batch_fusion_k))
+                    sv = self._pool.get(n, req.precision)
+                    svs.append(sv)
+                    batch.add(sv, fused, init_zero=True)
+                zs = batch.run(stream)
+                done = self.now()
+                for (req, fut, t_arr, _, t_adm), z in zip(items, zs):
+                    fut.set_result(Result(req.rid, z, t_arr, t_adm, done, req.circuit.n_qubits(),
+                                          req.precision, 0))
+                self.batches_run += 1
+                self.batched_requests += len(items)
+            except Exception as e:  # the batch fails, the engine keeps serving
+                try:
+                    stream.sync()
+                except Exception:
+                    pass
+                for _, fut, *_ in items:
+                    if not fut.done():
+                        fut.set_exception(e)
+            finally:
+                for sv in svs:
+                    self._pool.put(sv)
+                with self._cv:
+                    for *_, need, _ in items:
+                        self._in_use -= need
+                    self._batched_active -= len(items)
                     self._cv.notify_all()
 
     def _execute(self, req: Request, stream: Stream) -> np.ndarray:

@@ -192,6 +192,108 @@ def marginal_probabilities(sv: CudaStatevector, measured, stream: Stream | None 
     return out
 
 
+class CircuitBatch:
+    """Many small circuits run in one persistent launch (cast_b200_batch_*): one
+    CTA a circuit on its own device statevector, each circuit's <Z_q> reduced in
+    FP64 on the device.  ``add`` takes a gate list (objects with ``matrix()`` /
+    ``qubits()``, at most 4 qubits a gate - fuse with size_max <= 4) or a native
+    fused circuit; ``run`` executes every circuit added since the last
+    ``clear`` and returns their <Z> vectors in the order they were added."""
+
+    def __init__(self):
+        eb = L.errbuf()
+        self.handle = L.check_ptr(L.lib().cast_b200_batch_create(eb, L.ERR_LEN), eb, "batch_create")
+        self._sizes: list[int] = []
+
+    def add(self, sv: CudaStatevector, gates, init_zero: bool = True, ztol: float | None = None,
+            otol: float | None = None) -> int:
+        """Append a circuit acting on `sv`; returns its index in the batch."""
+        f64 = sv.precision() == CudaPrecision.F64
+        zt = ztol if ztol is not None else (1e-12 if f64 else 1e-6)
+        ot = otol if otol is not None else (1e-12 if f64 else 1e-6)
+        eb = L.errbuf()
+        if hasattr(gates, "handle"):  # a native fused circuit
+            rc = L.lib().cast_b200_batch_add_fused(self.handle, sv.dptr, sv.n_qubits(),
+                                                   int(sv.precision()), gates.handle, int(init_zero),
+                                                   zt, ot, eb, L.ERR_LEN)
+        else:
+            gates = list(gates)
+            ks = np.array([len(g.qubits()) for g in gates], dtype=np.uint32)
+            qs = np.array([q for g in gates for q in g.qubits()], dtype=np.uint32)
+            ms = (np.concatenate([np.ascontiguousarray(g.matrix(), dtype=np.complex128).reshape(-1)
+                                  for g in gates]) if gates else np.zeros(1, dtype=np.complex128))
+            rc = L.lib().cast_b200_batch_add(self.handle, sv.dptr, sv.n_qubits(), int(sv.precision()),
+                                             len(gates), ks.ctypes.data_as(L.c_u32p),
+                                             qs.ctypes.data_as(L.c_u32p),
+                                             ms.view(np.float64).ctypes.data_as(C.POINTER(L.Complex64)),
+                                             int(init_zero), zt, ot, eb, L.ERR_LEN)
+        L.check(rc, eb, "batch_add")
+        self._sizes.append(sv.n_qubits())
+        return len(self._sizes) - 1
+
+    def __len__(self):
+        return len(self._sizes)
+
+    def run(self, stream: Stream | None = None) -> list[np.ndarray]:
+        out = np.zeros(max(1, sum(self._sizes)))
+        eb = L.errbuf()
+        L.check(L.lib().cast_b200_batch_run(self.handle, out.ctypes.data_as(L.c_dp),
+                                            stream.handle if stream else None, eb, L.ERR_LEN),
+                eb, "batch_run")
+        res, at = [], 0
+        for n in self._sizes:
+            res.append(out[at:at + n].copy())
+            at += n
+        return res
+
+    def clear(self) -> None:
+        L.lib().cast_b200_batch_clear(self.handle)
+        self._sizes.clear()
+
+    def __del__(self):
+        try:
+            L.lib().cast_b200_batch_destroy(self.handle)
+        except Exception:
+            pass
+
+
+def sample(sv: CudaStatevector, n_shots: int, seed: int = 0, measured=None,
+           stream: Stream | None = None, uniforms=None) -> np.ndarray:
+    """Shot keys sampled on the device from |a_i|^2 (cast_b200_sample): the
+    sampled basis indices, or with `measured` their bits at those qubits packed
+    into bits 0..m-1 (the reference's compress_bits), in ascending order of the
+    sampled index.  `uniforms` (sorted, in [0, 1), one a shot) replaces the
+    device's Philox draws (cast_b200_sample_at)."""
+    q = np.ascontiguousarray([] if measured is None else list(measured), dtype=np.uint32)
+    out = np.zeros(n_shots, dtype=np.uint64)
+    eb = L.errbuf()
+    qp = q.ctypes.data_as(L.c_u32p) if q.size else None
+    h = stream.handle if stream else None
+    if uniforms is None:
+        rc = L.lib().cast_b200_sample(sv.dptr, sv.n_qubits(), int(sv.precision()), n_shots,
+                                      seed & ((1 << 64) - 1), qp, q.size,
+                                      out.ctypes.data_as(L.c_u64p), h, eb, L.ERR_LEN)
+    else:
+        u = np.ascontiguousarray(uniforms, dtype=np.float64)
+        if u.size != n_shots:
+            raise ValueError("one uniform a shot")
+        rc = L.lib().cast_b200_sample_at(sv.dptr, sv.n_qubits(), int(sv.precision()),
+                                         u.ctypes.data_as(L.c_dp), n_shots, qp, q.size,
+                                         out.ctypes.data_as(L.c_u64p), h, eb, L.ERR_LEN)
+    L.check(rc, eb, "sample")
+    return out
+
+
+def sample_histogram(sv: CudaStatevector, n_shots: int, seed: int = 0, measured=None,
+                     stream: Stream | None = None) -> dict:
+    """{outcome: count} over the measured qubits (all qubits when None): the
+    reference's batch_sample result (src/simulator/measure.rs:49-76), drawn on
+    the device without downloading the statevector."""
+    keys = sample(sv, n_shots, seed, measured, stream)
+    vals, counts = np.unique(keys, return_counts=True)
+    return {int(k): int(c) for k, c in zip(vals, counts)}
+
+
 def prepare_gates(graph: CircuitGraph, n_physical: int, repr_: Representation):
     """mod.rs:586-613: SV needs unitary gates; DM lifts each gate to a
     superoperator on 2n virtual qubits."""
@@ -235,6 +337,14 @@ class QuantumState:
         if self.is_pure():
             return self.sv.norm_squared()
         return float(self.populations().sum())
+
+    def sample(self, n_shots: int, measured=None, seed: int = 0) -> dict:
+        """Histogram {outcome: count} of n_shots measurements of the measured
+        qubits (all when None), drawn on the device (pure states)."""
+        if not self.is_pure():
+            raise ValueError("sampling is for statevectors; use the trajectory sampler for "
+                             "noisy circuits")
+        return sample_histogram(self.sv, n_shots, seed, measured)
 
     def expectation_z(self) -> np.ndarray:
         """<Z_q> for every physical qubit (pure states), FP64 on the device."""

@@ -123,6 +123,27 @@ int cast_b200_marginal_probabilities(uint64_t sv_dptr, uint32_t n_qubits, uint8_
  * 2n-qubit state (QuantumState::populations / trace, src/simulator/mod.rs:387-413). */
 int cast_b200_dm_populations(uint64_t rho_dptr, uint32_t n_physical, uint8_t precision,
                              double *out, void *stream, char *err_buf, size_t err_buf_len);
+/* Shot sampling on the device (replaces the reference's host-side path:
+ * marginal_probabilities downloads the statevector, src/simulator/mod.rs:282-291,
+ * and batch_sample draws by the inverse CDF, src/simulator/measure.rs:49-76).
+ * Draws n_shots basis states from |a_i|^2 / sum |a|^2 without copying the state
+ * off the device: the CDF is an exact 64-bit fixed-point prefix sum (each
+ * probability scaled by 2^62 / total), and a shot with uniform u takes the
+ * first index whose inclusive prefix is > floor(u * Q), Q the integer total
+ * (the last index if none).  out_keys[i] (host array of n_shots) receives the
+ * sampled index, or with n_measured > 0 its bits at measured[0..m) packed into
+ * bits 0..m-1; keys come in ascending order of the sampled index.
+ * cast_b200_sample draws the uniforms on the device (Philox-4x32-10 keyed by
+ * `seed`, sorted by construction: normalised exponential spacings);
+ * cast_b200_sample_at takes them from the caller (non-decreasing, in [0, 1)).
+ * Up to 36 qubits and 2^30 shots a call; synchronous on `stream`. */
+int cast_b200_sample(uint64_t sv_dptr, uint32_t n_qubits, uint8_t precision, uint64_t n_shots,
+                     uint64_t seed, const uint32_t *measured, uint32_t n_measured,
+                     uint64_t *out_keys, void *stream, char *err_buf, size_t err_buf_len);
+int cast_b200_sample_at(uint64_t sv_dptr, uint32_t n_qubits, uint8_t precision,
+                        const double *sorted_uniforms, uint64_t n_shots, const uint32_t *measured,
+                        uint32_t n_measured, uint64_t *out_keys, void *stream, char *err_buf,
+                        size_t err_buf_len);
 /* Amplitude damping on the qubits of `mask` for host-driven quantum-jump
  * trajectories on the plain path (no counterpart in the reference, whose
  * ensemble loop weights branches by fixed probabilities,
@@ -233,6 +254,36 @@ int cast_b200_traj_run(void *program, uint32_t n_traj, uint64_t seed, double *ou
 int cast_b200_traj_run_range(void *program, uint32_t first, uint32_t n_traj, uint64_t seed,
                              double *out_z, uint32_t *out_samples, void *stream, int use_graph,
                              char *err_buf, size_t err_buf_len);
+
+/* -- Many small circuits in one launch ------------------------------------------------
+ * No counterpart in the reference, which runs one circuit at a time
+ * (Simulator::simulate, src/simulator/mod.rs:523-547, one kernel per gate).  A
+ * batch holds independent circuits of 1..20 qubits, each with its own device
+ * statevector (2^n amplitudes of its precision, 16-byte aligned; circuits of a
+ * batch must not share memory), its own precision and gates of 1..4 qubits
+ * (qubits ascending; matrices snapped like the plain path's).  batch_run
+ * executes every circuit in ONE persistent kernel - one CTA a circuit, claimed
+ * from a device work counter, longest first - then writes <Z_q> (FP64) of every
+ * circuit to out_z, circuit after circuit in the order they were added
+ * (cast_b200_batch_num_z values); synchronous on `stream`.  The circuits'
+ * statevectors hold the final states afterwards.  init_zero: start from
+ * |0...0> (else from the statevector's contents).  A batch keeps its circuits
+ * until batch_clear and its device buffers until batch_destroy. */
+void *cast_b200_batch_create(char *err_buf, size_t err_buf_len);
+void cast_b200_batch_destroy(void *batch);
+int cast_b200_batch_add(void *batch, uint64_t sv_dptr, uint32_t n_qubits, uint8_t precision,
+                        uint32_t n_gates, const uint32_t *gate_k, const uint32_t *qubits,
+                        const cast_complex64_t *matrices, int init_zero, double ztol, double otol,
+                        char *err_buf, size_t err_buf_len);
+/* The gates of a cast_b200_fuse result (fused at size_max <= 4). */
+int cast_b200_batch_add_fused(void *batch, uint64_t sv_dptr, uint32_t n_qubits, uint8_t precision,
+                              const void *fused, int init_zero, double ztol, double otol,
+                              char *err_buf, size_t err_buf_len);
+uint32_t cast_b200_batch_num_circuits(const void *batch);
+uint32_t cast_b200_batch_num_z(const void *batch);
+void cast_b200_batch_clear(void *batch);
+int cast_b200_batch_run(void *batch, double *out_z, void *stream, char *err_buf,
+                        size_t err_buf_len);
 
 /* -- Allocation-free norm^2 -------------------------------------------------------
  * No counterpart in the reference: an extra variant of cast_cuda_norm_squared

@@ -309,3 +309,40 @@ class ThreadedState:
                                     out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double))):
             raise IndexError("amplitude range out of bounds")
         return out
+
+
+# ── shot sampling (src/simulator/measure.rs:49-76) ──────────────────────────
+
+
+def compress_bits(idx: np.ndarray, measured) -> np.ndarray:
+    """Bits of each index at the measured qubits packed into bits 0..m-1
+    (compress_bits in the reference's src/types/mod.rs)."""
+    idx = np.asarray(idx, dtype=np.uint64)
+    out = np.zeros_like(idx)
+    for j, q in enumerate(measured):
+        out |= ((idx >> np.uint64(q)) & np.uint64(1)) << np.uint64(j)
+    return out
+
+
+def batch_sample_fp64(probs: np.ndarray, u: np.ndarray) -> np.ndarray:
+    """The reference's inverse-CDF rule (measure.rs:61-75): cdf = running FP64
+    sum of the probabilities in index order; the outcome of u is the first index
+    whose cdf entry is > u, clamped to the last index."""
+    cdf = np.cumsum(np.asarray(probs, dtype=np.float64))
+    return np.minimum(np.searchsorted(cdf, np.asarray(u, dtype=np.float64), side="right"),
+                      cdf.size - 1).astype(np.uint64)
+
+
+def sample_fixed_point(psi: np.ndarray, u: np.ndarray, scale: float = 2.0 ** 62) -> np.ndarray:
+    """The same rule over the 64-bit fixed-point CDF the device uses: p_i =
+    re^2 + im^2 (separately rounded), q_i = round-half-even(p_i * scale) as
+    uint64, exact prefix sums, target t = floor(u * float(Q)) with Q the integer
+    total, outcome = first index whose inclusive prefix is > t (the last index
+    if none).  scale = 2^62 is the device's choice for a state whose total
+    probability lies in (0.5, 2)."""
+    psi = np.asarray(psi, dtype=np.complex128)
+    p = psi.real * psi.real + psi.imag * psi.imag
+    q = np.rint(p * scale).astype(np.uint64)
+    cdf = np.cumsum(q, dtype=np.uint64)
+    t = np.floor(np.asarray(u, dtype=np.float64) * float(cdf[-1])).astype(np.uint64)
+    return np.minimum(np.searchsorted(cdf, t, side="right"), cdf.size - 1).astype(np.uint64)

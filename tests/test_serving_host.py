@@ -89,6 +89,7 @@ def fake_engine(monkeypatch):
     engines = []
 
     def make(**kw):
+        kw.setdefault("batch_max_qubits", 0)  # every request on the worker path
         eng = S.ServingEngine(**kw)
         engines.append(eng)
         return eng
@@ -164,3 +165,79 @@ def test_oversized_requests_and_shutdown(fake_engine):
     assert done >= 1 and done + failed == 5
     with pytest.raises(RuntimeError, match="shut down"):
         eng.submit(_reqs(20, 1)[0])
+
+
+class _FakeSv:
+    def __init__(self, n, prec):
+        self.n, self.prec = n, prec
+
+    def n_qubits(self):
+        return self.n
+
+    def precision(self):
+        return self.prec
+
+    def nbytes(self):
+        return (16 if self.prec == CudaPrecision.F64 else 8) << self.n
+
+
+def test_small_requests_run_batched(monkeypatch):
+    """Small pure requests go to the batcher, which runs every request admitted
+    while its previous launch ran in one batch; a failing batch fails only its
+    own requests; memory returns to the budget."""
+    import threading
+    import time
+
+    runs = []
+
+    class FakeBatch:
+        def __init__(self):
+            self.items = []
+
+        def clear(self):
+            self.items = []
+
+        def add(self, sv, fused, init_zero=True):
+            self.items.append(sv)
+
+        def run(self, stream=None):
+            time.sleep(0.05)
+            runs.append(len(self.items))
+            if any(getattr(sv, "poison", False) for sv in self.items):
+                raise RuntimeError("batch failed")
+            return [np.full(sv.n, float(len(runs))) for sv in self.items]
+
+    pool_lock = threading.Lock()
+
+    def pool_get(self, n, prec):
+        with pool_lock:
+            return _FakeSv(n, prec)
+
+    monkeypatch.setattr(S, "Stream", _FakeStream)
+    monkeypatch.setattr(S, "CircuitBatch", FakeBatch)
+    monkeypatch.setattr(S._SvPool, "get", pool_get)
+    eng = S.ServingEngine(max_slots=2, mem_budget_bytes=1 << 40, batch_max_qubits=12)
+    try:
+        futs = [eng.submit(r) for r in _reqs(10, 40)]
+        res = [f.result(timeout=30) for f in futs]
+        assert [r.rid for r in res] == list(range(40))
+        assert sum(runs) == 40 and len(runs) < 40  # requests were grouped
+        assert eng.batched_requests == 40 and eng.batches_run == len(runs)
+        assert eng._in_use == 0 and eng._batched_active == 0 and eng._active == 0
+        # a failing batch fails its requests, later ones are served
+        orig = pool_get
+
+        def poisoned(self, n, prec):
+            sv = orig(self, n, prec)
+            sv.poison = True
+            return sv
+
+        monkeypatch.setattr(S._SvPool, "get", poisoned)
+        bad = eng.submit(_reqs(10, 1)[0])
+        with pytest.raises(RuntimeError, match="batch failed"):
+            bad.result(timeout=30)
+        monkeypatch.setattr(S._SvPool, "get", pool_get)
+        assert eng.submit(_reqs(10, 1)[0]).result(timeout=30).rid == 0
+        assert eng._in_use == 0 and eng._batched_active == 0
+    finally:
+        eng.shutdown()
