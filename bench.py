@@ -703,6 +703,56 @@ def fusion_sweep_leg(n: int, depth: int):
     return out
 
 
+def tensor_leg(n: int, depth: int, sweep: dict):
+    """Tensor-core fused path (complex64, split BF16, k = 5 and 6) against the
+    plain CUDA-core path at its best width (k = 4) on the full 30-qubit brickwork,
+    from the fusion sweep's runs; and 1 - |<psi_ref|psi>| against the FP64 CPU
+    restatement of CAST's statevector path on a 24-qubit brickwork of the same
+    construction."""
+    from cast_simulator_b200 import cuda as cu
+    from cast_simulator_b200.fusion import FusionConfig, optimize_native
+    from cast_simulator_b200.types import QuantumCircuit
+
+    peak = measured_peak_hbm()[0]
+    out = {"workload": f"brickwork-{n}q-d{depth}-c64", "runs": []}
+    circ = QuantumCircuit.brickwork(n, depth, 2024)
+    by_k = {}
+    for r in sweep["runs"]:
+        if r["precision"] == "c64" and (r["fusion_k"], r["tensor_cores"]) in ((4, False), (5, True), (6, True)):
+            by_k[r["fusion_k"]] = r
+    for k in (4, 5, 6):
+        r = by_k[k]
+        t = r["ms_per_circuit"] / 1e3
+        run = {"fusion_k": k, "tensor_cores": r["tensor_cores"], "fused_gates": r["fused_gates"],
+               "ms_per_circuit": r["ms_per_circuit"], "hbm_gbs": r["hbm_gbs"],
+               "hbm_frac": r["hbm_gbs"] / peak}
+        if r["tensor_cores"]:
+            gates = optimize_native(n, circ.gates(), FusionConfig.size_only(k)).gates()
+            # tensor-pipe work of the passes that ran there: 3 split products of the
+            # real (2D x 2D) GEMM per group, D = 2^kg
+            flops = sum(3 * 2 * (2 << g.n_qubits()) ** 2 * (1 << (n - g.n_qubits()))
+                        for g in gates if g.n_qubits() in (5, 6))
+            bf16 = measured_peak_bf16()
+            run["tensor_tflops"] = flops / t / 1e12
+            run["tensor_frac"] = flops / t / 1e12 / bf16 if bf16 else None
+        out["runs"].append(run)
+    base = out["runs"][0]["ms_per_circuit"]
+    for r in out["runs"]:
+        r["speedup_vs_plain_k4"] = base / r["ms_per_circuit"]
+    nf = 24
+    small = QuantumCircuit.brickwork(nf, depth, 2024)
+    ref = cpu_reference_state(nf, optimize_native(nf, small.gates(), FusionConfig.size_only(4)).gates(),
+                              os.cpu_count() or 1)
+    fid = {}
+    for k in (5, 6):
+        g = optimize_native(nf, small.gates(), FusionConfig.size_only(k)).gates()
+        _, sv = _run_fused(nf, g, cu.CudaPrecision.F32, True, reps=1, warm=False)
+        fid[f"k{k}"] = fidelity_vs(ref, sv.download())
+        del sv
+    out["fidelity_24q_vs_cpu_fp64"] = fid
+    return out
+
+
 def traffic_from_profile(n: int, precision: str, k: int):
     """DRAM bytes per launch of the dominant kernel from the committed ncu
     summary (captured on a smaller statevector and scaled by amplitudes)."""

@@ -31,7 +31,7 @@ def _cases(T, F):
     for i, n in enumerate([4, 7, 10, 12, 13, 16, 9, 14, 5, 11, 16, 8]):
         depth = int(rng.integers(3, 12))
         circ = T.QuantumCircuit.brickwork(n, depth, 100 + i)
-        k = [1, 2, 3, 4][i % 4]
+        k = [2, 3, 4][i % 3]
         fused = F.optimize_native(n, circ.gates(), F.FusionConfig.size_only(k))
         prec = 1 if i % 2 == 0 else 0
         out.append((n, prec, circ, fused, i % 3 == 2))
