@@ -836,6 +836,92 @@ def roofline_of(run: dict, n: int, precision: str) -> dict:
             "peak_kind": peak_kind}
 
 
+def sharded_line(args, ws: int, rank: int, local: int, pg) -> dict:
+    """The brickwork on one statevector sharded over the N ranks (weak scaling:
+    every rank holds 2^n amplitudes, the circuit has n + log2 N qubits), fused
+    at width k; gates on global qubits are preceded by pairwise qubit-swap
+    exchanges over NCCL, streamed through fixed staging buffers, with the
+    look-ahead planner choosing what to evict.  Timed like the headline: warm-up
+    runs, then `steps` runs bracketed by a barrier and CUDA events on the
+    launching stream, max over ranks.  e2e: the same run with <Z_q> read back to
+    the host every step (the gate matrices go from host to device every step)."""
+    import torch
+
+    from cast_simulator_b200 import distributed as D
+    from cast_simulator_b200.simulator import Event
+
+    g = ws.bit_length() - 1
+    if 1 << g != ws:
+        raise ValueError("the sharded statevector needs a power-of-two number of GPUs")
+    n_tot = args.n + g
+    circ, gates = build_fused(n_tot, args.depth, args.k)
+    f64 = args.precision == "f64"
+    dtype = torch.complex128 if f64 else torch.complex64
+    shard = torch.zeros(1 << args.n, dtype=dtype, device=f"cuda:{local}")
+    sv = D.ShardedStatevector(n_tot, shard, D.cuda_apply_local(1 if f64 else 0), group=None)
+
+    def step():
+        sv.set_zero()
+        sv.apply_circuit(gates)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ex0, amps0 = sv.n_exchanges, sv.exchanged_amps
+    st = torch.cuda.current_stream()
+    e0, e1 = Event(), Event()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(st.cuda_stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(st.cuda_stream)
+        e1.sync()
+    t = max(e1.elapsed_s(e0), 1e-12)
+    ex_step = (sv.n_exchanges - ex0) / max(1, args.steps)
+    amps_step = (sv.exchanged_amps - amps0) / max(1, args.steps)
+    if pg:
+        tt = torch.tensor([t], device=f"cuda:{local}", dtype=torch.float64)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t = float(tt.item())
+    amp = 16 if f64 else 8
+    bytes_per_pass = 2 * (1 << n_tot) * amp
+    value = args.steps * len(gates) * bytes_per_pass / t / 1e9
+    # e2e: <Z> back to the host every step
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+        z = sv.expectation_z()
+    e2e_t = time.perf_counter() - t0
+    if pg:
+        et = torch.tensor([e2e_t], device=f"cuda:{local}", dtype=torch.float64)
+        pg.all_reduce(et, op=pg.ReduceOp.MAX)
+        e2e_t = float(et.item())
+    return {
+        "metric": "HBM GB/s (fused-gate statevector passes)", "value": value, "unit": "GB/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+        "config": {"workload": f"brickwork-{n_tot}q-d{args.depth}-{'c128' if f64 else 'c64'}-k{args.k}",
+                   "n_qubits": n_tot, "shard_qubits": args.n, "depth": args.depth,
+                   "fusion_k": args.k, "unfused_gates": len(circ), "fused_gates": len(gates),
+                   "l2": "no flush: each shard is larger than L2",
+                   "parallelism": f"sv-shard{ws}"},
+        "exchange": {"per_step": ex_step, "amplitudes_per_step_per_rank": amps_step,
+                     "bytes_per_step_per_rank": 2 * amps_step * amp},
+        "e2e": {"value": args.steps * len(gates) * bytes_per_pass / e2e_t / 1e9, "unit": "GB/s",
+                "h2d_bytes_per_step": sum(16 * gg.matrix().size for gg in gates),
+                "d2h_bytes_per_step": 8 * (n_tot + 1)},
+        "gpu_launches": args.steps * len(gates),
+        "clocks": clk.summary(),
+        "z_expectation_sample": [float(x) for x in z[:4]],
+    }
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -855,6 +941,10 @@ def main(argv=None):
     ap.add_argument("--no-largest", action="store_true",
                     help="skip the 34q complex64 / 33q complex128 largest-fit leg")
     ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--sharded", action="store_true",
+                    help="one statevector sharded over the GPUs (the default when N > 1)")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with N > 1: N independent replicas of the 30-qubit headline instead")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
@@ -875,6 +965,14 @@ def main(argv=None):
 
     eb = L.errbuf()
     L.check(L.lib().cast_b200_set_device(local, eb, L.ERR_LEN), eb, "set_device")
+    if args.sharded or (ws > 1 and not args.replicas):
+        line = sharded_line(args, ws, rank, local, pg)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return 0
     prec = cu.CudaPrecision.F64 if args.precision == "f64" else cu.CudaPrecision.F32
     spec = cu.CudaKernelGenSpec.f64() if prec == cu.CudaPrecision.F64 else cu.CudaKernelGenSpec.f32()
     amp_bytes = 16 if prec == cu.CudaPrecision.F64 else 8

@@ -12,11 +12,17 @@ the same gate-application path:
   * **Local gates.** A gate whose physical targets are all below L runs on every
     rank's shard locally, through the device kernel (C ABI) on GPU ranks.
   * **Global targets.** Before a gate touches a global position P = L + b, that
-    position is swapped with a local position p the gate does not use (the
-    highest such). Rank r and its partner r ^ 2^b exchange the half of their
-    shards whose local bit p differs from their own bit b: a pairwise send/recv
-    of 2^(L-1) amplitudes, with no collective. The two positions then trade
-    logical qubits in ``perm``.
+    position is swapped with a local position p the gate does not use. Rank r
+    and its partner r ^ 2^b exchange the half of their shards whose local bit p
+    differs from their own bit b: 2^(L-1) amplitudes, with no collective, sent
+    in chunks through two fixed staging buffers (``chunk_amps`` amplitudes each,
+    allocated once), so an exchange needs no half-shard temporaries and the
+    shard can fill most of the device. The two positions then trade logical
+    qubits in ``perm``.
+  * **Which local position.** ``apply`` takes the highest free one.
+    ``apply_circuit`` looks ahead: it evicts the local position whose logical
+    qubit is next used furthest in the future (never, if possible) - Belady's
+    rule, which minimises the number of exchanges over the circuit.
   * **Reading out.** ``gather`` assembles the logical-order state on rank 0.
     ``expectation_z`` all-reduces per-position populations (FP64) and maps them
     back to logical qubits.
@@ -38,21 +44,36 @@ import numpy as np
 LocalApply = Callable[[object, np.ndarray, tuple], None]
 
 
-def swap_plan(targets_phys: tuple, n_local: int, in_use: set | None = None) -> list[tuple[int, int]]:
+def swap_plan(targets_phys: tuple, n_local: int, in_use: set | None = None,
+              priority: Callable[[int], float] | None = None) -> list[tuple[int, int]]:
     """(global position, local position) swaps that make every physical target
     local.
 
-    Each global target is paired with the highest local position that is neither
-    a target of this gate nor already chosen."""
+    Each global target is paired with a local position that is neither a target
+    of this gate nor already chosen: the one with the largest ``priority``
+    (ties, and no priority, go to the highest position)."""
     in_use = set(in_use or ()) | {q for q in targets_phys if q < n_local}
     plan = []
     for q in sorted(q for q in targets_phys if q >= n_local):
-        p = next((c for c in range(n_local - 1, -1, -1) if c not in in_use), None)
-        if p is None:
+        free = [c for c in range(n_local - 1, -1, -1) if c not in in_use]
+        if not free:
             raise ValueError("gate is wider than the local qubits of a shard")
+        p = max(free, key=priority) if priority else free[0]
         in_use.add(p)
         plan.append((q, p))
     return plan
+
+
+def next_uses(gates_qubits: list[tuple], n_qubits: int) -> list[dict]:
+    """For every gate index i, {logical qubit: index of its next use after i}
+    for the qubits used again later (others are absent: never used again)."""
+    out: list[dict] = [dict() for _ in gates_qubits]
+    upcoming: dict = {}
+    for i in range(len(gates_qubits) - 1, -1, -1):
+        out[i] = dict(upcoming)
+        for q in gates_qubits[i]:
+            upcoming[q] = i
+    return out
 
 
 def permute_bits(index: np.ndarray, perm: list[int]) -> np.ndarray:
@@ -72,7 +93,11 @@ class ShardedStatevector:
     a gate to the shard in place. On GPU ranks, ``cuda_apply_local`` runs the
     device kernels through the C ABI."""
 
-    def __init__(self, n_qubits: int, shard, apply_local: LocalApply, group=None):
+    def __init__(self, n_qubits: int, shard, apply_local: LocalApply, group=None,
+                 chunk_amps: int = 1 << 24):
+        """chunk_amps: amplitudes an exchange moves per send/recv (a power of
+        two; two staging buffers of this size are allocated on the shard's
+        device the first time an exchange runs)."""
         import torch.distributed as dist
 
         self.dist = dist
@@ -85,10 +110,15 @@ class ShardedStatevector:
         self.n, self.g, self.n_local = int(n_qubits), g, int(n_qubits) - g
         if self.n_local < 1 or shard.numel() != (1 << self.n_local):
             raise ValueError("shard must hold 2^(n - log2(world)) amplitudes")
+        if chunk_amps < 1 or chunk_amps & (chunk_amps - 1):
+            raise ValueError("chunk_amps must be a power of two")
         self.shard = shard
         self.apply_local = apply_local
         self.perm = list(range(self.n))  # logical -> physical position
         self.n_exchanges = 0
+        self.exchanged_amps = 0
+        self.chunk_amps = min(int(chunk_amps), max(1, 1 << (self.n_local - 1)))
+        self._stage = None  # (send, recv) staging buffers
 
     # -- state ------------------------------------------------------------------
     def set_zero(self) -> None:
@@ -101,11 +131,45 @@ class ShardedStatevector:
     def apply(self, matrix: np.ndarray, qubits) -> None:
         """Apply a gate given on logical qubits (in the order of the matrix's
         index bits)."""
+        self._apply(matrix, qubits, None)
+
+    def apply_circuit(self, gates) -> None:
+        """Apply gates (objects with ``matrix()`` and ``qubits()``, logical
+        qubits) in order, choosing the local position each exchange evicts by
+        look-ahead over the rest of the list."""
+        gates = list(gates)
+        nxt = next_uses([tuple(g.qubits()) for g in gates], self.n)
+        for i, g in enumerate(gates):
+            self._apply(g.matrix(), g.qubits(), nxt[i])
+
+    def _apply(self, matrix, qubits, next_use: dict | None) -> None:
         phys = tuple(self.perm[q] for q in qubits)
-        for gpos, lpos in swap_plan(phys, self.n_local):
+        prio = None
+        if next_use is not None:
+            at = {p: lq for lq, p in enumerate(self.perm)}  # physical -> logical
+            prio = lambda pos: next_use.get(at[pos], math.inf)  # noqa: E731
+        for gpos, lpos in swap_plan(phys, self.n_local, priority=prio):
             self._swap(gpos, lpos)
         phys = tuple(self.perm[q] for q in qubits)
         self.apply_local(self.shard, np.ascontiguousarray(matrix), phys)
+
+    def _blocks(self, lpos: int, half: int):
+        """The half of the shard whose local bit lpos is `half`, as views of at
+        most chunk_amps amplitudes each, in the order both partners walk them:
+        the shard is (rows, 2, run) with run = 2^lpos; a block is a slice of one
+        run, or whole runs of consecutive rows (a strided view)."""
+        run = 1 << lpos
+        rows = 1 << (self.n_local - lpos - 1)
+        c = self.chunk_amps
+        view = self.shard.view(rows, 2, run)
+        if run >= c:
+            for r in range(rows):
+                for off in range(0, run, c):
+                    yield view[r, half, off:off + c]
+        else:
+            per = c // run
+            for r0 in range(0, rows, per):
+                yield view[r0:r0 + per, half, :]
 
     def _swap(self, gpos: int, lpos: int) -> None:
         """Exchange global position gpos with local position lpos."""
@@ -114,15 +178,20 @@ class ShardedStatevector:
         b = gpos - self.n_local
         my_bit = (self.rank >> b) & 1
         partner = self.rank ^ (1 << b)
-        view = self.shard.view(1 << (self.n_local - lpos - 1), 2, 1 << lpos)
-        send = view[:, 1 - my_bit, :].contiguous()
-        recv = torch.empty_like(send)
-        # real views: not every backend transfers complex tensors
-        ops = [self.dist.P2POp(self.dist.isend, torch.view_as_real(send), partner, self.group),
-               self.dist.P2POp(self.dist.irecv, torch.view_as_real(recv), partner, self.group)]
-        for req in self.dist.batch_isend_irecv(ops):
-            req.wait()
-        view[:, 1 - my_bit, :] = recv
+        if self._stage is None:
+            self._stage = (torch.empty(self.chunk_amps, dtype=self.shard.dtype, device=self.shard.device),
+                           torch.empty(self.chunk_amps, dtype=self.shard.dtype, device=self.shard.device))
+        send, recv = self._stage
+        for blk in self._blocks(lpos, 1 - my_bit):
+            cnt = blk.numel()
+            send[:cnt].view(blk.shape).copy_(blk)
+            # real views: not every backend transfers complex tensors
+            ops = [self.dist.P2POp(self.dist.isend, torch.view_as_real(send[:cnt]), partner, self.group),
+                   self.dist.P2POp(self.dist.irecv, torch.view_as_real(recv[:cnt]), partner, self.group)]
+            for req in self.dist.batch_isend_irecv(ops):
+                req.wait()
+            blk.copy_(recv[:cnt].view(blk.shape))
+            self.exchanged_amps += cnt
         la = self.perm.index(gpos)
         lb = self.perm.index(lpos)
         self.perm[la], self.perm[lb] = lpos, gpos

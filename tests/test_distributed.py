@@ -1,6 +1,7 @@
-"""Sharded statevector with qubit-swap exchanges: the swap planner, the index
-permutation, and world-size 2 and 4 runs over gloo on CPU (one process per
-rank, the oracle as the local gate applier) against the oracle's unsharded run."""
+"""Sharded statevector with qubit-swap exchanges: the swap planner (greedy and
+look-ahead), the index permutation, and world-size 2 and 4 runs over gloo on
+CPU (one process per rank, the oracle as the local gate applier) against the
+oracle's unsharded run, with exchanges streamed through small staging chunks."""
 import os
 import socket
 
@@ -17,6 +18,18 @@ def test_swap_plan():
     assert D.swap_plan((6,), 6, in_use={5}) == [(6, 4)]
     with pytest.raises(ValueError, match="wider"):
         D.swap_plan((0, 1, 2), 2)
+
+
+def test_swap_plan_priority_and_next_uses():
+    # look-ahead: evict the local position whose logical qubit is used last
+    nxt = D.next_uses([(0, 1), (2,), (1, 5), (0,)], 6)
+    assert nxt[0] == {2: 1, 1: 2, 5: 2, 0: 3}
+    assert nxt[1] == {1: 2, 5: 2, 0: 3} and nxt[3] == {}
+    prio = {5: 1.0, 4: 7.0, 3: float("inf"), 2: 3.0, 1: 0.0, 0: 2.0}
+    assert D.swap_plan((6,), 6, priority=prio.get) == [(6, 3)]
+    assert D.swap_plan((6, 7), 6, priority=prio.get) == [(6, 3), (7, 4)]
+    # ties go to the highest position
+    assert D.swap_plan((6,), 6, priority=lambda p: 1.0) == [(6, 5)]
 
 
 def test_permute_bits():
@@ -44,7 +57,7 @@ def _circuit(n, seed):
     return gates
 
 
-def _worker(rank, world, port, n, seed, out_dir):
+def _worker(rank, world, port, n, seed, out_dir, chunk=1 << 24, lookahead=False):
     import sys
 
     import torch
@@ -65,27 +78,45 @@ def _worker(rank, world, port, n, seed, out_dir):
             O.apply_gate(shard.numpy(), mm, srt)  # in place on the shard's memory
 
         n_local = n - (world.bit_length() - 1)
-        sv = D.ShardedStatevector(n, torch.zeros(1 << n_local, dtype=torch.complex128), apply_local)
+        sv = D.ShardedStatevector(n, torch.zeros(1 << n_local, dtype=torch.complex128), apply_local,
+                                  chunk_amps=chunk)
         sv.set_zero()
-        for m, q in _circuit(n, seed):
-            sv.apply(m, q)
+        if lookahead:
+            class G:
+                def __init__(self, m, q):
+                    self._m, self._q = m, q
+
+                def matrix(self):
+                    return self._m
+
+                def qubits(self):
+                    return self._q
+
+            sv.apply_circuit([G(m, q) for m, q in _circuit(n, seed)])
+        else:
+            for m, q in _circuit(n, seed):
+                sv.apply(m, q)
         full = sv.gather()
         z = sv.expectation_z()
         if rank == 0:
             np.save(os.path.join(out_dir, "state.npy"), full)
             np.save(os.path.join(out_dir, "z.npy"), z)
-            np.save(os.path.join(out_dir, "ex.npy"), np.array([sv.n_exchanges]))
+            np.save(os.path.join(out_dir, "ex.npy"), np.array([sv.n_exchanges, sv.exchanged_amps]))
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 4])
-def test_sharded_matches_oracle(oracle, tmp_path, world):
+@pytest.mark.parametrize("world,chunk,lookahead", [(2, 1 << 24, False), (4, 1 << 24, False),
+                                                   (2, 4, False), (4, 2, True), (4, 16, True)])
+def test_sharded_matches_oracle(oracle, tmp_path, world, chunk, lookahead):
+    """Whole-half exchanges, exchanges streamed through staging chunks smaller
+    than one run and larger than one run, and the look-ahead planner: all give
+    the oracle's state and <Z>."""
     import torch.multiprocessing as mp
 
     n, seed = 8, 11 + world
-    mp.start_processes(_worker, args=(world, _free_port(), n, seed, str(tmp_path)), nprocs=world,
-                       join=True, start_method="spawn")
+    mp.start_processes(_worker, args=(world, _free_port(), n, seed, str(tmp_path), chunk, lookahead),
+                       nprocs=world, join=True, start_method="spawn")
     got = np.load(tmp_path / "state.npy")
     gates = []
     from cast_simulator_b200.types import _canonicalize
@@ -99,7 +130,45 @@ def test_sharded_matches_oracle(oracle, tmp_path, world):
     idx = np.arange(1 << n)
     z_ref = np.array([1 - 2 * p[(idx >> q) & 1 == 1].sum() for q in range(n)])
     assert np.max(np.abs(np.load(tmp_path / "z.npy") - z_ref)) < 1e-12
-    assert int(np.load(tmp_path / "ex.npy")[0]) > 0  # the circuit did cross shards
+    ex, amps = (int(x) for x in np.load(tmp_path / "ex.npy"))
+    assert ex > 0  # the circuit did cross shards
+    n_local = n - (world.bit_length() - 1)
+    assert amps == ex * (1 << (n_local - 1))  # each exchange moved half a shard
+
+
+def test_lookahead_needs_no_more_exchanges():
+    """Belady's rule on a host model of the planner: over random circuits the
+    look-ahead choice never makes more exchanges than the greedy one, and makes
+    fewer on most."""
+    rng = np.random.default_rng(3)
+    fewer = 0
+    for trial in range(30):
+        n, n_local = 12, 9
+        circ = []
+        for _ in range(120):
+            k = int(rng.integers(1, 4))
+            circ.append(tuple(int(x) for x in rng.choice(n, size=k, replace=False)))
+
+        def count(lookahead):
+            perm = list(range(n))
+            nxt = D.next_uses(circ, n)
+            swaps = 0
+            for i, qs in enumerate(circ):
+                phys = tuple(perm[q] for q in qs)
+                prio = None
+                if lookahead:
+                    at = {p: lq for lq, p in enumerate(perm)}
+                    prio = lambda pos, i=i, at=at: nxt[i].get(at[pos], float("inf"))  # noqa: E731
+                for g, l in D.swap_plan(phys, n_local, priority=prio):
+                    a, b = perm.index(g), perm.index(l)
+                    perm[a], perm[b] = l, g
+                    swaps += 1
+            return swaps
+
+        greedy, ahead = count(False), count(True)
+        assert ahead <= greedy
+        fewer += ahead < greedy
+    assert fewer >= 20
 
 
 def test_trajectory_range_partition():

@@ -36,3 +36,25 @@ def test_cuda_applier_single_rank(cblib, oracle):
         idx = np.arange(1 << n)
         z_ref = np.array([1 - 2 * p[(idx >> q) & 1 == 1].sum() for q in range(n)])
         assert np.max(np.abs(sv.expectation_z() - z_ref)) < tol
+
+
+def test_cuda_applier_apply_circuit_single_rank(cblib, oracle):
+    """apply_circuit (the look-ahead planner's entry point) through the device
+    kernels at world size 1: no exchanges, the oracle's state."""
+    import torch
+
+    from cast_simulator_b200 import distributed as D
+    from cast_simulator_b200.fusion import FusionConfig, optimize_native
+    from cast_simulator_b200.types import QuantumCircuit
+
+    n = 14
+    circ = QuantumCircuit.brickwork(n, 6, 9)
+    fused = optimize_native(n, circ.gates(), FusionConfig.size_only(4)).gates()
+    sv = D.ShardedStatevector(n, torch.zeros(1 << n, dtype=torch.complex128, device="cuda"),
+                              D.cuda_apply_local(1))
+    sv.set_zero()
+    sv.apply_circuit(fused)
+    torch.cuda.synchronize()
+    ref = oracle.simulate(n, [(g.matrix(), g.qubits()) for g in circ.gates()])
+    assert np.max(np.abs(sv.gather() - ref)) < 1e-10
+    assert sv.n_exchanges == 0
