@@ -559,10 +559,13 @@ def serving_leg(n_req: int, rates=(20.0, 80.0, 320.0)):
     256 trajectories; noisy circuits have at most 20 qubits, the trajectory
     kernel's range).  At each swept rate: p50/p99 latency and circuits/s of
       * the engine: continuous batching, small pure requests (<= 16 qubits) run
-        together in the circuit-batch kernel, the rest on worker streams;
+        together in the circuit-batch kernel, the rest on worker streams, complex64
+        requests of 20+ qubits as split-precision programs on the tensor cores;
       * the same engine with the circuit-batch kernel off;
-      * sequential execution: the same engine one request at a time
-        (max_slots = 1, no batching), measured on the same arrivals.
+      * sequential execution on the plain path: the same engine one request at a
+        time (max_slots = 1, no batching, no tensor cores), on the same arrivals.
+    Latency percentiles are also given per request class (pure <= 16 qubits,
+    pure 17..28, noisy).
     An unmeasured pass of the fastest stream warms each engine first (kernel
     module loads, first allocation of each pooled statevector size)."""
     from cast_simulator_b200 import serving as S
@@ -575,7 +578,7 @@ def serving_leg(n_req: int, rates=(20.0, 80.0, 320.0)):
            "rates": [{"rate_hz": r} for r in rates]}
     for label, kw in (("engine", {"max_slots": 8}),
                       ("engine_no_batch_kernel", {"max_slots": 8, "batch_max_qubits": 0}),
-                      ("sequential", {"max_slots": 1, "batch_max_qubits": 0})):
+                      ("sequential", {"max_slots": 1, "batch_max_qubits": 0, "split_min_qubits": 0})):
         eng = S.ServingEngine(**kw)
         try:
             eng.run_stream(stream(max(rates)))
@@ -588,6 +591,12 @@ def serving_leg(n_req: int, rates=(20.0, 80.0, 320.0)):
                 entry = {**S.latency_summary([r.latency for r in res]),
                          "circuits_per_s": n_req / wall, "max_concurrent": eng.max_concurrent,
                          "wall_s": wall}
+                classes = {"pure_small": [r.latency for r in res if not r.n_traj and r.n_qubits <= 16],
+                           "pure_large": [r.latency for r in res if not r.n_traj and r.n_qubits > 16],
+                           "noisy": [r.latency for r in res if r.n_traj]}
+                entry["by_class"] = {c: {"p50_ms": float(np.percentile(v, 50) * 1e3),
+                                         "p99_ms": float(np.percentile(v, 99) * 1e3), "n": len(v)}
+                                     for c, v in classes.items() if v}
                 if eng.batches_run > b0:
                     entry["batch_launches"] = eng.batches_run - b0
                     entry["batched_requests"] = eng.batched_requests - r0

@@ -108,9 +108,16 @@ class _SvPool:
 
 class ServingEngine:
     def __init__(self, max_slots: int = 8, mem_budget_bytes: int | None = None, fusion_k: int = 4,
-                 traj_fusion_k: int = 3, use_graph: bool = False, batch_max_qubits: int = 16,
-                 batch_fusion_k: int = 3, max_batch: int = 1024):
+                 traj_fusion_k: int | None = None, use_graph: bool = False,
+                 batch_max_qubits: int = 16, batch_fusion_k: int = 3, max_batch: int = 1024,
+                 split_min_qubits: int = 20):
         """max_slots: requests running at once on the worker streams.
+        traj_fusion_k: fusion width of noisy requests' trajectory programs (None:
+        3 up to 16 qubits, where the states sit in L1/L2 and the passes are bound
+        by instruction issue, 4 above, where fewer passes over HBM win).
+        split_min_qubits: complex64 pure requests of at least this many qubits
+        run as split-precision programs fused at k = 6 (dense 5- and 6-qubit
+        gates on the tensor cores, 1 - |<ref|psi>| ~ 1e-10; 0 turns it off).
         batch_max_qubits: pure requests of at most this many qubits run batched
         in the circuit-batch kernel (0 turns batching off); batch_fusion_k: their
         fusion width (<= 4); max_batch: circuits a batch launch takes at most
@@ -128,6 +135,7 @@ class ServingEngine:
         self.batch_max_qubits = batch_max_qubits
         self.batch_fusion_k = batch_fusion_k
         self.max_batch = max_batch
+        self.split_min_qubits = split_min_qubits
         self._bwork: collections.deque = collections.deque()
         self._bcv = threading.Condition()
         self._batched_active = 0
@@ -313,12 +321,16 @@ class ServingEngine:
     def _execute(self, req: Request, stream: Stream) -> np.ndarray:
         n = req.circuit.n_qubits()
         if req.n_traj:
-            prog = TrajectoryProgram(req.circuit, self.traj_fusion_k)
+            k = self.traj_fusion_k or (3 if n <= 16 else 4)
+            prog = TrajectoryProgram(req.circuit, k)
             z, _ = prog.run(req.n_traj, req.seed, stream, True)
             return z.mean(axis=0)
-        fused = optimize_native(n, req.circuit.gates(), FusionConfig.size_only(self.fusion_k))
+        split = (req.precision == CudaPrecision.F32 and self.split_min_qubits > 0
+                 and n >= self.split_min_qubits)
+        fused = optimize_native(n, req.circuit.gates(),
+                                FusionConfig.size_only(6 if split else self.fusion_k))
         tol = 1e-12 if req.precision == CudaPrecision.F64 else 1e-6
-        prog = GateProgram(req.precision, n, tol, tol)
+        prog = GateProgram(req.precision, n, tol, tol, split)
         eb = L.errbuf()
         L.check(L.lib().cast_b200_program_add_fused(prog.handle, fused.handle, eb, L.ERR_LEN), eb,
                 "program_add_fused")

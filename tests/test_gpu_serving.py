@@ -101,3 +101,25 @@ def test_failed_request_does_not_stop_the_engine(mods):
         assert fg.result().z.shape == (10,)
     finally:
         eng.shutdown()
+
+
+def test_large_complex64_requests_use_the_tensor_path(mods, oracle):
+    """A complex64 request of split_min_qubits or more runs as a split-precision
+    program (k = 6 on the tensor cores); its <Z_q> stays within the tensor
+    path's error of the oracle, and with the split turned off the engine gives
+    the plain path's result."""
+    cu, S, T = mods
+    n = 20
+    circ = T.QuantumCircuit.brickwork(n, 6, 77)
+    req = S.Request(circ, cu.CudaPrecision.F32, 0, 1, 0.0, 0)
+    sv = oracle.simulate(n, [(g.matrix(), g.qubits()) for g in circ.gates()])
+    p = np.abs(sv) ** 2
+    idx = np.arange(p.size)
+    z_ref = np.array([1 - 2 * p[(idx >> q) & 1 == 1].sum() for q in range(n)])
+    for split_min, tol in ((20, 1e-4), (0, 1e-5)):
+        eng = S.ServingEngine(max_slots=2, split_min_qubits=split_min)
+        try:
+            z = eng.submit(req).result().z
+        finally:
+            eng.shutdown()
+        assert np.max(np.abs(z - z_ref)) < tol, (split_min, np.max(np.abs(z - z_ref)))
