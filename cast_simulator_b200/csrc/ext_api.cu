@@ -227,7 +227,7 @@ int cast_b200_program_add_gate(void *program, const cast_complex64_t *matrix,
       if (cb2::sparse_gate(g)) ok = cb2::upload_sparse(g, err);  // CSR kernel, any precision mode
       else
         ok = (g.k < 6 || cb2::upload_gate_matrix(g, err)) &&
-             (!p->split || !cb2::tensor_path_supported(g) || cb2::prepare_tensor_gate(g, err));
+             (!p->split || !cb2::tensor_path_supported(g) || cb2::prepare_tensor_gate(g, p->n, err));
     }
     if (!ok) {
       cb2::free_gate_device(g);

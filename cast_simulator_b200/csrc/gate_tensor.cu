@@ -722,7 +722,8 @@ float bf16_value(uint16_t b) {
 }
 
 template <int K, typename Off, bool kStage>
-bool launch_um_k(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::string &err) {
+bool launch_um_k(const uint32_t *qubits, const void *d_tc, void *sv, uint32_t n, cudaStream_t s,
+                 std::string &err) {
   using C = UmCfg<K, kStage>;
   static std::once_flag once;
   static cudaError_t attr_rc = cudaSuccess;
@@ -740,7 +741,7 @@ bool launch_um_k(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::s
   if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(tensor gate kernel)", err)) return false;
   TcTargets t;
   for (uint32_t b = 0; b < kMaxGateQubits; ++b) {
-    const uint32_t q = b < g.k ? g.qubits[b] : 0;
+    const uint32_t q = b < (uint32_t)K ? qubits[b] : 0;
     t.lo_mask[b] = (1ull << q) - 1;
     t.stride[b] = 1ull << q;
   }
@@ -748,14 +749,15 @@ bool launch_um_k(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::s
   const uint64_t n_tiles = (n_groups + kTileGroups - 1) / kTileGroups;
   const unsigned grid = (unsigned)std::max<uint64_t>(
       1, std::min<uint64_t>(n_tiles, (uint64_t)blocks_per_sm * sm_count()));
-  const int quad = kStage && g.qubits[1] == 1;
+  const int quad = kStage && qubits[1] == 1;
   k_gate_umma<K, Off, kStage><<<grid, kUmThreads, C::SMEM, s>>>(
-      static_cast<float2 *>(sv), n_groups, t, static_cast<const uint4 *>(g.d_tc), quad);
+      static_cast<float2 *>(sv), n_groups, t, static_cast<const uint4 *>(d_tc), quad);
   return cuda_ok(cudaGetLastError(), "tensor gate kernel launch", err);
 }
 
 template <int K, typename Off>
-bool launch_ut_k(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::string &err) {
+bool launch_ut_k(const uint32_t *qubits, const void *d_tc, void *sv, uint32_t n, cudaStream_t s,
+                 std::string &err) {
   using C = UtCfg<K>;
   static std::once_flag once;
   static cudaError_t attr_rc = cudaSuccess;
@@ -766,15 +768,15 @@ bool launch_ut_k(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::s
   if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(tensor gate kernel, TMA)", err)) return false;
   TcTargets t;
   for (uint32_t b = 0; b < kMaxGateQubits; ++b) {
-    const uint32_t q = b < g.k ? g.qubits[b] : 0;
+    const uint32_t q = b < (uint32_t)K ? qubits[b] : 0;
     t.lo_mask[b] = (1ull << q) - 1;
     t.stride[b] = 1ull << q;
   }
   const uint64_t n_tiles = (1ull << (n - K)) / kTileGroups;
   const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(n_tiles, (uint64_t)sm_count()));
-  const int run_log2 = (int)std::min<uint32_t>(g.qubits[0], 7);
+  const int run_log2 = (int)std::min<uint32_t>(qubits[0], 7);
   k_gate_umma_tma<K, Off><<<grid, kTThreads, C::SMEM, s>>>(
-      static_cast<float2 *>(sv), 1ull << (n - K), t, static_cast<const uint4 *>(g.d_tc), run_log2);
+      static_cast<float2 *>(sv), 1ull << (n - K), t, static_cast<const uint4 *>(d_tc), run_log2);
   return cuda_ok(cudaGetLastError(), "tensor gate kernel launch (TMA)", err);
 }
 
@@ -787,19 +789,15 @@ bool tensor_path_supported(const GateData &g) {
 // Packs Mr (R x R, Mr[2r+c'][2m+c] as in the header) as the MMA's K-major
 // operand with the 128-byte swizzle: element (row, col) at byte
 // (col / 64) * R * 128 + row * 128 + (((col % 64) / 8 ^ row % 8) * 16) + (col % 8) * 2;
-// hi block first, then lo.
-bool prepare_tensor_gate(GateData &g, std::string &err) {
-  if (!tensor_path_supported(g)) {
-    err = "the tensor-core path takes complex64 gates with 5 or 6 qubits";
-    return false;
-  }
-  const int D = 1 << g.k, R = 2 * D;
+// hi block first, then lo.  m64 is the D x D matrix, interleaved re/im.
+std::vector<uint16_t> pack_tensor_operand(const double *m64, int k) {
+  const int D = 1 << k, R = 2 * D;
   const size_t per = (size_t)R * R;
   std::vector<uint16_t> packed(2 * per);
   for (int row = 0; row < R; ++row)
     for (int col = 0; col < R; ++col) {
       const int r = row >> 1, m = col >> 1;
-      const double a = g.m64[2 * ((size_t)r * D + m)], b = g.m64[2 * ((size_t)r * D + m) + 1];
+      const double a = m64[2 * ((size_t)r * D + m)], b = m64[2 * ((size_t)r * D + m) + 1];
       const bool out_im = row & 1, in_im = col & 1;
       const double v = out_im ? (in_im ? a : b) : (in_im ? -b : a);
       const uint16_t hi = bf16_bits_rn((float)v);
@@ -809,6 +807,57 @@ bool prepare_tensor_gate(GateData &g, std::string &err) {
       packed[byte / 2] = hi;
       packed[per + byte / 2] = lo;
     }
+  return packed;
+}
+
+// A 5-qubit gate runs on the 6-qubit kernel, padded with the identity on a spare
+// qubit: the tensor pass is bound by memory, not by the tensor pipe, and the
+// 6-qubit tile moves twice the bytes per tile handoff (measured at 30 qubits:
+// 4.3 ms for a 5-qubit pass, 3.6 ms for a 6-qubit one).  The spare qubit is the
+// lowest non-target >= 7 when there is one (a gate whose targets are all >= 7
+// stays eligible for the bulk-copy loaders), else the highest non-target.
+bool prepare_tensor_gate(GateData &g, uint32_t n, std::string &err) {
+  if (!tensor_path_supported(g)) {
+    err = "the tensor-core path takes complex64 gates with 5 or 6 qubits";
+    return false;
+  }
+  std::vector<uint16_t> packed;
+  g.tc_k = g.k;
+  for (uint32_t b = 0; b < g.k; ++b) g.tc_qubits[b] = g.qubits[b];
+  if (g.k == 5 && n > 5) {
+    uint32_t used = 0;
+    for (uint32_t b = 0; b < 5; ++b) used |= 1u << g.qubits[b];
+    int spare = -1;
+    for (uint32_t c = 7; c < n && spare < 0; ++c)
+      if (!((used >> c) & 1)) spare = (int)c;
+    for (int c = (int)n - 1; c >= 0 && spare < 0; --c)
+      if (!((used >> c) & 1)) spare = c;
+    uint32_t q6[6], j = 0, pos = 0;
+    for (uint32_t b = 0, i = 0; b < 6; ++b) {
+      if (j == 0 && (i == 5 || (uint32_t)spare < g.qubits[i])) {
+        q6[b] = (uint32_t)spare;
+        pos = b;
+        j = 1;
+      } else {
+        q6[b] = g.qubits[i++];
+      }
+    }
+    // M6[r][c] = M5[r without bit pos][c without bit pos] when bit pos of r and c agree, else 0
+    std::vector<double> m6(2 * 64 * 64, 0.0);
+    auto drop = [&](uint32_t x) { return ((x >> (pos + 1)) << pos) | (x & ((1u << pos) - 1)); };
+    for (uint32_t r = 0; r < 64; ++r)
+      for (uint32_t c = 0; c < 64; ++c)
+        if (((r >> pos) & 1) == ((c >> pos) & 1)) {
+          const size_t src = 2 * ((size_t)drop(r) * 32 + drop(c)), dst = 2 * ((size_t)r * 64 + c);
+          m6[dst] = g.m64[src];
+          m6[dst + 1] = g.m64[src + 1];
+        }
+    packed = pack_tensor_operand(m6.data(), 6);
+    g.tc_k = 6;
+    for (uint32_t b = 0; b < 6; ++b) g.tc_qubits[b] = q6[b];
+  } else {
+    packed = pack_tensor_operand(g.m64.data(), (int)g.k);
+  }
   if (g.d_tc) cudaFree(g.d_tc);
   g.d_tc = nullptr;
   if (!cuda_ok(cudaMalloc(&g.d_tc, packed.size() * 2), "cudaMalloc (tensor gate operand)", err))
@@ -818,29 +867,30 @@ bool prepare_tensor_gate(GateData &g, std::string &err) {
 }
 
 bool launch_gate_tensor(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::string &err) {
-  if (!g.d_tc || !tensor_path_supported(g)) {
-    err = "gate has no tensor-core operand";
+  if (!g.d_tc || !tensor_path_supported(g) || (g.tc_k != 5 && g.tc_k != 6) || n < g.tc_k) {
+    err = "gate has no tensor-core operand for this statevector";
     return false;
   }
+  const uint32_t *q = g.tc_qubits;
+  const void *op = g.d_tc;
   // member offsets are below 2^n amplitudes: 32-bit while n <= 32
-  const bool narrow = n <= 32, stage = g.qubits[0] == 0;
+  const bool narrow = n <= 32, stage = q[0] == 0;
   // lowest target >= 7 and whole tiles: every member's 128 groups are one 1 KB
   // run, fetched with one TMA bulk copy (shorter runs measured slower with TMA
   // than with register loads: 256-byte copies ran at 2.0 TB/s for k = 6)
-  // (k = 6 only: for k = 5 the register loaders measured faster, 4.08 vs 4.40 ms
-  // at 30 qubits)
-  if (g.k == 6 && g.qubits[0] >= 7 && n >= g.k + 7 && tma_enabled())
-    return narrow ? launch_ut_k<6, uint32_t>(g, sv, n, s, err) : launch_ut_k<6, uint64_t>(g, sv, n, s, err);
-  if (g.k == 5) {
-    if (narrow) return stage ? launch_um_k<5, uint32_t, true>(g, sv, n, s, err)
-                             : launch_um_k<5, uint32_t, false>(g, sv, n, s, err);
-    return stage ? launch_um_k<5, uint64_t, true>(g, sv, n, s, err)
-                 : launch_um_k<5, uint64_t, false>(g, sv, n, s, err);
+  if (g.tc_k == 6 && q[0] >= 7 && n >= 6 + 7 && tma_enabled())
+    return narrow ? launch_ut_k<6, uint32_t>(q, op, sv, n, s, err)
+                  : launch_ut_k<6, uint64_t>(q, op, sv, n, s, err);
+  if (g.tc_k == 5) {
+    if (narrow) return stage ? launch_um_k<5, uint32_t, true>(q, op, sv, n, s, err)
+                             : launch_um_k<5, uint32_t, false>(q, op, sv, n, s, err);
+    return stage ? launch_um_k<5, uint64_t, true>(q, op, sv, n, s, err)
+                 : launch_um_k<5, uint64_t, false>(q, op, sv, n, s, err);
   }
-  if (narrow) return stage ? launch_um_k<6, uint32_t, true>(g, sv, n, s, err)
-                           : launch_um_k<6, uint32_t, false>(g, sv, n, s, err);
-  return stage ? launch_um_k<6, uint64_t, true>(g, sv, n, s, err)
-               : launch_um_k<6, uint64_t, false>(g, sv, n, s, err);
+  if (narrow) return stage ? launch_um_k<6, uint32_t, true>(q, op, sv, n, s, err)
+                           : launch_um_k<6, uint32_t, false>(q, op, sv, n, s, err);
+  return stage ? launch_um_k<6, uint64_t, true>(q, op, sv, n, s, err)
+               : launch_um_k<6, uint64_t, false>(q, op, sv, n, s, err);
 }
 
 int set_tensor_loader(int mode) { return g_tensor_loader.exchange(mode); }

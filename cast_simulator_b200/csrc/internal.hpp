@@ -23,6 +23,8 @@ struct GateData {
   std::vector<float> m32;
   void *d_mat = nullptr;  // device copy in the gate's precision (owned by the holder)
   void *d_tc = nullptr;   // split-BF16 tensor-core gate operand (owned by the holder), if any
+  uint32_t tc_k = 0;      // qubits of the tensor-core operand (a 5-qubit gate is padded to 6)
+  uint32_t tc_qubits[kMaxGateQubits] = {0};
   void *d_sparse = nullptr;  // CSR copy for the sparse kernel (owned by the holder), if any
 };
 
@@ -85,7 +87,8 @@ void snap_matrix(GateData &g, const double *interleaved, double ztol, double oto
 // BF16.  prepare_tensor_gate uploads g.d_tc; launch_gate runs the tensor kernel
 // for gates that have it.
 bool tensor_path_supported(const GateData &g);
-bool prepare_tensor_gate(GateData &g, std::string &err);
+// n: qubits of the statevectors the gate will run on (a spare qubit for padding).
+bool prepare_tensor_gate(GateData &g, uint32_t n, std::string &err);
 bool launch_gate_tensor(const GateData &g, void *sv, uint32_t n, cudaStream_t s, std::string &err);
 // Reads and clears the tensor kernel's error word (nonzero: a bounded wait expired).
 bool tensor_error_status(uint32_t *out, std::string &err);

@@ -110,7 +110,8 @@ class ServingEngine:
     def __init__(self, max_slots: int = 8, mem_budget_bytes: int | None = None, fusion_k: int = 4,
                  traj_fusion_k: int | None = None, use_graph: bool = False,
                  batch_max_qubits: int = 16, batch_fusion_k: int = 3, max_batch: int = 1024,
-                 split_min_qubits: int = 20):
+                 split_min_qubits: int = 20, heavy_slots: int = 1, heavy_pure_qubits: int = 22,
+                 heavy_noisy_qubits: int = 17):
         """max_slots: requests running at once on the worker streams.
         traj_fusion_k: fusion width of noisy requests' trajectory programs (None:
         3 up to 16 qubits, where the states sit in L1/L2 and the passes are bound
@@ -118,6 +119,11 @@ class ServingEngine:
         split_min_qubits: complex64 pure requests of at least this many qubits
         run as split-precision programs fused at k = 6 (dense 5- and 6-qubit
         gates on the tensor cores, 1 - |<ref|psi>| ~ 1e-10; 0 turns it off).
+        heavy_slots: requests that fill the GPU by themselves (pure requests of
+        heavy_pure_qubits or more qubits, noisy ones of heavy_noisy_qubits or
+        more) run at most this many at a time: two of them running together only
+        interleave, and each finishes later than if they ran one after the other,
+        while small requests still overlap with them.
         batch_max_qubits: pure requests of at most this many qubits run batched
         in the circuit-batch kernel (0 turns batching off); batch_fusion_k: their
         fusion width (<= 4); max_batch: circuits a batch launch takes at most
@@ -136,6 +142,10 @@ class ServingEngine:
         self.batch_fusion_k = batch_fusion_k
         self.max_batch = max_batch
         self.split_min_qubits = split_min_qubits
+        self.heavy_slots = heavy_slots
+        self.heavy_pure_qubits = heavy_pure_qubits
+        self.heavy_noisy_qubits = heavy_noisy_qubits
+        self._heavy_active = 0
         self._bwork: collections.deque = collections.deque()
         self._bcv = threading.Condition()
         self._batched_active = 0
@@ -222,6 +232,7 @@ class ServingEngine:
                     self._batched_active += 1
                 else:
                     self._active += 1
+                    self._heavy_active += int(self._heavy(req))
                 self.max_concurrent = max(self.max_concurrent, self._active + self._batched_active)
             if batched:
                 with self._bcv:
@@ -235,13 +246,20 @@ class ServingEngine:
     def _batchable(self, req: Request) -> bool:
         return not req.n_traj and req.circuit.n_qubits() <= self.batch_max_qubits
 
+    def _heavy(self, req: Request) -> bool:
+        n = req.circuit.n_qubits()
+        return n >= (self.heavy_noisy_qubits if req.n_traj else self.heavy_pure_qubits)
+
     def _can_admit_head(self) -> bool:
         if not self._pending:
             return False
-        if self._batchable(self._pending[0][0]):
+        head = self._pending[0][0]
+        if self._batchable(head):
             if self._batched_active >= self.max_batch:
                 return False
         elif self._active >= self.max_slots:
+            return False
+        elif self._heavy(head) and self._heavy_active >= self.heavy_slots:
             return False
         need = request_bytes(self._pending[0][0])
         if self._in_use + need > self.budget:
@@ -270,6 +288,7 @@ class ServingEngine:
                 with self._cv:
                     self._in_use -= need
                     self._active -= 1
+                    self._heavy_active -= int(self._heavy(req))
                     self._cv.notify_all()
 
     def _batch_loop(self) -> None:

@@ -39,6 +39,11 @@ def _cases(rng, k):
     # lowest target 5, 7 and 9: register loads, then the TMA-fed kernel (1 KB runs)
     out += [(n, tuple([5] + list(range(n - k + 1, n)))), (n, tuple(range(7, 7 + k))),
             (n, tuple(range(9, 9 + k)))]
+    if k == 5:
+        # a 5-qubit gate runs padded to 6 qubits with the identity on a spare qubit:
+        # no spare >= 7 (the highest free qubit is used), and the padded gate
+        # filling the whole statevector
+        out += [(10, (2, 6, 7, 8, 9)), (6, (0, 1, 2, 3, 4)), (6, (1, 2, 3, 4, 5))]
     return out
 
 

@@ -241,3 +241,17 @@ def test_small_requests_run_batched(monkeypatch):
         assert eng._in_use == 0 and eng._batched_active == 0
     finally:
         eng.shutdown()
+
+
+def test_heavy_requests_run_one_at_a_time(fake_engine):
+    """Requests that fill the GPU (here pure requests of 22+ qubits) never run
+    together when heavy_slots = 1; small ones still overlap with them."""
+    make, state = fake_engine
+    eng = make(max_slots=4, mem_budget_bytes=1 << 50, heavy_slots=1, heavy_pure_qubits=14)
+    reqs = [S.Request(QuantumCircuit.brickwork(15 if i % 2 == 0 else 10, 2, 1), CudaPrecision.F64,
+                      0, i, 0.0, i) for i in range(8)]
+    for f in [eng.submit(r) for r in reqs]:
+        f.result(timeout=30)
+    assert eng._heavy_active == 0 and eng._active == 0
+    # every other request is heavy: at most one heavy plus the small ones ran at once
+    assert state["peak"] <= 2
