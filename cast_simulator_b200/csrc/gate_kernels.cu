@@ -191,10 +191,15 @@ __device__ __forceinline__ uint32_t swz(uint32_t i) {
   return i ^ ((i >> LOGE) & ((1u << LOGE) - 1));
 }
 
-// Amplitudes per tile: 4096 for k = 3, 2048 otherwise (measured at 30 qubits with
-// targets 0..k-1: k = 3 runs at 6.9 instead of 6.1 TB/s (FP64) with the larger
-// tile, k = 2 and 4 lose with it).
-constexpr uint32_t tile_bits(uint32_t k) { return k == 3 ? 12u : 11u; }
+// Amplitudes per tile.  FP64: 4096 for k = 3, 2048 otherwise (measured at 30
+// qubits with targets 0..k-1: k = 3 runs at 6.9 instead of 6.1 TB/s with the
+// larger tile, k = 2 and 4 lose with it).  FP32: 4096 from k = 3.  A CTA holds
+// one tile and the k = 4 kernel's registers allow four CTAs a SM, so the tile
+// size sets the bytes in flight: 2048 FP32 amplitudes (16 KB) gave 64 KB a SM
+// and 3.8 TB/s under ncu at 26 qubits, against 128 KB for the FP64 tile.
+template <typename T> constexpr uint32_t tile_bits(uint32_t k) {
+  return k == 3 || (sizeof(T) == 4 && k >= 3) ? 12u : 11u;
+}
 
 template <typename T, int K>
 __global__ void __launch_bounds__(TileThreads<K>::N) k_gate_tile(T *__restrict__ sv, TileArgs a,
@@ -202,7 +207,7 @@ __global__ void __launch_bounds__(TileThreads<K>::N) k_gate_tile(T *__restrict__
   constexpr int kTileThreads = TileThreads<K>::N;
   using V = typename Vec2<T>::type;
   constexpr int D = 1 << K;
-  constexpr uint32_t TILE = 1u << tile_bits(K);
+  constexpr uint32_t TILE = 1u << tile_bits<T>(K);
   constexpr int LOGE = sizeof(V) == 16 ? 3 : 4;  // elements per 128-byte block
   // groups per thread, fully unrolled (a runtime loop would let the compiler
   // hoist the matrix out of the constant bank into registers)
@@ -744,11 +749,11 @@ bool launch_tile(const GateData &g, void *sv, uint32_t n, const TileArgs &a, cud
   static cudaError_t attr_rc = cudaSuccess;
   std::call_once(once, [] {
     attr_rc = cudaFuncSetAttribute(k_gate_tile<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(sizeof(V) << tile_bits(K)));
+                                   (int)(sizeof(V) << tile_bits<T>(K)));
   });
   if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(tile gate kernel)", err)) return false;
-  const uint64_t n_tiles = 1ull << (n - tile_bits(K));
-  const size_t smem = sizeof(V) << tile_bits(K);
+  const uint64_t n_tiles = 1ull << (n - tile_bits<T>(K));
+  const size_t smem = sizeof(V) << tile_bits<T>(K);
   MatParam<T, K> scratch;
   const MatParam<T, K> *mp = mat_param<T, K>(g, scratch);
   T *p = static_cast<T *>(sv);
@@ -822,7 +827,7 @@ bool tile_chosen(const GateData &g, uint32_t n, TileArgs &a) {
   if (ov != 2 && !tile_wins) return false;
   if (ov == 2 && low_bits == 0) return false;
   std::memset(&a, 0, sizeof(a));
-  return tile_geometry(g, n, a, tile_bits(g.k));
+  return tile_geometry(g, n, a, g.precision == 1 ? tile_bits<double>(g.k) : tile_bits<float>(g.k));
 }
 
 template <typename T>

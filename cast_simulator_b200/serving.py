@@ -121,9 +121,11 @@ class ServingEngine:
         gates on the tensor cores, 1 - |<ref|psi>| ~ 1e-10; 0 turns it off).
         heavy_slots: requests that fill the GPU by themselves (pure requests of
         heavy_pure_qubits or more qubits, noisy ones of heavy_noisy_qubits or
-        more) run at most this many at a time: two of them running together only
-        interleave, and each finishes later than if they ran one after the other,
-        while small requests still overlap with them.
+        more) execute on the GPU at most this many at a time: two of them running
+        together only interleave, and each finishes later than if they ran one
+        after the other.  Only the device phase waits: a heavy request is
+        admitted as usual and fuses and builds its program while another one
+        runs, and small requests still overlap with it.
         batch_max_qubits: pure requests of at most this many qubits run batched
         in the circuit-batch kernel (0 turns batching off); batch_fusion_k: their
         fusion width (<= 4); max_batch: circuits a batch launch takes at most
@@ -145,7 +147,7 @@ class ServingEngine:
         self.heavy_slots = heavy_slots
         self.heavy_pure_qubits = heavy_pure_qubits
         self.heavy_noisy_qubits = heavy_noisy_qubits
-        self._heavy_active = 0
+        self._gpu_heavy = threading.Semaphore(max(1, heavy_slots))
         self._bwork: collections.deque = collections.deque()
         self._bcv = threading.Condition()
         self._batched_active = 0
@@ -232,7 +234,6 @@ class ServingEngine:
                     self._batched_active += 1
                 else:
                     self._active += 1
-                    self._heavy_active += int(self._heavy(req))
                 self.max_concurrent = max(self.max_concurrent, self._active + self._batched_active)
             if batched:
                 with self._bcv:
@@ -258,8 +259,6 @@ class ServingEngine:
             if self._batched_active >= self.max_batch:
                 return False
         elif self._active >= self.max_slots:
-            return False
-        elif self._heavy(head) and self._heavy_active >= self.heavy_slots:
             return False
         need = request_bytes(self._pending[0][0])
         if self._in_use + need > self.budget:
@@ -288,7 +287,6 @@ class ServingEngine:
                 with self._cv:
                     self._in_use -= need
                     self._active -= 1
-                    self._heavy_active -= int(self._heavy(req))
                     self._cv.notify_all()
 
     def _batch_loop(self) -> None:
@@ -338,12 +336,20 @@ class ServingEngine:
                     self._cv.notify_all()
 
     def _execute(self, req: Request, stream: Stream) -> np.ndarray:
+        """Host preparation, then the device phase (behind the heavy-request
+        semaphore for requests that fill the GPU)."""
+        prep = self._prepare(req)
+        if self._heavy(req):
+            with self._gpu_heavy:
+                return self._launch(req, prep, stream)
+        return self._launch(req, prep, stream)
+
+    def _prepare(self, req: Request):
+        """Fusion and program construction on the host: a trajectory program
+        for a noisy request, a gate program for a pure one."""
         n = req.circuit.n_qubits()
         if req.n_traj:
-            k = self.traj_fusion_k or (3 if n <= 16 else 4)
-            prog = TrajectoryProgram(req.circuit, k)
-            z, _ = prog.run(req.n_traj, req.seed, stream, True)
-            return z.mean(axis=0)
+            return TrajectoryProgram(req.circuit, self.traj_fusion_k or (3 if n <= 16 else 4))
         split = (req.precision == CudaPrecision.F32 and self.split_min_qubits > 0
                  and n >= self.split_min_qubits)
         fused = optimize_native(n, req.circuit.gates(),
@@ -353,6 +359,14 @@ class ServingEngine:
         eb = L.errbuf()
         L.check(L.lib().cast_b200_program_add_fused(prog.handle, fused.handle, eb, L.ERR_LEN), eb,
                 "program_add_fused")
+        return prog
+
+    def _launch(self, req: Request, prog, stream: Stream) -> np.ndarray:
+        """Runs a prepared request on `stream` and returns its <Z_q>."""
+        n = req.circuit.n_qubits()
+        if req.n_traj:
+            z, _ = prog.run(req.n_traj, req.seed, stream, True)
+            return z.mean(axis=0)
         sv = self._pool.get(n, req.precision)
         ok = False
         try:

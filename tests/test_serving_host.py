@@ -243,15 +243,52 @@ def test_small_requests_run_batched(monkeypatch):
         eng.shutdown()
 
 
-def test_heavy_requests_run_one_at_a_time(fake_engine):
-    """Requests that fill the GPU (here pure requests of 22+ qubits) never run
-    together when heavy_slots = 1; small ones still overlap with them."""
-    make, state = fake_engine
-    eng = make(max_slots=4, mem_budget_bytes=1 << 50, heavy_slots=1, heavy_pure_qubits=14)
-    reqs = [S.Request(QuantumCircuit.brickwork(15 if i % 2 == 0 else 10, 2, 1), CudaPrecision.F64,
-                      0, i, 0.0, i) for i in range(8)]
-    for f in [eng.submit(r) for r in reqs]:
-        f.result(timeout=30)
-    assert eng._heavy_active == 0 and eng._active == 0
-    # every other request is heavy: at most one heavy plus the small ones ran at once
-    assert state["peak"] <= 2
+def test_heavy_requests_run_one_at_a_time_on_the_device(monkeypatch):
+    """Requests that fill the GPU (here pure requests of 14+ qubits) never run
+    their device phase together when heavy_slots = 1, but they are admitted and
+    prepared meanwhile, and small requests overlap with them."""
+    import threading
+    import time
+
+    st = {"heavy": 0, "heavy_peak": 0, "all": 0, "all_peak": 0, "prepared_while_heavy": 0,
+          "lock": threading.Lock()}
+
+    def prepare(self, req):
+        with st["lock"]:
+            if st["heavy"]:
+                st["prepared_while_heavy"] += 1
+        return None
+
+    def launch(self, req, prep, stream):
+        heavy = req.circuit.n_qubits() >= 14
+        with st["lock"]:
+            st["all"] += 1
+            st["all_peak"] = max(st["all_peak"], st["all"])
+            if heavy:
+                st["heavy"] += 1
+                st["heavy_peak"] = max(st["heavy_peak"], st["heavy"])
+        try:
+            time.sleep(0.03)
+            return np.zeros(req.circuit.n_qubits())
+        finally:
+            with st["lock"]:
+                st["all"] -= 1
+                if heavy:
+                    st["heavy"] -= 1
+
+    monkeypatch.setattr(S, "Stream", _FakeStream)
+    monkeypatch.setattr(S.ServingEngine, "_prepare", prepare)
+    monkeypatch.setattr(S.ServingEngine, "_launch", launch)
+    eng = S.ServingEngine(max_slots=6, mem_budget_bytes=1 << 50, batch_max_qubits=0, heavy_slots=1,
+                          heavy_pure_qubits=14)
+    try:
+        reqs = [S.Request(QuantumCircuit.brickwork(15 if i % 2 == 0 else 10, 2, 1), CudaPrecision.F64,
+                          0, i, 0.0, i) for i in range(12)]
+        for f in [eng.submit(r) for r in reqs]:
+            f.result(timeout=30)
+        assert st["heavy_peak"] == 1  # heavy device phases never overlapped
+        assert st["all_peak"] >= 2  # small requests ran beside a heavy one
+        assert st["prepared_while_heavy"] >= 1  # requests were prepared meanwhile
+        assert eng._active == 0 and eng._in_use == 0
+    finally:
+        eng.shutdown()
