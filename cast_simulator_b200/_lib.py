@@ -104,6 +104,7 @@ FFI_CUDA = [
 CAST_B200 = [
     ("cast_b200_set_device", C.c_int, [C.c_int, C.c_char_p, C.c_size_t]),
     ("cast_b200_stream_create_nonblocking", C.c_void_p, [C.c_char_p, C.c_size_t]),
+    ("cast_b200_stream_create_priority", C.c_void_p, [C.c_int, C.c_char_p, C.c_size_t]),
     ("cast_b200_sv_zero_async", C.c_int,
      [C.c_uint64, C.c_size_t, C.c_uint8, C.c_void_p, C.c_char_p, C.c_size_t]),
     ("cast_b200_set_gate_path", C.c_int, [C.c_int]),

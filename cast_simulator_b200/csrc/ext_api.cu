@@ -3,6 +3,8 @@
 #include "../../include/cast_b200.h"
 #include "internal.hpp"
 
+#include <algorithm>
+
 #include <exception>
 #include <map>
 #include <mutex>
@@ -89,6 +91,26 @@ void *cast_b200_stream_create_nonblocking(char *err_buf, size_t err_buf_len) {
   std::string err;
   cudaStream_t s = nullptr;
   if (!cuda_ok(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate", err)) {
+    write_err(err_buf, err_buf_len, err);
+    return nullptr;
+  }
+  clear_err(err_buf, err_buf_len);
+  return s;
+}
+
+void *cast_b200_stream_create_priority(int priority, char *err_buf, size_t err_buf_len) {
+  std::string err;
+  int least = 0, greatest = 0;
+  cudaStream_t s = nullptr;
+  if (!cuda_ok(cudaDeviceGetStreamPriorityRange(&least, &greatest), "cudaDeviceGetStreamPriorityRange",
+               err)) {
+    write_err(err_buf, err_buf_len, err);
+    return nullptr;
+  }
+  // numerically lower is more urgent; clamp into the device's range
+  const int p = std::min(std::max(priority, greatest), least);
+  if (!cuda_ok(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, p),
+               "cudaStreamCreateWithPriority", err)) {
     write_err(err_buf, err_buf_len, err);
     return nullptr;
   }

@@ -191,15 +191,11 @@ __device__ __forceinline__ uint32_t swz(uint32_t i) {
   return i ^ ((i >> LOGE) & ((1u << LOGE) - 1));
 }
 
-// Amplitudes per tile.  FP64: 4096 for k = 3, 2048 otherwise (measured at 30
-// qubits with targets 0..k-1: k = 3 runs at 6.9 instead of 6.1 TB/s with the
-// larger tile, k = 2 and 4 lose with it).  FP32: 4096 from k = 3.  A CTA holds
-// one tile and the k = 4 kernel's registers allow four CTAs a SM, so the tile
-// size sets the bytes in flight: 2048 FP32 amplitudes (16 KB) gave 64 KB a SM
-// and 3.8 TB/s under ncu at 26 qubits, against 128 KB for the FP64 tile.
-template <typename T> constexpr uint32_t tile_bits(uint32_t k) {
-  return k == 3 || (sizeof(T) == 4 && k >= 3) ? 12u : 11u;
-}
+// Amplitudes per tile: 4096 for k = 3, 2048 otherwise (measured at 30 qubits with
+// targets 0..k-1: k = 3 runs at 6.9 instead of 6.1 TB/s (FP64) with the larger
+// tile, k = 2 and 4 lose with it; FP32 k = 4 with 4096-amplitude tiles, 32 KB and
+// five CTAs a SM: 275 us under ncu at 26 qubits against 269 us with 2048).
+template <typename T> constexpr uint32_t tile_bits(uint32_t k) { return k == 3 ? 12u : 11u; }
 
 template <typename T, int K>
 __global__ void __launch_bounds__(TileThreads<K>::N) k_gate_tile(T *__restrict__ sv, TileArgs a,

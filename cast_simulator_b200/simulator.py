@@ -32,8 +32,15 @@ class Stream:
     invalidated by other threads' stream-0 work); ``blocking=True`` gives the
     reference's CU_STREAM_DEFAULT kind (cast_cuda_stream_create)."""
 
-    def __init__(self, blocking: bool = False):
+    def __init__(self, blocking: bool = False, priority: int | None = None):
+        """priority: a non-blocking stream with this scheduling priority (lower is
+        more urgent, clamped into the device's range; see
+        cast_b200_stream_create_priority)."""
         eb = L.errbuf()
+        if priority is not None:
+            self.handle = L.check_ptr(L.lib().cast_b200_stream_create_priority(int(priority), eb,
+                                                                               L.ERR_LEN), eb, "stream")
+            return
         fn = L.lib().cast_cuda_stream_create if blocking else L.lib().cast_b200_stream_create_nonblocking
         self.handle = L.check_ptr(fn(eb, L.ERR_LEN), eb, "stream")
 

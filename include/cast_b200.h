@@ -35,6 +35,12 @@ int cast_b200_set_device(int device, char *err_buf, size_t err_buf_len);
  * and cast_cuda_sv_zero (src/cpp/cuda/cuda_exec.cpp:268-279, 452-479) are the
  * blocking / host-synchronous forms. */
 void *cast_b200_stream_create_nonblocking(char *err_buf, size_t err_buf_len);
+/* A non-blocking stream with a scheduling priority (no counterpart in the
+ * reference): numerically lower is more urgent, clamped into the device's range
+ * (cudaDeviceGetStreamPriorityRange: 0 is the default, negative values are more
+ * urgent).  When several streams have work waiting, thread blocks of the more
+ * urgent stream's kernels start first as SMs free up. */
+void *cast_b200_stream_create_priority(int priority, char *err_buf, size_t err_buf_len);
 int cast_b200_sv_zero_async(uint64_t dptr, size_t n_elements, uint8_t precision, void *stream,
                             char *err_buf, size_t err_buf_len);
 
