@@ -372,7 +372,10 @@ def largest_leg(threads: int, depth: int = 10, n64: int = 34, n128: int = 33, n_
         amp = 8 if label == "c64" else 16
         for name, circ in (("brickwork", QuantumCircuit.brickwork(n, depth, 2024)),
                            ("qft-cx", QuantumCircuit.qft_cx(n))):
-            variants = [(4, False)] + ([(5, True), (6, True)] if label == "c64" else [])
+            # complex64: the split-precision tensor path at k = 5, 6; complex128: the
+            # QFT-CX fused at k = 6 runs its sparse blocks on the CSR kernels
+            variants = [(4, False)] + ([(5, True), (6, True)] if label == "c64" else
+                                       [(6, False)] if name == "qft-cx" else [])
             base = None
             for k, split in variants:
                 fused = optimize_native(n, circ.gates(), FusionConfig.size_only(k)).gates()

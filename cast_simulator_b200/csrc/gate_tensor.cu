@@ -67,9 +67,7 @@ constexpr uint32_t kErrLoaderWait = 1, kErrMmaFullWait = 2, kErrMmaAccWait = 4,
 
 __device__ uint32_t g_umma_error;
 
-// 0 auto (TMA-fed with the gate in tensor memory where eligible), 1 register
-// loaders everywhere, 2 TMA-fed with the gate in shared memory where eligible
-std::atomic<int> g_tensor_loader{0};
+std::atomic<int> g_tensor_loader{0};  // 0 auto, 1 register loaders, 2 TMA where eligible
 bool tma_enabled() { return g_tensor_loader.load() != 1; }
 
 template <int K, bool kStage> struct UmCfg {
@@ -709,309 +707,6 @@ __global__ void __launch_bounds__(kTThreads, 1)
   }
 }
 
-// ---- TMA-fed, gate in tensor memory (k = 6) --------------------------------------
-// The TMA-fed kernel above is bound by the raw tile bytes it keeps in flight, and
-// its shared memory is full: 64 KB of gate, two operand stages, three raw slots.
-// Here the split gate lives in tensor memory as the MMA's A operand, and the GEMM
-// is issued the other way round,
-//
-//     D^T (R x 128)  =  Mr (R x R) . X (R x 128 groups),
-//
-// so the output reals are the MMA's M = 128 rows (TMEM lanes) and the tile's 128
-// groups its N columns.  The operand stages (X as the K-major B operand) keep the
-// converters' layout unchanged, and the freed 64 KB hold two more raw slots: five,
-// 160 KB of loads in flight per SM.  Tensor memory: accumulators at columns 0 and
-// 128, the gate's hi rows at 256 and lo rows at 320 (R rows x R BF16 = 64 columns
-// each, two BF16 a column, even K index in the low half).
-// Warps:
-//   0-7   epilogue: warp w reads TMEM sub-partition w % 4 (reals 32 (w % 4) ..
-//         +31, i.e. 16 members, re and im on adjacent lanes) and half w / 4 of the
-//         columns (64 groups); adjacent lanes swap halves with one shuffle, so each
-//         lane holds (re, im) of one member for 16 consecutive groups and writes
-//         them as 8 16-byte stores.  At start warps 0-3 write the gate rows of their
-//         sub-partition into tensor memory;
-//   8-15  converters, 16 producer, 17 MMA issue: as in the kernel above.
-template <int K> struct UttCfg {
-  static constexpr int D = 1 << K;
-  static constexpr int R = 2 * D;                          // output reals = MMA M = K extent
-  static constexpr int KH = D / kStageMembers;             // K atoms per tile
-  static constexpr int S = 2;                              // operand stages
-  static constexpr int RS = 5;                             // raw slots
-  static constexpr uint32_t XBYTES = kTileGroups * 128;    // one K atom of X (hi or lo)
-  static constexpr uint32_t STAGE = 2 * XBYTES;
-  static constexpr uint32_t RAW = kStageMembers * kTileGroups * 8;
-  static constexpr uint32_t GCOLS = R / 2;                 // TMEM columns of one BF16 gate copy
-  static constexpr uint32_t TACC = kTileGroups;            // columns of one accumulator
-  static constexpr uint32_t COL_GHI = 2 * TACC, COL_GLO = COL_GHI + GCOLS;
-  static constexpr uint32_t TCOLS = 512;
-  static constexpr uint32_t NBARS = 2 * RS + 2 * S + 5;
-  static constexpr uint32_t OFF_OP = 0;
-  static constexpr uint32_t OFF_RAW = OFF_OP + S * STAGE;
-  static constexpr uint32_t OFF_BARS = OFF_RAW + RS * RAW;
-  static constexpr uint32_t OFF_MOFF = OFF_BARS + NBARS * 8;
-  static constexpr uint32_t OFF_GBASE = OFF_MOFF + D * 8;
-  static constexpr uint32_t OFF_MISC = OFF_GBASE + kTileGroups * 8;
-  static constexpr uint32_t SMEM = OFF_MISC + 16 + 1024;
-  // kind::f16: F32 accumulate, BF16 A and B, K-major, N = 128 groups, M = R reals
-  static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) |
-                                    ((uint32_t)(kTileGroups >> 3) << 17) | ((uint32_t)(R >> 4) << 24);
-  static_assert(K == 6 && R == 128, "M = 128 output reals: the 6-qubit gate");
-  static_assert(COL_GLO + GCOLS <= TCOLS, "TMEM columns");
-  static_assert(SMEM <= 227 * 1024, "shared memory");
-  static_assert(OFF_RAW % 1024 == 0 && OFF_GBASE % 8 == 0, "alignment");
-};
-
-__device__ __forceinline__ void tc_mma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc,
-                                          uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}\n" ::"r"(d_tmem),
-      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-
-// 32 lanes x 32 consecutive 32-bit columns from registers into tensor memory.
-__device__ __forceinline__ void tc_st32(uint32_t taddr, const uint32_t (&v)[32]) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
-      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};\n" ::"r"(taddr),
-      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
-      "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]),
-      "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]),
-      "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]),
-      "r"(v[30]), "r"(v[31])
-      : "memory");
-}
-
-// gate_rows: hi rows then lo rows, R rows of GCOLS 32-bit words (BF16 pairs of the
-// row's K reals), as packed by the host for this kernel.
-template <int K, typename Off>
-__global__ void __launch_bounds__(kTThreads, 1)
-    k_gate_umma_tt(float2 *__restrict__ psi, uint64_t n_groups, TcTargets t,
-                   const uint32_t *__restrict__ gate_rows, int run_log2) {
-  using C = UttCfg<K>;
-  extern __shared__ __align__(1024) unsigned char smem_dyn[];
-  unsigned char *sm = reinterpret_cast<unsigned char *>(
-      (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~static_cast<uintptr_t>(1023));
-  const uint32_t s_base = smem_u32(sm);
-  const uint32_t s_bar = s_base + C::OFF_BARS;
-  auto raw_full = [&](int r) { return s_bar + 8u * r; };
-  auto raw_empty = [&](int r) { return s_bar + 8u * (C::RS + r); };
-  auto op_full = [&](int q) { return s_bar + 8u * (2 * C::RS + q); };
-  auto op_empty = [&](int q) { return s_bar + 8u * (2 * C::RS + C::S + q); };
-  auto accfull_bar = [&](int b) { return s_bar + 8u * (2 * C::RS + 2 * C::S + b); };
-  auto accempty_bar = [&](int b) { return s_bar + 8u * (2 * C::RS + 2 * C::S + 2 + b); };
-  const uint32_t drain_bar = s_bar + 8u * (2 * C::RS + 2 * C::S + 4);
-  Off *moff = reinterpret_cast<Off *>(sm + C::OFF_MOFF);
-  uint64_t *gbase = reinterpret_cast<uint64_t *>(sm + C::OFF_GBASE);
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sm + C::OFF_MISC);
-  volatile uint32_t *abort_flag = tmem_slot + 1;
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint64_t n_tiles = n_groups / kTileGroups;  // whole tiles only (checked on the host)
-
-  for (int m = threadIdx.x; m < C::D; m += kTThreads) moff[m] = (Off)tc_off<K>(m, t);
-  for (int g = threadIdx.x; g < kTileGroups; g += kTThreads) gbase[g] = tc_base<K>((uint64_t)g, t);
-  if (threadIdx.x == 0) {
-    for (int r = 0; r < C::RS; ++r) {
-      mbar_init(raw_full(r), 1);
-      mbar_init(raw_empty(r), kTConvThreads);
-    }
-    for (int q = 0; q < C::S; ++q) {
-      mbar_init(op_full(q), kTConvThreads);
-      mbar_init(op_empty(q), 1);
-    }
-    for (int b = 0; b < 2; ++b) {
-      mbar_init(accfull_bar(b), 1);
-      mbar_init(accempty_bar(b), kTEpiWarps * 32);
-    }
-    mbar_init(drain_bar, 1);
-    *abort_flag = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
-  if (warp == kTMmaWarp) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
-                     smem_u32(tmem_slot)),
-                 "r"(C::TCOLS)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = *tmem_slot;
-  // the gate into tensor memory: warp w < 4 writes rows 32 w .. 32 w + 31 (its lanes)
-  if (warp < 4) {
-    const uint32_t row = 32u * warp + lane;
-    const uint32_t lane_addr = tmem + ((32u * warp) << 16);
-#pragma unroll
-    for (int copy = 0; copy < 2; ++copy) {
-      const uint32_t *src = gate_rows + ((size_t)copy * C::R + row) * C::GCOLS;
-      const uint32_t col0 = copy ? C::COL_GLO : C::COL_GHI;
-#pragma unroll
-      for (int c0 = 0; c0 < (int)C::GCOLS; c0 += 32) {
-        uint32_t v[32];
-#pragma unroll
-        for (int i = 0; i < 32; ++i) v[i] = src[c0 + i];
-        tc_st32(lane_addr + col0 + c0, v);
-      }
-    }
-    asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-
-  if (warp == kTMmaWarp) {
-    // ---- MMA issuer: tile `it` consumes operand stages h = it * KH + kp --------
-    uint32_t it = 0;
-    bool issued = false, ok = true;
-    for (uint64_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x, ++it) {
-      const uint32_t b = it & 1, v = it >> 1;
-      for (int kp = 0; kp < C::KH; ++kp) {
-        const uint32_t h = it * C::KH + kp, q = h % C::S, u = h / C::S;
-        if (!mbar_wait_warp(op_full(q), u & 1, abort_flag, kErrMmaFullWait)) { ok = false; break; }
-        if (kp == 0 && !mbar_wait_warp(accempty_bar(b), (v & 1) ^ 1, abort_flag, kErrMmaAccWait)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        if (lane == 0) {
-          const uint32_t xh = s_base + C::OFF_OP + q * C::STAGE, xl = xh + C::XBYTES;
-          const uint32_t d = tmem + b * C::TACC;
-#pragma unroll
-          for (int ks = 0; ks < 4; ++ks) {
-            // K reals kp * 64 + ks * 16 .. +15: 8 columns of each gate copy
-            const uint32_t ah = tmem + C::COL_GHI + kp * 32 + ks * 8;
-            const uint32_t al = tmem + C::COL_GLO + kp * 32 + ks * 8;
-            const uint64_t b_hi = umma_desc_sw128(xh + ks * 32), b_lo = umma_desc_sw128(xl + ks * 32);
-            tc_mma_ts(d, ah, b_lo, C::IDESC, (kp > 0 || ks > 0) ? 1u : 0u);
-            tc_mma_ts(d, al, b_hi, C::IDESC, 1u);
-            tc_mma_ts(d, ah, b_hi, C::IDESC, 1u);
-          }
-          tc_commit(op_empty(q));
-          if (kp == C::KH - 1) tc_commit(accfull_bar(b));
-        }
-        __syncwarp();
-        issued = true;
-      }
-    }
-    if (issued) {
-      if (lane == 0) tc_commit(drain_bar);
-      __syncwarp();
-      volatile uint32_t never = 0;
-      mbar_wait_warp(drain_bar, 0, &never, kErrDrainWait);
-    }
-  } else if (warp == kTProdWarp) {
-    // ---- producer: bulk copies of raw slot h = it * KH + kp --------------------
-    const int run = 1 << run_log2, runs = kTileGroups >> run_log2;
-    const int copies = kStageMembers * runs;
-    uint32_t h = 0;
-    bool ok = true;
-    for (uint64_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
-      const float2 *tp = psi + tc_base<K>(tile * kTileGroups, t);
-      for (int kp = 0; kp < C::KH; ++kp) {
-        const uint32_t r = h % C::RS, u = h / C::RS;
-        if (!mbar_wait_warp(raw_empty(r), (u & 1) ^ 1, abort_flag, kErrProducerWait)) {
-          ok = false;
-          break;
-        }
-        if (lane == 0) mbar_arrive_expect_tx(raw_full(r), C::RAW);
-        __syncwarp();
-        const uint32_t dst0 = s_base + C::OFF_RAW + r * C::RAW;
-        for (int c = lane; c < copies; c += 32) {
-          const int ml = c / runs, rr = c % runs;
-          bulk_g2s(dst0 + ml * (kTileGroups * 8) + (rr << run_log2) * 8,
-                   tp + gbase[rr << run_log2] + moff[kp * kStageMembers + ml], run * 8, raw_full(r));
-        }
-        ++h;
-      }
-    }
-    // every copy this CTA issued has landed before its shared memory is released
-    volatile uint32_t never = 0;
-    for (uint32_t j = h > (uint32_t)C::RS ? h - C::RS : 0; j < h; ++j)
-      mbar_wait_warp(raw_full(j % C::RS), (j / C::RS) & 1, &never, kErrDrainWait);
-  } else if (warp >= kTEpiWarps) {
-    // ---- converters: raw slot -> split BF16 -> operand stage -------------------
-    const int ct = threadIdx.x - kTEpiWarps * 32;
-    const int gg = ct % kTileGroups, half = ct / kTileGroups;
-    for (uint32_t h = 0;; ++h) {
-      const uint64_t tile = blockIdx.x + (uint64_t)(h / C::KH) * gridDim.x;
-      if (tile >= n_tiles) break;
-      const uint32_t r = h % C::RS, ur = h / C::RS, q = h % C::S, uq = h / C::S;
-      if (!mbar_wait_warp(raw_full(r), ur & 1, abort_flag, kErrConvertWait)) break;
-      if (!mbar_wait_warp(op_empty(q), (uq & 1) ^ 1, abort_flag, kErrConvertWait)) break;
-      const unsigned char *raw = sm + C::OFF_RAW + r * C::RAW + gg * 8;
-      unsigned char *xh = sm + C::OFF_OP + q * C::STAGE, *xl = xh + C::XBYTES;
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj) {
-        const int chunk = 4 * half + jj;
-        uint32_t hb4[4], lb4[4];
-#pragma unroll
-        for (int m = 0; m < 4; ++m) {
-          const float2 v = *reinterpret_cast<const float2 *>(raw + (4 * chunk + m) * (kTileGroups * 8));
-          const __nv_bfloat162 hv = __floats2bfloat162_rn(v.x, v.y);
-          const uint32_t hb = bf162_bits(hv);
-          const __nv_bfloat162 lv = __floats2bfloat162_rn(v.x - __uint_as_float(hb << 16),
-                                                          v.y - __uint_as_float(hb & 0xFFFF0000u));
-          hb4[m] = hb;
-          lb4[m] = bf162_bits(lv);
-        }
-        const uint32_t off = (uint32_t)gg * 128 + ((uint32_t)(chunk ^ (gg & 7)) << 4);
-        *reinterpret_cast<uint4 *>(xh + off) = make_uint4(hb4[0], hb4[1], hb4[2], hb4[3]);
-        *reinterpret_cast<uint4 *>(xl + off) = make_uint4(lb4[0], lb4[1], lb4[2], lb4[3]);
-      }
-      fence_async_smem();
-      mbar_arrive(op_full(q));
-      mbar_arrive(raw_empty(r));
-    }
-  } else {
-    // ---- epilogue: TMEM (reals x groups) -> lane pairs -> HBM ----------------------
-    const int quarter = warp & 3, half = warp >> 2;
-    const int m = 16 * quarter + (lane >> 1);  // member; re on even lanes, im on odd
-    const bool odd = lane & 1;
-    uint32_t it = 0;
-    for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++it) {
-      const uint32_t b = it & 1, v = it >> 1;
-      if (!mbar_wait_warp(accfull_bar(b), v & 1, abort_flag, kErrEpilogueWait)) break;
-      tc_fence_after();
-      float2 *const tb = psi + tc_base<K>(tile * kTileGroups, t) + moff[m];
-      const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + b * C::TACC + half * 64;
-#pragma unroll
-      for (int ci = 0; ci < 2; ++ci) {
-        float rr[32];
-        tc_ld32(taddr + ci * 32, rr);
-        if (ci == 1) {
-          tc_fence_before();
-          mbar_arrive(accempty_bar(b));
-        }
-        // even lane keeps groups 0..15 of the chunk (its re, the partner's im),
-        // odd lane groups 16..31 (the partner's re, its im)
-        float2 out[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const float give = odd ? rr[i] : rr[16 + i];
-          const float got = __shfl_xor_sync(0xffffffffu, give, 1);
-          out[i] = odd ? make_float2(got, rr[16 + i]) : make_float2(rr[i], got);
-        }
-        const int g0 = half * 64 + ci * 32 + (odd ? 16 : 0);
-#pragma unroll
-        for (int i = 0; i < 16; i += 2)
-          *reinterpret_cast<float4 *>(tb + gbase[g0 + i]) =
-              make_float4(out[i].x, out[i].y, out[i + 1].x, out[i + 1].y);
-      }
-    }
-  }
-  tc_fence_before();
-  __syncthreads();
-  if (warp == kTMmaWarp) {
-    tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
-                 "r"(C::TCOLS)
-                 : "memory");
-  }
-}
-
 uint16_t bf16_bits_rn(float f) {
   uint32_t u;
   std::memcpy(&u, &f, 4);
@@ -1085,31 +780,6 @@ bool launch_ut_k(const uint32_t *qubits, const void *d_tc, void *sv, uint32_t n,
   return cuda_ok(cudaGetLastError(), "tensor gate kernel launch (TMA)", err);
 }
 
-template <int K, typename Off>
-bool launch_utt_k(const uint32_t *qubits, const void *gate_rows, void *sv, uint32_t n, cudaStream_t s,
-                  std::string &err) {
-  using C = UttCfg<K>;
-  static std::once_flag once;
-  static cudaError_t attr_rc = cudaSuccess;
-  std::call_once(once, [] {
-    attr_rc = cudaFuncSetAttribute(k_gate_umma_tt<K, Off>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)C::SMEM);
-  });
-  if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(tensor gate kernel, gate in TMEM)", err)) return false;
-  TcTargets t;
-  for (uint32_t b = 0; b < kMaxGateQubits; ++b) {
-    const uint32_t q = b < (uint32_t)K ? qubits[b] : 0;
-    t.lo_mask[b] = (1ull << q) - 1;
-    t.stride[b] = 1ull << q;
-  }
-  const uint64_t n_tiles = (1ull << (n - K)) / kTileGroups;
-  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(n_tiles, (uint64_t)sm_count()));
-  k_gate_umma_tt<K, Off><<<grid, kTThreads, C::SMEM, s>>>(
-      static_cast<float2 *>(sv), 1ull << (n - K), t, static_cast<const uint32_t *>(gate_rows),
-      (int)std::min<uint32_t>(qubits[0], 7));
-  return cuda_ok(cudaGetLastError(), "tensor gate kernel launch (gate in TMEM)", err);
-}
-
 }  // namespace
 
 bool tensor_path_supported(const GateData &g) {
@@ -1138,30 +808,6 @@ std::vector<uint16_t> pack_tensor_operand(const double *m64, int k) {
       packed[per + byte / 2] = lo;
     }
   return packed;
-}
-
-// The same split operand as rows for tensor memory (the A operand of the kernel
-// with the gate in TMEM): hi rows then lo rows, row r = output real r, word c of
-// a row = the BF16 pair (Mr[r][2c], Mr[r][2c+1]), the even column in the low half.
-std::vector<uint32_t> pack_tensor_rows(const double *m64, int k) {
-  const int D = 1 << k, R = 2 * D;
-  std::vector<uint32_t> rows(2 * (size_t)R * (R / 2));
-  for (int row = 0; row < R; ++row)
-    for (int col = 0; col < R; col += 2) {
-      uint16_t hb[2], lb[2];
-      for (int e = 0; e < 2; ++e) {
-        const int c = col + e, r = row >> 1, m = c >> 1;
-        const double a = m64[2 * ((size_t)r * D + m)], b = m64[2 * ((size_t)r * D + m) + 1];
-        const bool out_im = row & 1, in_im = c & 1;
-        const double v = out_im ? (in_im ? a : b) : (in_im ? -b : a);
-        hb[e] = bf16_bits_rn((float)v);
-        lb[e] = bf16_bits_rn((float)(v - (double)bf16_value(hb[e])));
-      }
-      const size_t w = (size_t)row * (R / 2) + col / 2;
-      rows[w] = (uint32_t)hb[0] | ((uint32_t)hb[1] << 16);
-      rows[(size_t)R * (R / 2) + w] = (uint32_t)lb[0] | ((uint32_t)lb[1] << 16);
-    }
-  return rows;
 }
 
 // A 5-qubit gate runs on the 6-qubit kernel, padded with the identity on a spare
@@ -1207,20 +853,10 @@ bool prepare_tensor_gate(GateData &g, uint32_t n, std::string &err) {
           m6[dst + 1] = g.m64[src + 1];
         }
     packed = pack_tensor_operand(m6.data(), 6);
-    const std::vector<uint32_t> rows = pack_tensor_rows(m6.data(), 6);
-    const size_t at = packed.size();
-    packed.resize(at + 2 * rows.size());
-    std::memcpy(packed.data() + at, rows.data(), rows.size() * 4);
     g.tc_k = 6;
     for (uint32_t b = 0; b < 6; ++b) g.tc_qubits[b] = q6[b];
   } else {
     packed = pack_tensor_operand(g.m64.data(), (int)g.k);
-    if (g.k == 6) {  // 6-qubit gates also carry the tensor-memory rows
-      const std::vector<uint32_t> rows = pack_tensor_rows(g.m64.data(), 6);
-      const size_t at = packed.size();
-      packed.resize(at + 2 * rows.size());
-      std::memcpy(packed.data() + at, rows.data(), rows.size() * 4);
-    }
   }
   if (g.d_tc) cudaFree(g.d_tc);
   g.d_tc = nullptr;
@@ -1242,15 +878,9 @@ bool launch_gate_tensor(const GateData &g, void *sv, uint32_t n, cudaStream_t s,
   // lowest target >= 7 and whole tiles: every member's 128 groups are one 1 KB
   // run, fetched with one TMA bulk copy (shorter runs measured slower with TMA
   // than with register loads: 256-byte copies ran at 2.0 TB/s for k = 6)
-  if (g.tc_k == 6 && q[0] >= 7 && n >= 6 + 7 && tma_enabled()) {
-    if (g_tensor_loader.load() == 2)
-      return narrow ? launch_ut_k<6, uint32_t>(q, op, sv, n, s, err)
-                    : launch_ut_k<6, uint64_t>(q, op, sv, n, s, err);
-    // the tensor-memory rows follow the two 64 KB shared-memory operand blocks
-    const void *rows = static_cast<const unsigned char *>(op) + 2 * 128 * 128 * 2;
-    return narrow ? launch_utt_k<6, uint32_t>(q, rows, sv, n, s, err)
-                  : launch_utt_k<6, uint64_t>(q, rows, sv, n, s, err);
-  }
+  if (g.tc_k == 6 && q[0] >= 7 && n >= 6 + 7 && tma_enabled())
+    return narrow ? launch_ut_k<6, uint32_t>(q, op, sv, n, s, err)
+                  : launch_ut_k<6, uint64_t>(q, op, sv, n, s, err);
   if (g.tc_k == 5) {
     if (narrow) return stage ? launch_um_k<5, uint32_t, true>(q, op, sv, n, s, err)
                              : launch_um_k<5, uint32_t, false>(q, op, sv, n, s, err);

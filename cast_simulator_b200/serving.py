@@ -111,7 +111,7 @@ class ServingEngine:
                  traj_fusion_k: int | None = None, use_graph: bool = False,
                  batch_max_qubits: int = 16, batch_fusion_k: int = 3, max_batch: int = 1024,
                  split_min_qubits: int = 20, heavy_slots: int = 1, heavy_pure_qubits: int = 22,
-                 heavy_noisy_qubits: int = 17):
+                 heavy_noisy_qubits: int = 17, heavy_priority: bool = False):
         """max_slots: requests running at once on the worker streams.
         traj_fusion_k: fusion width of noisy requests' trajectory programs (None:
         3 up to 16 qubits, where the states sit in L1/L2 and the passes are bound
@@ -126,6 +126,9 @@ class ServingEngine:
         after the other.  Only the device phase waits: a heavy request is
         admitted as usual and fuses and builds its program while another one
         runs, and small requests still overlap with it.
+        heavy_priority: heavy requests run on a more urgent stream (their thread
+        blocks start first when SMs free up), so the small requests around them
+        slow them down less.
         batch_max_qubits: pure requests of at most this many qubits run batched
         in the circuit-batch kernel (0 turns batching off); batch_fusion_k: their
         fusion width (<= 4); max_batch: circuits a batch launch takes at most
@@ -148,6 +151,7 @@ class ServingEngine:
         self.heavy_pure_qubits = heavy_pure_qubits
         self.heavy_noisy_qubits = heavy_noisy_qubits
         self._gpu_heavy = threading.Semaphore(max(1, heavy_slots))
+        self.heavy_priority = heavy_priority
         self._bwork: collections.deque = collections.deque()
         self._bcv = threading.Condition()
         self._batched_active = 0
@@ -269,6 +273,7 @@ class ServingEngine:
 
     def _worker(self) -> None:
         stream = Stream()
+        urgent = Stream(priority=-1000) if self.heavy_priority else stream
         while True:
             with self._work_cv:
                 while not self._work and not self._stop:
@@ -277,7 +282,7 @@ class ServingEngine:
                     return
                 req, fut, t_arr, need, t_adm = self._work.popleft()
             try:
-                z = self._execute(req, stream)
+                z = self._execute(req, urgent if self._heavy(req) else stream)
                 res = Result(req.rid, z, t_arr, t_adm, self.now(), req.circuit.n_qubits(),
                              req.precision, req.n_traj)
                 fut.set_result(res)
