@@ -1072,16 +1072,24 @@ def main(argv=None):
             "value": min(args.steps, 10) * len(orun["gates"]) * ob / orun["t"] / 1e9, "unit": "GB/s",
             "ms_per_step": orun["t"] / min(args.steps, 10) * 1e3, "dtype": other,
             "roofline": roofline_of(orun, n, other), "clocks": orun["clocks"]}
-        line["qft"] = qft_leg()
+        import gc
+
+        def leg(key, fn, *a):
+            # each leg's device objects (programs, graphs, statevectors) are released
+            # before the next one starts
+            line[key] = fn(*a)
+            gc.collect()
+
+        leg("qft", qft_leg)
         if not args.no_sweep:
-            line["fusion_sweep"] = fusion_sweep_leg(n, args.depth)
-            line["tensor_path"] = tensor_leg(n, args.depth, line["fusion_sweep"])
-        line["sampling"] = sampling_leg(n, args.depth)
-        line["circuit_batch"] = circuit_batch_leg()
-        line["trajectories"] = trajectory_leg()
-        line["serving"] = serving_leg(args.serve_requests)
+            leg("fusion_sweep", fusion_sweep_leg, n, args.depth)
+            leg("tensor_path", tensor_leg, n, args.depth, line["fusion_sweep"])
+        leg("sampling", sampling_leg, n, args.depth)
+        leg("circuit_batch", circuit_batch_leg)
+        leg("trajectories", trajectory_leg)
+        leg("serving", serving_leg, args.serve_requests)
         if not args.no_largest:
-            line["largest_fit"] = largest_leg(threads)
+            leg("largest_fit", largest_leg, threads)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg:

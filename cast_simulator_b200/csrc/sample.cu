@@ -21,10 +21,11 @@
 //     with the true T (an unnormalised state), so the integers never overflow;
 //  2. exact exclusive scans: of the chunk totals (C_c, where chunk c starts in
 //     the CDF) and, for seeded sampling, of the shots' exponential spacings;
-//  3. assignment: one CTA per chunk binary-searches the sorted targets for the
-//     shots in [C_c, C_c+1); a chunk with none exits at once, the others stage
-//     q_i in shared memory, form the chunk's inclusive prefix sums and
-//     binary-search them per shot.
+//  3. assignment: one thread per chunk binary-searches the sorted targets for
+//     the chunk's first shot (all chunks in parallel); then one CTA per chunk
+//     takes its shots [first_c, first_c+1): a chunk with none exits at once, the
+//     others stage q_i in shared memory, form the chunk's inclusive prefix sums
+//     and binary-search them per shot.
 //
 // Sorted uniforms without a sort: with E_0..E_N i.i.d. Exp(1) and
 // S_i = E_0 + ... + E_{i-1}, (S_1/S_{N+1}, ..., S_N/S_{N+1}) are distributed as
@@ -235,40 +236,43 @@ struct Targets {
   }
 };
 
-// Pass 3.
-template <typename T>
-__global__ void __launch_bounds__(kSmpThreads) k_sample_assign(
-    const T *__restrict__ x, uint32_t cb, uint64_t n_chunks, const uint64_t *__restrict__ start,
-    const Targets tg, uint64_t n_shots, double scale, const __grid_constant__ KeyMap km,
-    uint64_t *__restrict__ out) {
-  using V = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
-  // one padding slot after every 16: a thread's run of 16 starts 17 slots after
-  // its neighbour's, so the runs of a warp sit in different banks
-  __shared__ uint64_t q[(1u << kMaxChunkBits) + (1u << kMaxChunkBits) / 16];
-  __shared__ uint64_t ws[kSmpThreads / 32];
-  __shared__ uint64_t range[2];
-  const uint64_t chunk = blockIdx.x;
-  if (threadIdx.x < 2) {
-    // first shot whose target is >= the chunk's start (resp. the next chunk's);
-    // the first chunk starts at shot 0 and the last ends at the last shot
-    const bool upper = threadIdx.x == 1;
+// Shot ranges: first[c] = the first shot whose target is >= the start of chunk c
+// (first[0] = 0, first[n_chunks] = n_shots), one thread a chunk, all chunks'
+// binary searches in parallel; chunk c takes shots first[c] .. first[c+1] - 1.
+__global__ void k_chunk_first_shot(const uint64_t *__restrict__ start, uint64_t n_chunks,
+                                   const Targets tg, uint64_t n_shots, uint64_t *__restrict__ first) {
+  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c <= n_chunks;
+       c += (uint64_t)gridDim.x * blockDim.x) {
     uint64_t a = 0, b = n_shots;
-    if (upper && chunk + 1 == n_chunks) {
-      a = n_shots;
-    } else if (!upper && chunk == 0) {
+    if (c == 0) {
       b = 0;
+    } else if (c == n_chunks) {
+      a = n_shots;
     } else {
-      const uint64_t bound = start[chunk + (upper ? 1 : 0)];
+      const uint64_t bound = start[c];
       while (a < b) {
         const uint64_t mid = a + (b - a) / 2;
         if (tg(mid) < bound) a = mid + 1;
         else b = mid;
       }
     }
-    range[threadIdx.x] = a;
+    first[c] = a;
   }
-  __syncthreads();
-  const uint64_t lo = range[0], hi = range[1];
+}
+
+// Pass 3.
+template <typename T>
+__global__ void __launch_bounds__(kSmpThreads) k_sample_assign(
+    const T *__restrict__ x, uint32_t cb, const uint64_t *__restrict__ start,
+    const uint64_t *__restrict__ first, const Targets tg, double scale,
+    const __grid_constant__ KeyMap km, uint64_t *__restrict__ out) {
+  using V = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+  // one padding slot after every 16: a thread's run of 16 starts 17 slots after
+  // its neighbour's, so the runs of a warp sit in different banks
+  __shared__ uint64_t q[(1u << kMaxChunkBits) + (1u << kMaxChunkBits) / 16];
+  __shared__ uint64_t ws[kSmpThreads / 32];
+  const uint64_t chunk = blockIdx.x;
+  const uint64_t lo = first[chunk], hi = first[chunk + 1];
   if (lo >= hi) return;
   const uint32_t c = 1u << cb;
   const uint32_t nt = c < (uint32_t)kSmpThreads ? c : (uint32_t)kSmpThreads;
@@ -314,7 +318,7 @@ bool sample_impl(const void *sv, uint32_t n, uint64_t n_shots, bool seeded, uint
   const uint64_t tiles_c = (n_chunks + tile - 1) / tile, tiles_s = (n_sp + tile - 1) / tile;
   // 8-byte slots: chunk totals (int, FP64), chunk starts, tile totals (both
   // scans), grand totals, spacings (raw and scanned) or uniforms, keys
-  const uint64_t slots = 3 * n_chunks + tiles_c + tiles_s + 4 + (seeded ? 2 * n_sp : n_shots) + n_shots;
+  const uint64_t slots = 4 * n_chunks + 1 + tiles_c + tiles_s + 4 + (seeded ? 2 * n_sp : n_shots) + n_shots;
   char *scratch = nullptr;
   if (!cuda_ok(cudaMallocAsync((void **)&scratch, slots * 8, s), "cudaMallocAsync (sampling scratch)",
                err))
@@ -322,7 +326,8 @@ bool sample_impl(const void *sv, uint32_t n, uint64_t n_shots, bool seeded, uint
   uint64_t *qtot = reinterpret_cast<uint64_t *>(scratch);
   double *ptot = reinterpret_cast<double *>(qtot + n_chunks);
   uint64_t *start = qtot + 2 * n_chunks;
-  uint64_t *tt_c = start + n_chunks;
+  uint64_t *first = start + n_chunks;  // n_chunks + 1 entries
+  uint64_t *tt_c = first + n_chunks + 1;
   uint64_t *tt_s = tt_c + tiles_c;
   uint64_t *grand = tt_s + tiles_s;  // [0] Q, [1] spacing total, [2] FP64 T (bits)
   uint64_t *sp_raw = grand + 4;
@@ -376,8 +381,10 @@ bool sample_impl(const void *sv, uint32_t n, uint64_t n_shots, bool seeded, uint
   }
   if (ok) {
     Targets tg{seeded ? sp : nullptr, totals[1], seeded ? nullptr : u_dev, (double)totals[0]};
-    k_sample_assign<T><<<(unsigned)n_chunks, kSmpThreads, 0, s>>>(x, cb, n_chunks, start, tg, n_shots,
-                                                                   scale, km, keys);
+    const unsigned fg = (unsigned)std::min<uint64_t>((n_chunks + 256) / 256, 16ull * sm_count());
+    k_chunk_first_shot<<<fg, 256, 0, s>>>(start, n_chunks, tg, n_shots, first);
+    k_sample_assign<T><<<(unsigned)n_chunks, kSmpThreads, 0, s>>>(x, cb, start, first, tg, scale, km,
+                                                                   keys);
     ok = cuda_ok(cudaGetLastError(), "sampling assignment launch", err) &&
          cuda_ok(cudaMemcpyAsync(host_out, keys, n_shots * 8, cudaMemcpyDeviceToHost, s),
                  "cudaMemcpyAsync (sampled keys)", err);
