@@ -119,13 +119,13 @@ class ClockSampler:
 
 
 def build_fused(n: int, depth: int, k: int, seed: int = 2024):
-    from cast_simulator_b200.fusion import CircuitGraph, FusionConfig, optimize
+    """The brickwork construction fused at width k by the native planner (the
+    same decisions as fusion.optimize, tests/test_native_fusion.py)."""
+    from cast_simulator_b200.fusion import FusionConfig, optimize_native
     from cast_simulator_b200.types import QuantumCircuit
 
     circ = QuantumCircuit.brickwork(n, depth, seed)
-    g = CircuitGraph.from_circuit(circ)
-    optimize(g, FusionConfig.size_only(k))
-    return circ, g.gates_in_row_order()
+    return circ, optimize_native(n, circ.gates(), FusionConfig.size_only(k)).gates()
 
 
 _CB_LIB = None

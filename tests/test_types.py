@@ -84,3 +84,35 @@ def test_dead_gate_elimination():
     c = QuantumCircuit(3).add(QuantumGate.h(0)).add(QuantumGate.h(2)).add(QuantumGate.cx(0, 1))
     c = c.with_measured_qubits([1])
     assert [g.qubits() for g in c.eliminate_dead_gates().gates()] == [(0,), (0, 1)]
+
+
+def test_u3_matches_the_openqasm_definition(oracle):
+    """Dense U3 (theta != 0, as every brickwork layer uses it) pinned to the
+    OpenQASM 2.0 definition, written here from first principles rather than
+    from either implementation: U(theta, phi, lambda) =
+    e^{i(phi+lambda)/2} Rz(phi) Ry(theta) Rz(lambda), with Rz(a) =
+    diag(e^{-ia/2}, e^{ia/2}) and Ry(t) = [[cos t/2, -sin t/2], [sin t/2,
+    cos t/2]].  Both the package's and the oracle's U3 must equal it to 1e-15,
+    as must the Rx / Ry / Rz of both (U3(t, -pi/2, pi/2) = Rx(t) up to phase is
+    the identity the fixtures' decompositions rely on)."""
+    rng = np.random.default_rng(9)
+
+    def rz(a):
+        return np.diag([np.exp(-0.5j * a), np.exp(0.5j * a)])
+
+    def ry(t):
+        c, s = np.cos(t / 2), np.sin(t / 2)
+        return np.array([[c, -s], [s, c]], dtype=complex)
+
+    for _ in range(50):
+        th, ph, la = rng.uniform(-2 * np.pi, 2 * np.pi, size=3)
+        want = np.exp(0.5j * (ph + la)) * rz(ph) @ ry(th) @ rz(la)
+        assert np.max(np.abs(QuantumGate.u3(th, ph, la, 0).matrix() - want)) < 1e-15
+        assert np.max(np.abs(oracle.named(oracle.U3, th, ph, la) - want)) < 1e-15
+        # rotations: Rx(t) = Rz(-pi/2) Ry(t) Rz(pi/2)
+        rx = rz(-np.pi / 2) @ ry(th) @ rz(np.pi / 2)
+        for mine, ref in ((QuantumGate.rx(th, 0).matrix(), rx), (QuantumGate.ry(th, 0).matrix(), ry(th)),
+                          (QuantumGate.rz(th, 0).matrix(), rz(th))):
+            assert np.max(np.abs(mine - ref)) < 1e-15
+        for kind, ref in ((oracle.RX, rx), (oracle.RY, ry(th)), (oracle.RZ, rz(th))):
+            assert np.max(np.abs(oracle.named(kind, th) - ref)) < 1e-15
