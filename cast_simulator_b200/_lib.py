@@ -108,6 +108,8 @@ CAST_B200 = [
     ("cast_b200_sv_zero_async", C.c_int,
      [C.c_uint64, C.c_size_t, C.c_uint8, C.c_void_p, C.c_char_p, C.c_size_t]),
     ("cast_b200_set_gate_path", C.c_int, [C.c_int]),
+    ("cast_b200_set_kernel_choice", C.c_int,
+     [C.c_uint8, C.c_uint32, C.c_uint32, C.c_int, C.c_uint32, C.c_char_p, C.c_size_t]),
     ("cast_b200_apply_gate", C.c_int,
      [C.c_uint64, C.c_uint32, C.c_uint8, C.POINTER(Complex64), c_u32p, C.c_uint32, C.c_double,
       C.c_double, C.c_void_p, C.c_char_p, C.c_size_t]),

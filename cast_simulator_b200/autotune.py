@@ -22,7 +22,12 @@ AI = peak / bw_slope to the hardware-adaptive cost model
     and engine with the least predicted time;
   * ``tune_trajectories`` times the batched-trajectory kernel of a noisy
     circuit at each fusion width and launch shape (threads per CTA, CTAs in
-    flight) and returns the fastest.
+    flight) and returns the fastest;
+  * ``tune_kernels`` times, for every class of dense k <= 4 gates with targets
+    below qubit 5 (precision, k, the set of such targets), the register kernel
+    and the tile kernel at 2048 and 4096 amplitudes a tile, and routes each
+    class to its fastest (``set_kernel_choice``); the
+    choices go into ``HardwareProfile.kernel_choices`` for later processes.
 
 Command line:
 
@@ -31,6 +36,7 @@ Command line:
     python -m cast_simulator_b200.autotune choose --n 30 --depth 20 --precision f32
     python -m cast_simulator_b200.autotune choose --circuit qft --n 30 --precision f64
     python -m cast_simulator_b200.autotune traj --n 16 --depth 30
+    python -m cast_simulator_b200.autotune kernels --n 26 [--profile prof.json]
 """
 from __future__ import annotations
 
@@ -293,6 +299,108 @@ def tune_trajectories(circuit, n_traj: int = 4096, ks=(2, 3, 4), threads=(0, 512
     return TrajChoice(top["fusion_k"], top["threads"], top["max_ctas"], top["traj_per_s"], cands)
 
 
+# (engine, tile bits) candidates for the low-target classes
+KERNEL_CANDIDATES = (("register", 0), ("tile", 11), ("tile", 12))
+
+
+def kernel_classes(ks=range(1, 5)):
+    """Every (k, low_mask) class of dense gates with at least one target below
+    qubit 5: low_mask is that set of targets as bits."""
+    return [(k, m) for k in ks for m in range(1, 32) if bin(m).count("1") <= k]
+
+
+def class_targets(n: int, k: int, low_mask: int) -> tuple:
+    """The representative target set of a class: its low targets, the rest at
+    the top, the middle and qubit 8 of an n-qubit register."""
+    lows = [b for b in range(5) if (low_mask >> b) & 1]
+    return tuple(sorted(lows + [n - 1, n // 2, 8][:k - len(lows)]))
+
+
+def _time_targets(n: int, prec, q: tuple, reps: int, sv, st, rng) -> float:
+    from .simulator import Event, GateProgram
+
+    prog = GateProgram(prec, n, 1e-12, 1e-12)
+    prog.add(haar(len(q), rng), q)
+    e0, e1 = Event(), Event()
+    best = math.inf
+    for i in range(reps + 1):
+        e0.record(st)
+        prog.run(sv, st, use_graph=False)
+        e1.record(st)
+        e1.sync()
+        if i:
+            best = min(best, e1.elapsed_s(e0))
+    return best
+
+
+def tune_kernels(n: int = 26, precisions=("f64", "f32"), ks=range(1, 5), reps: int = 5,
+                 apply: bool = True, seed: int = 7, margin: float = 0.02) -> list[dict]:
+    """Time every candidate kernel on every low-target class (best of ``reps``
+    launches of a Haar-random gate on the class's representative targets) and
+    return one record per class: its winner, the built-in rule's choice and
+    each candidate's milliseconds.  A tile kernel wins only when it beats the
+    register kernel by more than ``margin`` (the launch-to-launch spread).  With
+    ``apply`` the winners are routed process-wide, else every class goes back to
+    the built-in rule."""
+    from .cuda import CudaPrecision, CudaStatevector
+    from .simulator import Stream, gate_engine, set_kernel_choice
+
+    rng = np.random.default_rng(seed)
+    st = Stream()
+    out = []
+    for pname in precisions:
+        prec = CudaPrecision.F64 if pname == "f64" else CudaPrecision.F32
+        sv = CudaStatevector(n, prec)
+        sv.zero()
+        for k, mask in kernel_classes(ks):
+            q = class_targets(n, k, mask)
+            set_kernel_choice(prec, k, mask, None)
+            builtin = gate_engine(haar(k, rng), q, n, prec)
+            ms = {}
+            for eng, tb in KERNEL_CANDIDATES:
+                set_kernel_choice(prec, k, mask, eng, tb)
+                ms[f"{eng}{tb or ''}"] = 1e3 * _time_targets(n, prec, q, reps, sv, st, rng)
+            (eng, tb), best = min(((c, ms[f"{c[0]}{c[1] or ''}"]) for c in KERNEL_CANDIDATES),
+                                  key=lambda x: x[1])
+            if best > ms["register"] * (1.0 - margin):
+                eng, tb = "register", 0
+            set_kernel_choice(prec, k, mask, eng if apply else None, tb if apply else 0)
+            out.append({"precision": pname, "k": k, "low_mask": mask, "targets": list(q),
+                        "engine": eng, "tile_bits": tb, "builtin": builtin, "ms": ms})
+        del sv
+    return out
+
+
+def cxx_table(choices) -> str:
+    """The built-in routing table of the gate library (gate_kernels.cu,
+    kDefaultChoice) from ``tune_kernels`` records of both precisions: per
+    precision and k a 32-character row indexed by the low-target mask, 'r' the
+    register kernel, 'a' / 'b' the tile kernel with 2048 / 4096 amplitudes."""
+    code = {("register", 0): "r", ("tile", 11): "a", ("tile", 12): "b"}
+    tab = {(c["precision"], c["k"], c["low_mask"]): code[(c["engine"], c["tile_bits"])]
+           for c in choices}
+    lines = []
+    for p in ("f32", "f64"):
+        rows = ['"' + "".join(tab.get((p, k, m), "-") for m in range(32)) + '"'
+                for k in range(1, 5)]
+        lines.append("    {\"\", " + ", ".join(rows) + "},")
+    return "\n".join(lines)
+
+
+def apply_kernel_choices(choices) -> int:
+    """Route the classes of ``choices`` (``tune_kernels`` records, or a
+    ``HardwareProfile`` holding them) process-wide; returns how many."""
+    from .cuda import CudaPrecision
+    from .simulator import set_kernel_choice
+
+    if isinstance(choices, HardwareProfile):
+        choices = choices.kernel_choices
+    for c in choices:
+        prec = CudaPrecision.F64 if c["precision"] == "f64" else CudaPrecision.F32
+        set_kernel_choice(prec, c["k"], c["low_mask"], c["engine"], c["tile_bits"])
+    return len(choices)
+
+
 def _main(argv=None) -> None:
     ap = argparse.ArgumentParser(prog="python -m cast_simulator_b200.autotune")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -318,8 +426,27 @@ def _main(argv=None) -> None:
     t.add_argument("--traj", type=int, default=4096)
     t.add_argument("--p", type=float, default=1e-3)
     t.add_argument("--gamma", type=float, default=5e-4)
+    kk = sub.add_parser("kernels", help="register / tile kernel and tile size per low-target class")
+    kk.add_argument("--n", type=int, default=26)
+    kk.add_argument("--precision", choices=("f64", "f32", "both"), default="both")
+    kk.add_argument("--reps", type=int, default=5)
+    kk.add_argument("--profile", help="profile JSON to store the choices in (created if absent)")
+    kk.add_argument("--cxx-table", action="store_true",
+                    help="print the winners as the library's built-in routing table")
     a = ap.parse_args(argv)
-    if a.cmd == "traj":
+    if a.cmd == "kernels":
+        import os
+
+        precs = ("f64", "f32") if a.precision == "both" else (a.precision,)
+        ch = tune_kernels(a.n, precs, reps=a.reps)
+        if a.profile:
+            prof = (HardwareProfile.load(a.profile) if os.path.exists(a.profile)
+                    else HardwareProfile(0.0, 0.0, 0.0, math.inf))
+            keep = [c for c in prof.kernel_choices if c["precision"] not in precs]
+            prof.kernel_choices = keep + ch
+            prof.save(a.profile)
+        print(cxx_table(ch) if a.cxx_table else json.dumps({"n": a.n, "choices": ch}))
+    elif a.cmd == "traj":
         from .types import QuantumCircuit
 
         circ = QuantumCircuit.brickwork(a.n, a.depth, 31337, depolarizing=a.p, damping=a.gamma)

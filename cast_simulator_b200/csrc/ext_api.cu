@@ -155,6 +155,17 @@ int cast_b200_set_device(int device, char *err_buf, size_t err_buf_len) {
 
 int cast_b200_set_gate_path(int path) { return cb2::set_gate_path(path); }
 
+int cast_b200_set_kernel_choice(uint8_t precision, uint32_t k, uint32_t low_mask, int engine,
+                                uint32_t tile_bits, char *err_buf, size_t err_buf_len) {
+  std::string err;
+  if (!cb2::set_kernel_choice(precision, k, low_mask, engine, tile_bits, err)) {
+    write_err(err_buf, err_buf_len, err);
+    return 1;
+  }
+  clear_err(err_buf, err_buf_len);
+  return 0;
+}
+
 int cast_b200_gate_engine(uint8_t precision, uint32_t sv_n_qubits, const cast_complex64_t *matrix,
                           const uint32_t *qubits, uint32_t n_gate_qubits, double ztol,
                           double otol, int split, char *err_buf, size_t err_buf_len) {

@@ -64,8 +64,18 @@ struct Targets {
 // m[3e], m[3e+1], m[3e+2] = c, d - c, c + d; every other k keeps (re, im) pairs.
 template <int K> struct ThreeMult { static constexpr bool on = K == 4; };
 
+// FP32 4-qubit gates compute two rows at once with the packed FP32 pair FMA of
+// sm_100 (__ffma2_rn: two independent IEEE fmas in one instruction), halving
+// the FMA instructions a pass issues; every lane performs the same fma sequence
+// as the scalar form, so the results are bit-identical.  The 3M entries are
+// then interleaved by row pair: for rows 2p, 2p+1 and column c the six floats
+// at 6 (p D + c) are (c_0, c_1, (d-c)_0, (d-c)_1, (c+d)_0, (c+d)_1).
+template <typename T, int K> struct PairedRows {
+  static constexpr bool on = sizeof(T) == 4 && ThreeMult<K>::on;
+};
+
 template <typename T, int K> struct MatParam {
-  T m[(ThreeMult<K>::on ? 3 : 2) * (1 << K) * (1 << K)];
+  __align__(8) T m[(ThreeMult<K>::on ? 3 : 2) * (1 << K) * (1 << K)];
 };
 
 // Row r of M times the D amplitudes x, for the register and tile kernels.
@@ -99,6 +109,26 @@ __device__ __forceinline__ V gate_row(const MatParam<T, K> &M, int r, const V (&
     o.y = im;
   }
   return o;
+}
+
+// Rows 2p and 2p + 1 of M times x in the paired FP32 3M form.
+template <int K>
+__device__ __forceinline__ void gate_row_pair(const MatParam<float, K> &M, int p,
+                                              const float2 (&x)[1 << K], const float (&sx)[1 << K],
+                                              float2 &o0, float2 &o1) {
+  constexpr int D = 1 << K;
+  float2 s1 = make_float2(0.f, 0.f), s2 = s1, s3 = s1;
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    const float2 *m = reinterpret_cast<const float2 *>(&M.m[6 * (p * D + c)]);
+    s1 = __ffma2_rn(m[0], make_float2(sx[c], sx[c]), s1);
+    s2 = __ffma2_rn(m[1], make_float2(x[c].x, x[c].x), s2);
+    s3 = __ffma2_rn(m[2], make_float2(x[c].y, x[c].y), s3);
+  }
+  const float2 re = __fadd2_rn(s1, make_float2(-s3.x, -s3.y));
+  const float2 im = __fadd2_rn(s1, s2);
+  o0 = make_float2(re.x, im.x);
+  o1 = make_float2(re.y, im.y);
 }
 
 // a + b of each amplitude, the shared operand of S1 (3M form only).
@@ -159,8 +189,18 @@ __global__ void __launch_bounds__(kRegThreads) k_gate_reg(T *__restrict__ sv, ui
     if (g0 + (uint64_t)u * kRegThreads >= n_groups) break;
     T sx[D];
     row_sums<T, K>(x[u], sx);
+    if constexpr (PairedRows<T, K>::on) {
 #pragma unroll
-    for (int r = 0; r < D; ++r) psi[base[u] + member_offset<K>(r, t)] = gate_row<T, K>(M, r, x[u], sx);
+      for (int p = 0; p < D / 2; ++p) {
+        float2 o0, o1;
+        gate_row_pair<K>(M, p, x[u], sx, o0, o1);
+        psi[base[u] + member_offset<K>(2 * p, t)] = o0;
+        psi[base[u] + member_offset<K>(2 * p + 1, t)] = o1;
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < D; ++r) psi[base[u] + member_offset<K>(r, t)] = gate_row<T, K>(M, r, x[u], sx);
+    }
   }
 }
 
@@ -191,19 +231,26 @@ __device__ __forceinline__ uint32_t swz(uint32_t i) {
   return i ^ ((i >> LOGE) & ((1u << LOGE) - 1));
 }
 
-// Amplitudes per tile: 4096 for k = 3, 2048 otherwise (measured at 30 qubits with
-// targets 0..k-1: k = 3 runs at 6.9 instead of 6.1 TB/s (FP64) with the larger
-// tile, k = 2 and 4 lose with it; FP32 k = 4 with 4096-amplitude tiles, 32 KB and
-// five CTAs a SM: 275 us under ncu at 26 qubits against 269 us with 2048).
-template <typename T> constexpr uint32_t tile_bits(uint32_t k) { return k == 3 ? 12u : 11u; }
+// Built-in routing of dense k <= 4 gates with a target below qubit 5, per
+// precision (FP32, FP64), k and the mask of those targets: 'r' the register
+// kernel, 'a' the tile kernel with 2048 amplitudes a tile, 'b' with 4096 ('-'
+// masks with more than k bits).  Measured on a B200 by the kernel autotuner
+// (autotune kernels --n 30 --cxx-table: the fastest of the three on a
+// Haar-random gate over a 30-qubit register, a tile kernel only where it beats
+// the register kernel by more than 2%; the 26-qubit run picks kernels within 2%
+// of these).  cast_b200_set_kernel_choice overrides it per class.
+constexpr char kDefaultChoice[2][5][33] = {
+    {"", "-rr-r---r-------r---------------", "-rrarrr-rrr-r---rrr-r---r-------", "-rrbrrrbrrrbrbb-rrrbrrr-rrr-r---", "-rrbrrrbrrrbrbbbrrrbrrrbrrrbrbb-"},
+    {"", "-rr-r---r-------r---------------", "-rrbrar-rrr-r---rrr-r---r-------", "-rrbrbrbrrrbrbb-rrrrrbr-rrr-r---", "-rrrrrrarrrrrrrarrrrrrrarrrrrrr-"},
+};
 
-template <typename T, int K>
+template <typename T, int K, int TB>
 __global__ void __launch_bounds__(TileThreads<K>::N) k_gate_tile(T *__restrict__ sv, TileArgs a,
                                                                  MatParam<T, K> M) {
   constexpr int kTileThreads = TileThreads<K>::N;
   using V = typename Vec2<T>::type;
   constexpr int D = 1 << K;
-  constexpr uint32_t TILE = 1u << tile_bits<T>(K);
+  constexpr uint32_t TILE = 1u << TB;
   constexpr int LOGE = sizeof(V) == 16 ? 3 : 4;  // elements per 128-byte block
   // groups per thread, fully unrolled (a runtime loop would let the compiler
   // hoist the matrix out of the constant bank into registers)
@@ -241,14 +288,24 @@ __global__ void __launch_bounds__(TileThreads<K>::N) k_gate_tile(T *__restrict__
       }
       T sx[D];
       row_sums<T, K>(x, sx);
-#pragma unroll
-      for (int r = 0; r < D; ++r) {
-        const V o = gate_row<T, K>(M, r, x, sx);
+      auto put = [&](int r, const V &o) {
         uint32_t po = base;
 #pragma unroll
         for (int b = 0; b < K; ++b)
           if ((r >> b) & 1) po += a.loc_lo_mask[b] + 1;
         s[swz<LOGE>(po)] = o;
+      };
+      if constexpr (PairedRows<T, K>::on) {
+#pragma unroll
+        for (int p = 0; p < D / 2; ++p) {
+          float2 o0, o1;
+          gate_row_pair<K>(M, p, x, sx, o0, o1);
+          put(2 * p, o0);
+          put(2 * p + 1, o1);
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < D; ++r) put(r, gate_row<T, K>(M, r, x, sx));
       }
     }
   }
@@ -568,12 +625,17 @@ const MatParam<T, K> *mat_param(const GateData &g, MatParam<T, K> &scratch) {
   if constexpr (ThreeMult<K>::on) {
     constexpr size_t E = size_t(1) << (2 * K);
     const bool wide = g.m64.size() == 2 * E;
+    constexpr size_t D = size_t(1) << K;
     for (size_t e = 0; e < E; ++e) {
       const double c = wide ? g.m64[2 * e] : (double)g.m32[2 * e];
       const double d = wide ? g.m64[2 * e + 1] : (double)g.m32[2 * e + 1];
-      scratch.m[3 * e] = (T)c;
-      scratch.m[3 * e + 1] = (T)(d - c);
-      scratch.m[3 * e + 2] = (T)(c + d);
+      // scalar form: entry e at 3e; paired form: see PairedRows
+      const size_t r = e / D, col = e % D;
+      const size_t at = PairedRows<T, K>::on ? 6 * ((r / 2) * D + col) + (r & 1) : 3 * e;
+      const size_t step = PairedRows<T, K>::on ? 2 : 1;
+      scratch.m[at] = (T)c;
+      scratch.m[at + step] = (T)(d - c);
+      scratch.m[at + 2 * step] = (T)(c + d);
     }
     return &scratch;
   } else {
@@ -737,26 +799,33 @@ bool tile_geometry(const GateData &g, uint32_t n, TileArgs &a, uint32_t target) 
   return false;
 }
 
-template <typename T, int K>
-bool launch_tile(const GateData &g, void *sv, uint32_t n, const TileArgs &a, cudaStream_t s,
-                 std::string &err) {
+template <typename T, int K, int TB>
+bool launch_tile_tb(const GateData &g, void *sv, uint32_t n, const TileArgs &a, cudaStream_t s,
+                    std::string &err) {
   using V = typename Vec2<T>::type;
   static std::once_flag once;
   static cudaError_t attr_rc = cudaSuccess;
   std::call_once(once, [] {
-    attr_rc = cudaFuncSetAttribute(k_gate_tile<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(sizeof(V) << tile_bits<T>(K)));
+    attr_rc = cudaFuncSetAttribute(k_gate_tile<T, K, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(V) << TB));
   });
   if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(tile gate kernel)", err)) return false;
-  const uint64_t n_tiles = 1ull << (n - tile_bits<T>(K));
-  const size_t smem = sizeof(V) << tile_bits<T>(K);
+  const uint64_t n_tiles = 1ull << (n - TB);
+  const size_t smem = sizeof(V) << TB;
   MatParam<T, K> scratch;
   const MatParam<T, K> *mp = mat_param<T, K>(g, scratch);
   T *p = static_cast<T *>(sv);
   void *args[] = {&p, const_cast<TileArgs *>(&a), const_cast<MatParam<T, K> *>(mp)};
-  return cuda_ok(cudaLaunchKernel((const void *)k_gate_tile<T, K>, dim3((unsigned)n_tiles),
+  return cuda_ok(cudaLaunchKernel((const void *)k_gate_tile<T, K, TB>, dim3((unsigned)n_tiles),
                                   dim3(TileThreads<K>::N), args, smem, s),
                  "tile gate kernel launch", err);
+}
+
+template <typename T, int K>
+bool launch_tile(const GateData &g, void *sv, uint32_t n, const TileArgs &a, cudaStream_t s,
+                 std::string &err) {
+  return a.tb + a.k_hi == 12 ? launch_tile_tb<T, K, 12>(g, sv, n, a, s, err)
+                             : launch_tile_tb<T, K, 11>(g, sv, n, a, s, err);
 }
 
 template <typename T, int K>
@@ -799,16 +868,16 @@ std::atomic<int> g_gate_path{[] {
 
 int gate_path_override() { return g_gate_path.load(std::memory_order_relaxed); }
 
-// Whether a dense gate of k <= 4 runs on the tile kernel (fills `a` when it
-// does).  Measured on B200 (30 qubits, every placement of k = 1..4 with low
-  // targets): the register kernel loses bandwidth when a warp's loads of one
-  // member touch many cache lines for a few bytes each and the lines do not
-  // survive in L1 until the group's other members are loaded.  FP64: the tile
-  // kernel runs at 6.9 TB/s and is at or above the register kernel once two
-  // targets lie below qubit 5 (k = 4 on qubits 1..4: 6.9 against 6.1).  FP32:
-  // with targets 0 and 1 (register kernel 2.0-4.2 TB/s), or with the lowest
-  // target 1 and three targets below 5 (k = 3 on 1..3: 6.0 against 4.1);
-  // elsewhere the register kernel is faster (k = 3 on 2..4: 6.4 against 6.0).
+// Per-class kernel choices written by the autotuner (cast_b200_set_kernel_choice).
+// A class is (precision, k = 1..4, the mask of targets below qubit 5).  engine:
+// -1 the built-in rule below, 0 register kernel, 1 tile kernel; tile_bits: 0 the
+// built-in size, 11 or 12 (2048 / 4096 amplitudes a tile).
+struct KernelChoice {
+  std::atomic<int> engine{-1};
+  std::atomic<int> tile_bits{0};
+};
+KernelChoice g_choice[2][5][32];
+
 bool tile_chosen(const GateData &g, uint32_t n, TileArgs &a) {
   if (g.k > 4) return false;
   const int ov = gate_path_override();
@@ -816,14 +885,19 @@ bool tile_chosen(const GateData &g, uint32_t n, TileArgs &a) {
   uint32_t low_bits = 0;
   for (uint32_t b = 0; b < g.k; ++b)
     if (g.qubits[b] < 5) low_bits |= 1u << g.qubits[b];
-  const int n_low = __builtin_popcount(low_bits);
-  const bool tile_wins = g.precision == 1
-                             ? n_low >= 2
-                             : ((low_bits & 0x3u) == 0x3u || (g.qubits[0] == 1 && n_low >= 3));
-  if (ov != 2 && !tile_wins) return false;
-  if (ov == 2 && low_bits == 0) return false;
+  if (low_bits == 0) return false;
+  const int p = g.precision ? 1 : 0;
+  const char def = kDefaultChoice[p][g.k][low_bits];
+  bool tile = def == 'a' || def == 'b';
+  int tb = def == 'b' ? 12 : 11;
+  const KernelChoice &c = g_choice[p][g.k][low_bits];
+  const int tuned = c.engine.load(std::memory_order_relaxed);
+  if (tuned >= 0) tile = tuned == 1;
+  const int tuned_tb = c.tile_bits.load(std::memory_order_relaxed);
+  if (tuned_tb == 11 || tuned_tb == 12) tb = tuned_tb;
+  if (ov != 2 && !tile) return false;
   std::memset(&a, 0, sizeof(a));
-  return tile_geometry(g, n, a, g.precision == 1 ? tile_bits<double>(g.k) : tile_bits<float>(g.k));
+  return tile_geometry(g, n, a, (uint32_t)tb);
 }
 
 template <typename T>
@@ -863,6 +937,21 @@ bool launch_t(const GateData &g, void *sv, uint32_t n, const Targets &t, cudaStr
 }  // namespace
 
 int set_gate_path(int path) { return g_gate_path.exchange(path < 0 || path > 2 ? 0 : path); }
+
+bool set_kernel_choice(uint8_t precision, uint32_t k, uint32_t low_mask, int engine,
+                       uint32_t tile_bits_, std::string &err) {
+  if (precision > 1 || k < 1 || k > 4 || low_mask == 0 || low_mask > 31 ||
+      (uint32_t)__builtin_popcount(low_mask) > k || engine < -1 || engine > 1 ||
+      (tile_bits_ != 0 && tile_bits_ != 11 && tile_bits_ != 12)) {
+    err = "kernel choice: precision 0/1, k 1..4, low mask 1..31 with at most k bits, engine "
+          "-1/0/1, tile bits 0/11/12";
+    return false;
+  }
+  KernelChoice &c = g_choice[precision][k][low_mask];
+  c.engine.store(engine);
+  c.tile_bits.store((int)tile_bits_);
+  return true;
+}
 
 int sm_count() {
   std::call_once(g_sm_once, [] {

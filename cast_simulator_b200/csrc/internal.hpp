@@ -99,6 +99,10 @@ int set_tensor_loader(int mode);
 // Device helpers shared between translation units.
 int sm_count();
 int set_gate_path(int path);  // 0 auto, 1 register, 2 tile; returns previous
+// Autotuned choice for dense gates of k <= 4 with targets below qubit 5 (see
+// cast_b200_set_kernel_choice).
+bool set_kernel_choice(uint8_t precision, uint32_t k, uint32_t low_mask, int engine,
+                       uint32_t tile_bits, std::string &err);
 bool upload_gate_matrix(GateData &g, std::string &err);  // fills g.d_mat
 
 // Reductions (reduce_kernels.cu): synchronous on `s`, except scale (enqueued).

@@ -233,6 +233,9 @@ class HardwareProfile:
     raw: list = field(default_factory=list)
     tensor_gflops_s: float = 0.0
     tensor_min_k: int = 0
+    # measured register / tile kernel choice per low-target gate class
+    # (autotune.tune_kernels records; applied by autotune.apply_kernel_choices)
+    kernel_choices: list = field(default_factory=list)
 
     @staticmethod
     def compute_bw_slope(peak_bw_gib_s: float, scalar_bytes: int) -> float:

@@ -164,6 +164,19 @@ def gate_engine(matrix: np.ndarray, qubits, n_qubits: int, precision: CudaPrecis
     return ENGINES[e]
 
 
+def set_kernel_choice(precision: CudaPrecision, k: int, low_mask: int, engine: str | None,
+                      tile_bits: int = 0) -> None:
+    """Route one class of dense gates (k <= 4 qubits, the targets below qubit 5
+    forming ``low_mask``) to the ``"register"`` or ``"tile"`` kernel, with
+    2^``tile_bits`` amplitudes a tile (11, 12, or 0 for the built-in size);
+    ``engine=None`` restores the built-in rule.  Process-wide, for launches after
+    the call."""
+    code = {None: -1, "register": 0, "tile": 1}[engine]
+    eb = L.errbuf()
+    L.check(L.lib().cast_b200_set_kernel_choice(int(precision), k, low_mask, code, tile_bits, eb,
+                                                L.ERR_LEN), eb)
+
+
 def inner_product(a: CudaStatevector, b: CudaStatevector, stream: Stream | None = None) -> complex:
     if a.n_qubits() != b.n_qubits() or a.precision() != b.precision():
         raise ValueError("statevector size/precision mismatch")

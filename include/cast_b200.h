@@ -50,6 +50,21 @@ int cast_b200_sv_zero_async(uint64_t dptr, size_t n_elements, uint8_t precision,
  * setting.  No reference counterpart (the reference has one code generator). */
 int cast_b200_set_gate_path(int path);
 
+/* Kernel choice for one class of dense gates with k <= 4 that have a target
+ * below qubit 5 (the targets a warp's contiguous loads cannot stride over).  A
+ * class is (precision 0 FP32 / 1 FP64, k, low_mask = the set of targets below
+ * qubit 5 as bits, 1..31 with at most k bits).  engine -1 restores the built-in
+ * rule, 0 routes the class to the register kernel, 1 to the shared-memory tile
+ * kernel; tile_bits 0 keeps the built-in tile size, 11 or 12 sets 2048 or 4096
+ * amplitudes a tile.  Written by the kernel autotuner from measured times; takes
+ * effect for launches after the call (CUDA graphs captured before it keep the
+ * kernels they captured) and applies process-wide.  cast_b200_set_gate_path's
+ * forced paths override it.  Returns 0, or 1 with a message for an
+ * out-of-range class or value.  No reference counterpart (the reference tunes
+ * one generated kernel per gate through its code generator). */
+int cast_b200_set_kernel_choice(uint8_t precision, uint32_t k, uint32_t low_mask, int engine,
+                                uint32_t tile_bits, char *err_buf, size_t err_buf_len);
+
 /* -- One-call gate application ------------------------------------------------
  * Snap (ztol/otol scaled by 1/2^k, as cuda_gen.cpp:84-103) and apply one gate
  * in place on `stream`.  Takes over the compile -> load -> launch sequence of

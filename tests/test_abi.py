@@ -182,6 +182,48 @@ def test_gate_engine_routing(cblib):
         gate_engine(haar(2), (0, 25), 20, F64)
 
 
+def test_kernel_choice_routing(cblib):
+    """Autotuned choices route a low-target class to the register or tile
+    kernel, leave other classes and high-target gates alone, and reset to the
+    built-in rule; out-of-range classes are refused with a message."""
+    from cast_simulator_b200 import _lib as L
+    from cast_simulator_b200.cuda import CudaPrecision as P
+    from cast_simulator_b200.simulator import gate_engine, set_kernel_choice
+
+    rng = np.random.default_rng(4)
+    z = rng.standard_normal((16, 16)) + 1j * rng.standard_normal((16, 16))
+    m4 = np.linalg.qr(z)[0]
+    try:
+        set_kernel_choice(P.F64, 4, 0b1111, "register")
+        assert gate_engine(m4, (0, 1, 2, 3), 20, P.F64) == "register"
+        assert gate_engine(m4, (0, 1, 2, 3), 20, P.F32) == "tile"  # the other precision
+        assert gate_engine(m4, (0, 1, 2, 4), 20, P.F64) == "tile"  # another low mask
+        set_kernel_choice(P.F32, 4, 0b10100, "tile", 12)
+        assert gate_engine(m4, (2, 4, 10, 15), 20, P.F32) == "tile"
+        assert gate_engine(m4, (2, 4, 9, 10), 11, P.F32) == "register"  # no 4096-amplitude tile
+        assert gate_engine(m4, (10, 11, 12, 15), 20, P.F32) == "register"  # no low target
+        set_kernel_choice(P.F64, 4, 0b1111, None)
+        assert gate_engine(m4, (0, 1, 2, 3), 20, P.F64) == "tile"
+        for bad in [(P.F64, 5, 1, "tile", 0), (P.F64, 2, 0b111, "tile", 0), (P.F64, 2, 0, "tile", 0),
+                    (P.F64, 2, 32, "tile", 0), (P.F64, 2, 3, "tile", 10)]:
+            with pytest.raises(L.CudaError, match="kernel choice"):
+                set_kernel_choice(*bad)
+    finally:
+        set_kernel_choice(P.F64, 4, 0b1111, None)
+        set_kernel_choice(P.F32, 4, 0b10100, None)
+
+
+def test_kernel_classes_cover_low_masks():
+    from cast_simulator_b200.autotune import class_targets, kernel_classes
+
+    cls = kernel_classes()
+    assert len(cls) == 5 + 15 + 25 + 30
+    for k, mask in cls:
+        q = class_targets(26, k, mask)
+        assert len(set(q)) == k and list(q) == sorted(q)
+        assert sum(1 << b for b in q if b < 5) == mask
+
+
 def test_compile_is_reentrant(cblib):
     """The reference compiles gates from several worker threads at once
     (cuda/kernel.rs:1078-1096): concurrent calls give exactly the descriptors

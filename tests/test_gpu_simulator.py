@@ -93,6 +93,65 @@ def test_forced_kernel_paths(mods, oracle, path, prec):
         lib.cast_b200_set_gate_path(old)
 
 
+@pytest.mark.parametrize("prec", [1, 0])
+def test_kernel_choice_tile_sizes(mods, oracle, prec):
+    """Each kernel a low-target class can be routed to (register, tile of 2048
+    or 4096 amplitudes) agrees with the oracle."""
+    L, cu, F, S, T = mods
+    lib = L.lib()
+    rng = np.random.default_rng(9)
+    n = 14
+    pats = [(0,), (4,), (0, 1), (1, 3), (0, 13), (0, 1, 2), (2, 4, 12), (0, 1, 2, 3), (1, 2, 3, 4),
+            (0, 4, 9, 13), (3, 7, 12, 13)]
+    try:
+        for q in pats:
+            d = 1 << len(q)
+            z = rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))
+            m = np.linalg.qr(z)[0]
+            mask = sum(1 << b for b in q if b < 5)
+            init = oracle.random_state(n, 4)
+            ref = init.copy()
+            oracle.apply_gate(ref, m, q)
+            for eng, tb in [("register", 0), ("tile", 11), ("tile", 12)]:
+                S.set_kernel_choice(cu.CudaPrecision(prec), len(q), mask, eng, tb)
+                assert S.gate_engine(m, q, n, cu.CudaPrecision(prec)) == eng
+                sv = cu.CudaStatevector(n, cu.CudaPrecision(prec))
+                sv.upload(init)
+                prog = S.GateProgram(cu.CudaPrecision(prec), n, 1e-12, 1e-12)
+                prog.add(m, q)
+                prog.run(sv, None, use_graph=False)
+                got = sv.download()
+                assert np.max(np.abs(got - ref)) < (1e-12 if prec else 1e-5), (q, eng, tb)
+            S.set_kernel_choice(cu.CudaPrecision(prec), len(q), mask, None)
+    finally:
+        for k in range(1, 5):
+            for mask in range(1, 32):
+                if bin(mask).count("1") <= k:
+                    S.set_kernel_choice(cu.CudaPrecision(prec), k, mask, None)
+
+
+def test_tune_kernels_small(mods):
+    """The kernel autotuner runs over every class of a small register, returns a
+    valid winner per class and leaves the built-in rule in place without apply."""
+    from cast_simulator_b200 import autotune as A
+
+    L, cu, F, S, T = mods
+    recs = A.tune_kernels(14, ("f32",), ks=(2, 3), reps=1, apply=False)
+    assert len(recs) == len(A.kernel_classes((2, 3)))
+    rng = np.random.default_rng(1)
+    for r in recs:
+        assert (r["engine"], r["tile_bits"]) in A.KERNEL_CANDIDATES
+        assert set(r["ms"]) == {"register", "tile11", "tile12"}
+        assert all(v > 0 for v in r["ms"].values())
+        d = 1 << r["k"]
+        z = rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))
+        assert S.gate_engine(np.linalg.qr(z)[0], tuple(r["targets"]), 14,
+                             cu.CudaPrecision.F32) == r["builtin"]
+    assert A.apply_kernel_choices(recs[:2]) == 2
+    for r in recs[:2]:
+        S.set_kernel_choice(cu.CudaPrecision.F32, r["k"], r["low_mask"], None)
+
+
 def test_apply_gate_large_k_and_errors(mods, oracle):
     L, cu, F, S, T = mods
     lib = L.lib()
