@@ -519,24 +519,28 @@ def sampling_leg(n: int = 30, depth: int = 20, n_shots: int = 1_000_000, k: int 
     from cast_simulator_b200 import cuda as cu
     from cast_simulator_b200.simulator import Event, Stream, sample
 
+    import torch
+
     _, gates = build_fused(n, depth, k)
     _, sv = _run_fused(n, gates, cu.CudaPrecision.F64, reps=1, warm=False, use_graph=False)
     st = Stream()
     sample(sv, 1000, seed=1, stream=st)  # first launches
+    # the keys land in one reused page-locked buffer: a direct DMA, no driver staging
+    keys = torch.empty(n_shots, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
     e0, e1 = Event(), Event()
     ts = []
-    keys = None
-    for r in range(3):
+    for r in range(5):
         e0.record(st)
-        keys = sample(sv, n_shots, seed=10 + r, stream=st)
+        sample(sv, n_shots, seed=10 + r, stream=st, out=keys)
         e1.record(st)
         e1.sync()
         ts.append(e1.elapsed_s(e0))
     t = float(np.median(ts))
     state_bytes = (1 << n) * 16
     out = {"workload": f"brickwork-{n}q-d{depth}-c128 final state, {n_shots} shots",
-           "ms": t * 1e3, "shots_per_s": n_shots / t,
+           "ms": t * 1e3, "ms_runs": [x * 1e3 for x in ts], "shots_per_s": n_shots / t,
            "state_reads_gbs": 2 * state_bytes / t / 1e9,
+           "output": "keys copied to a reused page-locked host buffer",
            "distinct_outcomes": int(np.unique(keys).size)}
     t0 = time.perf_counter()
     psi = sv.download()

@@ -278,14 +278,19 @@ class CircuitBatch:
 
 
 def sample(sv: CudaStatevector, n_shots: int, seed: int = 0, measured=None,
-           stream: Stream | None = None, uniforms=None) -> np.ndarray:
+           stream: Stream | None = None, uniforms=None, out: np.ndarray | None = None) -> np.ndarray:
     """Shot keys sampled on the device from |a_i|^2 (cast_b200_sample): the
     sampled basis indices, or with `measured` their bits at those qubits packed
     into bits 0..m-1 (the reference's compress_bits), in ascending order of the
     sampled index.  `uniforms` (sorted, in [0, 1), one a shot) replaces the
-    device's Philox draws (cast_b200_sample_at)."""
+    device's Philox draws (cast_b200_sample_at).  `out` (a contiguous uint64
+    array of n_shots, e.g. a reused page-locked buffer) receives the keys and is
+    returned; by default a new array is allocated."""
     q = np.ascontiguousarray([] if measured is None else list(measured), dtype=np.uint32)
-    out = np.zeros(n_shots, dtype=np.uint64)
+    if out is None:
+        out = np.empty(n_shots, dtype=np.uint64)
+    elif out.dtype != np.uint64 or out.size != n_shots or not out.flags["C_CONTIGUOUS"]:
+        raise ValueError("out must be a contiguous uint64 array of n_shots")
     eb = L.errbuf()
     qp = q.ctypes.data_as(L.c_u32p) if q.size else None
     h = stream.handle if stream else None

@@ -157,7 +157,9 @@ int cast_b200_dm_populations(uint64_t rho_dptr, uint32_t n_physical, uint8_t pre
  * cast_b200_sample draws the uniforms on the device (Philox-4x32-10 keyed by
  * `seed`, sorted by construction: normalised exponential spacings);
  * cast_b200_sample_at takes them from the caller (non-decreasing, in [0, 1)).
- * Up to 36 qubits and 2^30 shots a call; synchronous on `stream`. */
+ * Up to 36 qubits and 2^30 shots a call; synchronous on `stream`.  A pinned
+ * (page-locked) out_keys takes the keys by one direct DMA; after an error its
+ * contents are unspecified. */
 int cast_b200_sample(uint64_t sv_dptr, uint32_t n_qubits, uint8_t precision, uint64_t n_shots,
                      uint64_t seed, const uint32_t *measured, uint32_t n_measured,
                      uint64_t *out_keys, void *stream, char *err_buf, size_t err_buf_len);

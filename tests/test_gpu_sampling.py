@@ -129,6 +129,27 @@ def test_edge_cases(mods, oracle):
         S.sample(ref, 2, uniforms=[0.5, 1.0])
 
 
+def test_caller_output_buffer(mods, oracle):
+    """Keys written into a caller's buffer (reused across calls, page-locked or
+    not) equal those of a fresh array; a buffer of the wrong type or size is
+    refused before the device is touched."""
+    import torch
+
+    cu, S = mods
+    sv, _ = _upload(cu, oracle.random_state(14, 8), 1)
+    fresh = S.sample(sv, 30000, seed=5)
+    pinned = torch.empty(30000, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+    plain = np.zeros(30000, dtype=np.uint64)
+    for buf in (pinned, plain, pinned):
+        got = S.sample(sv, 30000, seed=5, out=buf)
+        assert got is buf
+        assert np.array_equal(got, fresh)
+    with pytest.raises(ValueError):
+        S.sample(sv, 30000, seed=5, out=np.zeros(30000, dtype=np.int32))
+    with pytest.raises(ValueError):
+        S.sample(sv, 30000, seed=5, out=np.zeros(100, dtype=np.uint64))
+
+
 def test_quantum_state_sample_histogram(mods, oracle):
     """QuantumState.sample on a simulated circuit: H on qubit 0 and CX(0, 3) give
     outcomes 0b0000 and 0b1001 only, in roughly equal counts."""
