@@ -104,22 +104,34 @@ __global__ void __launch_bounds__(kRedThreads) k_scale(T *__restrict__ x, uint64
   if (blockIdx.x == 0 && threadIdx.x < n - nv * N) x[nv * N + threadIdx.x] *= s;
 }
 
-// Scratch: partial sums + the final value, allocated once per process and
-// grown on demand (the reference keeps the same kind of process-wide scratch,
-// cuda_kernels.cu:203-230).  The mutex serialises users of the scratch.
+// Scratch: partial sums + the final value, one buffer per device, allocated on
+// first use and grown on demand (the reference keeps the same kind of
+// process-wide scratch, cuda_kernels.cu:203-230).  The mutex serialises users
+// of the scratch.  Returns the current device's buffer, or null with a message.
 std::mutex g_scratch_mu;
-double *g_scratch = nullptr;
-int g_scratch_len = 0;
+constexpr int kMaxScratchDevices = 64;
+double *g_scratch_dev[kMaxScratchDevices] = {};
+int g_scratch_len[kMaxScratchDevices] = {};
 
-bool ensure_scratch(int len, std::string &err) {
-  if (g_scratch && g_scratch_len >= len) return true;
-  if (g_scratch) cudaFree(g_scratch);
-  g_scratch = nullptr;
-  g_scratch_len = 0;
-  if (!cuda_ok(cudaMalloc(&g_scratch, sizeof(double) * len), "cudaMalloc (norm scratch)", err))
-    return false;
-  g_scratch_len = len;
-  return true;
+double *ensure_scratch(int len, std::string &err) {
+  int dev = 0;
+  if (!cuda_ok(cudaGetDevice(&dev), "cudaGetDevice", err)) return nullptr;
+  if (dev < 0 || dev >= kMaxScratchDevices) {
+    err = "reduction scratch: device index out of range";
+    return nullptr;
+  }
+  double *&p = g_scratch_dev[dev];
+  int &have = g_scratch_len[dev];
+  if (p && have >= len) return p;
+  if (p) cudaFree(p);
+  p = nullptr;
+  have = 0;
+  if (!cuda_ok(cudaMalloc(&p, sizeof(double) * len), "cudaMalloc (norm scratch)", err)) {
+    p = nullptr;
+    return nullptr;
+  }
+  have = len;
+  return p;
 }
 
 unsigned red_grid(uint64_t nv) {
@@ -132,7 +144,8 @@ template <typename T>
 bool norm_sq_impl(const void *x, uint64_t n, double *out, cudaStream_t s, std::string &err) {
   std::lock_guard<std::mutex> lock(g_scratch_mu);
   const unsigned grid = red_grid(n / V16<T>::N);
-  if (!ensure_scratch((int)grid + 1, err)) return false;
+  double *const g_scratch = ensure_scratch((int)grid + 1, err);
+  if (!g_scratch) return false;
   k_norm_pass1<T><<<grid, kRedThreads, 0, s>>>(static_cast<const T *>(x), n, g_scratch);
   k_norm_pass2<<<1, kRedThreads, 0, s>>>(g_scratch, (int)grid, g_scratch + grid);
   if (!cuda_ok(cudaGetLastError(), "norm kernel launch", err)) return false;
@@ -329,7 +342,8 @@ bool inner_impl(const void *a, const void *b, uint32_t n, double *re, double *im
   std::lock_guard<std::mutex> lock(g_scratch_mu);
   const uint64_t amps = 1ull << n;
   const unsigned grid = red_grid(amps);
-  if (!ensure_scratch(2 * (int)grid + 2, err)) return false;
+  double *const g_scratch = ensure_scratch(2 * (int)grid + 2, err);
+  if (!g_scratch) return false;
   k_inner_pass1<T><<<grid, kRedThreads, 0, s>>>(static_cast<const T *>(a), static_cast<const T *>(b),
                                                  amps, g_scratch);
   k_sum_columns<<<2, kRedThreads, 0, s>>>(g_scratch, (int)grid, 2, g_scratch + 2 * grid);
@@ -351,7 +365,8 @@ bool pop_impl(const void *x, uint32_t n, double *p1, double *norm, cudaStream_t 
   const uint64_t chunks = (1ull << n) >> (n < 3 ? n : 3);
   const unsigned grid = std::min<unsigned>(red_grid(chunks), 2 * sm_count());
   constexpr int W = kMaxPopQubits + 1;
-  if (!ensure_scratch(W * ((int)grid + 1), err)) return false;
+  double *const g_scratch = ensure_scratch(W * ((int)grid + 1), err);
+  if (!g_scratch) return false;
   cudaMemsetAsync(g_scratch, 0, sizeof(double) * W * grid, s);
   k_populations<T><<<grid, kRedThreads, 0, s>>>(static_cast<const T *>(x), n, g_scratch);
   k_sum_columns<<<W, kRedThreads, 0, s>>>(g_scratch, (int)grid, W, g_scratch + (size_t)W * grid);
@@ -374,7 +389,8 @@ bool marg_impl(const void *x, uint32_t n, const uint32_t *measured, uint32_t m, 
   const uint32_t nb = 1u << m;
   const unsigned grid = std::min<unsigned>(red_grid(1ull << n), 2 * sm_count());
   const int need = (int)(nb * (grid + 1)) + 16;
-  if (!ensure_scratch(need, err)) return false;
+  double *const g_scratch = ensure_scratch(need, err);
+  if (!g_scratch) return false;
   uint32_t *dq = reinterpret_cast<uint32_t *>(g_scratch + (size_t)nb * (grid + 1));
   if (!cuda_ok(cudaMemcpyAsync(dq, measured, sizeof(uint32_t) * m, cudaMemcpyHostToDevice, s),
                "cudaMemcpyAsync (measured qubits)", err))
@@ -405,7 +421,8 @@ bool damp_sums_impl(const void *x, uint32_t n, uint64_t mask, double gamma, doub
                     cudaStream_t s, std::string &err) {
   std::lock_guard<std::mutex> lock(g_scratch_mu);
   const unsigned grid = red_grid(1ull << n);
-  if (!ensure_scratch(2 * (int)grid + 2, err)) return false;
+  double *const g_scratch = ensure_scratch(2 * (int)grid + 2, err);
+  if (!g_scratch) return false;
   double res[2];
   k_damp_sums<T><<<grid, kRedThreads, 0, s>>>(static_cast<const T *>(x), n, mask,
                                                powers(1.0 - gamma, 1.0), g_scratch);
