@@ -22,20 +22,24 @@
 //               group) -> coalesced 8-byte stores, 32 consecutive groups of one
 //               member per warp instruction;
 //   warps 4-15  loaders: 8-byte global loads of 4 members per (group, chunk),
-//               split into BF16 hi/lo in registers, 16-byte shared stores in the
-//               UMMA K-major layout with the 128-byte swizzle (8 rows x 128 B
-//               atoms, the 16-byte chunk index XORed with the row: conflict-free
-//               for these stores and for the tensor core's operand reads);
+//               split into BF16 hi/lo in registers and written with tcgen05.st
+//               straight into tensor memory, where the MMA takes its A operand
+//               (tcgen05.mma with [a_tmem]): the tile's 128 groups are the 128
+//               lanes, and a 32-member K atom (one stage) is 32 columns of hi and
+//               32 of lo, two BF16 a column with the even K index in the low half.
+//               Loader warp w writes lanes 32 (w % 4) .. +31, the groups it loads;
 //   warp 16     allocates tensor memory and issues the MMAs (one thread).
-// An operand stage holds one 64-real K atom (32 members) of a tile's 128 groups,
-// hi and lo (32 KB); a tile takes 2^k / 32 consecutive stages.  The loader warps
-// form 3 groups of 128 threads, group j owning stage j, so three stages of loads
-// (96 KB) are in flight per SM.  Shared memory is kept small on purpose: it is
-// carved from the same array as the L1 that holds those loads in flight (k = 6:
-// 64 KB gate + 96 KB stages).  Tensor memory holds two accumulators so the
-// epilogue of one tile overlaps the MMAs of the next.  Every wait on an mbarrier is bounded:
-// on expiry the CTA records an error code (read back by tensor_error_status),
-// drains its outstanding MMAs, frees its tensor memory and exits.
+// A tile takes 2^k / 32 consecutive stages.  The loader warps form 3 groups of
+// 128 threads, group j owning stage j, so three stages of loads (96 KB) are in
+// flight per SM.  Shared memory holds only the split gate (the MMA's B operand,
+// 64 KB for k = 6) and bookkeeping: it is carved from the same array as the L1
+// that holds the loads in flight, and with the data operand in tensor memory
+// instead of in shared stages a 6-qubit pass at 30 qubits went from 3.47 to
+// 2.82 ms.  Tensor memory (512 columns): two accumulators, so the epilogue of
+// one tile overlaps the MMAs of the next, and the three A stages.  Every wait on
+// an mbarrier is bounded: on expiry the CTA records an error code (read back by
+// tensor_error_status), drains its outstanding MMAs, frees its tensor memory and
+// exits.
 #include "internal.hpp"
 
 #include <cuda_bf16.h>
@@ -54,7 +58,7 @@ constexpr int kLoadWarps = 12;                     // warps 4-15
 constexpr int kMmaWarp = kEpiWarps + kLoadWarps;   // warp 16
 constexpr int kUmThreads = (kMmaWarp + 1) * 32;    // 544
 constexpr int kLoadThreads = kLoadWarps * 32;
-constexpr int kStages = 3;                          // operand stages = loader groups
+constexpr int kStages = 3;                          // A stages in TMEM = loader groups
 constexpr int kStageMembers = 32;                   // members per stage: one 64-real K atom
 constexpr int kLoadItems = kStageMembers / 4;       // 4-member chunks per loader thread per stage
 constexpr uint32_t kSuspendNs = 20000;             // hardware suspend hint per try_wait poll
@@ -67,8 +71,8 @@ constexpr uint32_t kErrLoaderWait = 1, kErrMmaFullWait = 2, kErrMmaAccWait = 4,
 
 __device__ uint32_t g_umma_error;
 
-std::atomic<int> g_tensor_loader{0};  // 0 auto, 1 register loaders, 2 TMA where eligible
-bool tma_enabled() { return g_tensor_loader.load() != 1; }
+std::atomic<int> g_tensor_loader{0};  // 0 / 1 register loaders, 2 TMA where eligible
+bool tma_enabled() { return g_tensor_loader.load() == 2; }
 
 template <int K, bool kStage> struct UmCfg {
   static constexpr int D = 1 << K;
@@ -77,13 +81,13 @@ template <int K, bool kStage> struct UmCfg {
   static constexpr int LG = kStages;                       // loader groups: one per stage
   static constexpr int GS = kLoadThreads / LG;             // threads per loader group: one per group row
   static constexpr uint32_t ATOM_G = R * 128;              // one 64-wide K block of Mr
-  static constexpr uint32_t XBYTES = kTileGroups * 128;    // one K atom of X for the tile (hi or lo)
   static constexpr uint32_t GBYTES = R * R * 2;            // one BF16 gate (hi or lo)
-  static constexpr uint32_t STAGE = 2 * XBYTES;
   static constexpr int S = kStages;
-  static constexpr uint32_t TCOLS = 2 * R;                 // two FP32 accumulators of N = R columns
+  static constexpr uint32_t ACOLS = 2 * kStageMembers;     // one A stage in TMEM: hi then lo columns
+  static constexpr uint32_t COL_A = 2 * R;                 // after two FP32 accumulators of N = R columns
+  static constexpr uint32_t TCOLS = 512;
   static constexpr uint32_t NBARS = 2 * S + 5;             // full, empty, accfull x2, accempty x2, drain
-  static constexpr uint32_t OFF_BARS = 2 * GBYTES + S * STAGE;
+  static constexpr uint32_t OFF_BARS = 2 * GBYTES;
   static constexpr uint32_t OFF_MOFF = OFF_BARS + NBARS * 8;         // member offsets (u64 x D)
   static constexpr uint32_t OFF_GBASE = OFF_MOFF + D * 8;            // group bases (u64 x 128)
   static constexpr uint32_t OFF_MISC = OFF_GBASE + kTileGroups * 8;   // tmem slot, abort flag
@@ -98,7 +102,7 @@ template <int K, bool kStage> struct UmCfg {
   static_assert(LG * GS == kLoadThreads && GS == kTileGroups && KH * kStageMembers == D,
                 "one loader thread per group row, whole K atoms per stage");
   static_assert(K >= 5 && R % 64 == 0 && R <= 256, "N, and K blocks of one 128-byte swizzle atom");
-  static_assert(TCOLS >= 32 && (TCOLS & (TCOLS - 1)) == 0 && TCOLS <= 512, "TMEM columns");
+  static_assert(COL_A + S * ACOLS <= TCOLS, "TMEM columns");
   static_assert(SMEM <= 227 * 1024, "shared memory");
   static_assert(OFF_STG % 16 == 0 && STG_ROW % 16 == 0 && OFF_GBASE % 8 == 0, "alignment");
 };
@@ -208,6 +212,38 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tc_mma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc,
+                                          uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// 32 lanes x 32 consecutive 32-bit columns from registers into tensor memory.
+__device__ __forceinline__ void tc_st32(uint32_t taddr, const uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};\n" ::"r"(taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+      "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]),
+      "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]),
+      "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]),
+      "r"(v[30]), "r"(v[31])
+      : "memory");
+}
+
+// 32 lanes x 16 consecutive 32-bit columns from registers into tensor memory.
+__device__ __forceinline__ void tc_st16(uint32_t taddr, const uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16};\n" ::"r"(taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+      "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+      : "memory");
+}
+
 // Shared-memory matrix descriptor, K-major with the 128-byte swizzle: rows of
 // 128 bytes (64 BF16 along K), 8-row atoms 1024 bytes apart (SBO), leading
 // offset unused (1), version 1 (bits 46-47), layout type 2 (bits 61-63).  The
@@ -238,7 +274,6 @@ __global__ void __launch_bounds__(kUmThreads, 1)
   unsigned char *sm = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~static_cast<uintptr_t>(1023));
   const uint32_t s_gate = smem_u32(sm);               // hi at +0, lo at +GBYTES
-  const uint32_t s_stage = s_gate + 2 * C::GBYTES;     // stage i: hi at +i*STAGE, lo at +XBYTES
   const uint32_t s_bar = s_gate + C::OFF_BARS;
   auto full_bar = [&](int s) { return s_bar + 8u * s; };
   auto empty_bar = [&](int s) { return s_bar + 8u * (C::S + s); };
@@ -302,16 +337,16 @@ __global__ void __launch_bounds__(kUmThreads, 1)
         }
         tc_fence_after();
         if (lane == 0) {
-          const uint32_t xh = s_stage + s * C::STAGE, xl = xh + C::XBYTES;
           const uint32_t gh = s_gate + kp * C::ATOM_G, gl = gh + C::GBYTES;
           const uint32_t d = tmem + b * C::R;
 #pragma unroll
           for (int ks = 0; ks < 4; ++ks) {
-            const uint64_t a_hi = umma_desc_sw128(xh + ks * 32), a_lo = umma_desc_sw128(xl + ks * 32);
+            // K reals kp * 64 + ks * 16 .. +15: 8 columns of the stage's hi and lo blocks
+            const uint32_t ah = tmem + C::COL_A + s * C::ACOLS + ks * 8, al = ah + kStageMembers;
             const uint64_t b_hi = umma_desc_sw128(gh + ks * 32), b_lo = umma_desc_sw128(gl + ks * 32);
-            tc_mma(d, a_lo, b_hi, C::IDESC, (kp > 0 || ks > 0) ? 1u : 0u);
-            tc_mma(d, a_hi, b_lo, C::IDESC, 1u);
-            tc_mma(d, a_hi, b_hi, C::IDESC, 1u);
+            tc_mma_ts(d, al, b_hi, C::IDESC, (kp > 0 || ks > 0) ? 1u : 0u);
+            tc_mma_ts(d, ah, b_lo, C::IDESC, 1u);
+            tc_mma_ts(d, ah, b_hi, C::IDESC, 1u);
           }
           tc_commit(empty_bar(s));
           if (kp == C::KH - 1) tc_commit(accfull_bar(b));
@@ -335,7 +370,8 @@ __global__ void __launch_bounds__(kUmThreads, 1)
     const int lt = threadIdx.x - kEpiWarps * 32;
     const int lg = lt / C::GS, gg = lt % C::GS;  // group row gg of every tile
     const uint64_t gb = tc_base<K>((uint64_t)gg, t);
-    unsigned char *xh = sm + 2 * C::GBYTES + lg * C::STAGE, *xl = xh + C::XBYTES;
+    // stage lg's columns in this warp's TMEM sub-partition (lanes of groups gg & ~31)
+    const uint32_t acol = tmem + ((uint32_t)(gg & ~31) << 16) + C::COL_A + lg * C::ACOLS;
     // stage h holds K atom h % KH of tile h / KH; group lg fills stages h = lg, lg + S, ...
     for (uint32_t h = lg;; h += C::S) {
       const uint32_t ti = h / C::KH, kp = h % C::KH, u = h / C::S;
@@ -365,23 +401,24 @@ __global__ void __launch_bounds__(kUmThreads, 1)
         }
       }
       if (!mbar_wait_warp(empty_bar(lg), (u & 1) ^ 1, abort_flag, kErrLoaderWait)) break;
+      tc_fence_after();
+      // member 4 j + q of the stage is column 4 j + q of the hi and of the lo block
+      uint32_t hb[kStageMembers], lb[kStageMembers];
 #pragma unroll
       for (int j = 0; j < kLoadItems; ++j) {
-        uint32_t hb4[4], lb4[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const __nv_bfloat162 hv = __floats2bfloat162_rn(v[j][q].x, v[j][q].y);
-          const uint32_t hb = bf162_bits(hv);
-          const __nv_bfloat162 lv = __floats2bfloat162_rn(v[j][q].x - __uint_as_float(hb << 16),
-                                                          v[j][q].y - __uint_as_float(hb & 0xFFFF0000u));
-          hb4[q] = hb;
-          lb4[q] = bf162_bits(lv);
+          const uint32_t h2 = bf162_bits(hv);
+          hb[4 * j + q] = h2;
+          lb[4 * j + q] = bf162_bits(__floats2bfloat162_rn(v[j][q].x - __uint_as_float(h2 << 16),
+                                                           v[j][q].y - __uint_as_float(h2 & 0xFFFF0000u)));
         }
-        const uint32_t off = (uint32_t)gg * 128 + ((uint32_t)(j ^ (gg & 7)) << 4);
-        *reinterpret_cast<uint4 *>(xh + off) = make_uint4(hb4[0], hb4[1], hb4[2], hb4[3]);
-        *reinterpret_cast<uint4 *>(xl + off) = make_uint4(lb4[0], lb4[1], lb4[2], lb4[3]);
       }
-      fence_async_smem();
+      tc_st32(acol, hb);
+      tc_st32(acol + kStageMembers, lb);
+      asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+      tc_fence_before();
       mbar_arrive(full_bar(lg));
     }
   } else {
@@ -443,19 +480,17 @@ __global__ void __launch_bounds__(kUmThreads, 1)
   }
 }
 
-// ---- TMA-fed variant ----------------------------------------------------------
+// ---- TMA-fed variant (loader mode 2) -------------------------------------------
 // For gates whose lowest target qubit is >= 7 (launched for those only; the kernel
 // itself handles runs of 2^min(q0, 7) amplitudes), the 128 groups of a tile are
-// one contiguous 1 KB run for every member, so the raw
-// FP32 tile is fetched with TMA bulk copies (cp.async.bulk, completion counted
-// on an mbarrier) into a ring of raw slots, one 32-member K atom per slot.  The
-// copies occupy neither L1 nor registers, so the loads in flight are bounded
-// only by the ring (96 KB for k = 6, 128 KB for k = 5).  Warps:
+// one contiguous 1 KB run for every member, so the raw FP32 tile can be fetched
+// with TMA bulk copies (cp.async.bulk, completion counted on an mbarrier) into
+// a ring of raw slots, one 32-member K atom per slot; the copies occupy neither
+// L1 nor registers.  Warps:
 //   0-7   epilogue: warp w reads TMEM sub-partition w % 4 (32 groups) and half
-//         w / 4 of the accumulator columns, so twice as many warps keep stores in
-//         flight as in k_gate_umma;
-//   8-15  converters: thread (gg, half) splits group row gg, members
-//         16 half .. 16 half + 15 of a raw slot into the swizzled operand stage;
+//         w / 4 of the accumulator columns;
+//   8-15  converters: thread (gg, half) splits members 16 half .. 16 half + 15
+//         of group row gg of a raw slot into the A stage in tensor memory;
 //   16    producer: lane 0 arms the slot's mbarrier with the slot's bytes, the 32
 //         lanes issue its bulk copies; before exiting it waits (bounded) for the
 //         copies of the last slots it armed;
@@ -480,21 +515,25 @@ __device__ __forceinline__ void bulk_g2s(uint32_t smem_dst, const void *gmem_src
       : "memory");
 }
 
-template <int K> struct UtCfg {
+// The data operand sits in tensor memory as in k_gate_umma, so the 64 KB gate
+// leaves room for five 32 KB raw slots (160 KB of copies in flight per SM).
+// Tensor memory: accumulators at columns 0 and R, four A stages of 64 columns
+// from 2R (512 columns).  Converter warp w writes lanes 32 (w % 4) .. +31, the
+// groups it converts.
+template <int K> struct UxCfg {
   static constexpr int D = 1 << K;
   static constexpr int R = 2 * D;
-  static constexpr int KH = D / kStageMembers;             // K atoms (slots, stages) per tile
-  static constexpr int S = 2;                              // operand stages
-  static constexpr int RS = K == 6 ? 3 : 4;                // raw slots
+  static constexpr int KH = D / kStageMembers;             // K atoms (slots, A stages) per tile
+  static constexpr int S = 4;                              // A stages in tensor memory
+  static constexpr int RS = 5;                             // raw slots
   static constexpr uint32_t ATOM_G = R * 128;
-  static constexpr uint32_t XBYTES = kTileGroups * 128;    // one K atom of X (hi or lo)
-  static constexpr uint32_t STAGE = 2 * XBYTES;
-  static constexpr uint32_t RAW = kStageMembers * kTileGroups * 8;  // FP32 amplitudes of one slot
+  static constexpr uint32_t RAW = kStageMembers * kTileGroups * 8;
   static constexpr uint32_t GBYTES = R * R * 2;
-  static constexpr uint32_t TCOLS = 2 * R;
+  static constexpr uint32_t ACOLS = 2 * kStageMembers;     // hi then lo, one column a member
+  static constexpr uint32_t COL_A = 2 * R;
+  static constexpr uint32_t TCOLS = 512;
   static constexpr uint32_t NBARS = 2 * RS + 2 * S + 5;
-  static constexpr uint32_t OFF_OP = 2 * GBYTES;
-  static constexpr uint32_t OFF_RAW = OFF_OP + S * STAGE;
+  static constexpr uint32_t OFF_RAW = 2 * GBYTES;
   static constexpr uint32_t OFF_BARS = OFF_RAW + RS * RAW;
   static constexpr uint32_t OFF_MOFF = OFF_BARS + NBARS * 8;
   static constexpr uint32_t OFF_GBASE = OFF_MOFF + D * 8;
@@ -502,16 +541,17 @@ template <int K> struct UtCfg {
   static constexpr uint32_t SMEM = OFF_MISC + 16 + 1024;
   static constexpr uint32_t IDESC =
       (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(R >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-  static_assert(K >= 5 && KH * kStageMembers == D, "whole K atoms");
+  static_assert(K == 6 && KH * kStageMembers == D, "the 6-qubit gate, whole K atoms");
+  static_assert(COL_A + S * ACOLS <= TCOLS, "tensor memory columns");
   static_assert(SMEM <= 227 * 1024, "shared memory");
-  static_assert(OFF_RAW % 1024 == 0 && OFF_OP % 1024 == 0 && OFF_GBASE % 8 == 0, "alignment");
+  static_assert(OFF_RAW % 1024 == 0 && OFF_GBASE % 8 == 0, "alignment");
 };
 
 template <int K, typename Off>
 __global__ void __launch_bounds__(kTThreads, 1)
-    k_gate_umma_tma(float2 *__restrict__ psi, uint64_t n_groups, TcTargets t,
-                    const uint4 *__restrict__ gate, int run_log2) {
-  using C = UtCfg<K>;
+    k_gate_umma_tx(float2 *__restrict__ psi, uint64_t n_groups, TcTargets t,
+                   const uint4 *__restrict__ gate, int run_log2) {
+  using C = UxCfg<K>;
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char *sm = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~static_cast<uintptr_t>(1023));
@@ -519,8 +559,8 @@ __global__ void __launch_bounds__(kTThreads, 1)
   const uint32_t s_bar = s_gate + C::OFF_BARS;
   auto raw_full = [&](int r) { return s_bar + 8u * r; };
   auto raw_empty = [&](int r) { return s_bar + 8u * (C::RS + r); };
-  auto op_full = [&](int q) { return s_bar + 8u * (2 * C::RS + q); };
-  auto op_empty = [&](int q) { return s_bar + 8u * (2 * C::RS + C::S + q); };
+  auto a_full = [&](int q) { return s_bar + 8u * (2 * C::RS + q); };
+  auto a_empty = [&](int q) { return s_bar + 8u * (2 * C::RS + C::S + q); };
   auto accfull_bar = [&](int b) { return s_bar + 8u * (2 * C::RS + 2 * C::S + b); };
   auto accempty_bar = [&](int b) { return s_bar + 8u * (2 * C::RS + 2 * C::S + 2 + b); };
   const uint32_t drain_bar = s_bar + 8u * (2 * C::RS + 2 * C::S + 4);
@@ -544,8 +584,8 @@ __global__ void __launch_bounds__(kTThreads, 1)
       mbar_init(raw_empty(r), kTConvThreads);
     }
     for (int q = 0; q < C::S; ++q) {
-      mbar_init(op_full(q), kTConvThreads);
-      mbar_init(op_empty(q), 1);
+      mbar_init(a_full(q), kTConvThreads);
+      mbar_init(a_empty(q), 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(accfull_bar(b), 1);
@@ -569,32 +609,32 @@ __global__ void __launch_bounds__(kTThreads, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp == kTMmaWarp) {
-    // ---- MMA issuer: tile `it` consumes operand stages h = it * KH + kp --------
+    // ---- MMA issuer: tile `it` consumes A stages h = it * KH + kp --------------
     uint32_t it = 0;
     bool issued = false, ok = true;
     for (uint64_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x, ++it) {
       const uint32_t b = it & 1, v = it >> 1;
       for (int kp = 0; kp < C::KH; ++kp) {
         const uint32_t h = it * C::KH + kp, q = h % C::S, u = h / C::S;
-        if (!mbar_wait_warp(op_full(q), u & 1, abort_flag, kErrMmaFullWait)) { ok = false; break; }
+        if (!mbar_wait_warp(a_full(q), u & 1, abort_flag, kErrMmaFullWait)) { ok = false; break; }
         if (kp == 0 && !mbar_wait_warp(accempty_bar(b), (v & 1) ^ 1, abort_flag, kErrMmaAccWait)) {
           ok = false;
           break;
         }
         tc_fence_after();
         if (lane == 0) {
-          const uint32_t xh = s_gate + C::OFF_OP + q * C::STAGE, xl = xh + C::XBYTES;
           const uint32_t gh = s_gate + kp * C::ATOM_G, gl = gh + C::GBYTES;
           const uint32_t d = tmem + b * C::R;
 #pragma unroll
           for (int ks = 0; ks < 4; ++ks) {
-            const uint64_t a_hi = umma_desc_sw128(xh + ks * 32), a_lo = umma_desc_sw128(xl + ks * 32);
+            // K reals kp * 64 + ks * 16 .. +15: 8 columns of the stage's hi and lo blocks
+            const uint32_t ah = tmem + C::COL_A + q * C::ACOLS + ks * 8, al = ah + kStageMembers;
             const uint64_t b_hi = umma_desc_sw128(gh + ks * 32), b_lo = umma_desc_sw128(gl + ks * 32);
-            tc_mma(d, a_lo, b_hi, C::IDESC, (kp > 0 || ks > 0) ? 1u : 0u);
-            tc_mma(d, a_hi, b_lo, C::IDESC, 1u);
-            tc_mma(d, a_hi, b_hi, C::IDESC, 1u);
+            tc_mma_ts(d, al, b_hi, C::IDESC, (kp > 0 || ks > 0) ? 1u : 0u);
+            tc_mma_ts(d, ah, b_lo, C::IDESC, 1u);
+            tc_mma_ts(d, ah, b_hi, C::IDESC, 1u);
           }
-          tc_commit(op_empty(q));
+          tc_commit(a_empty(q));
           if (kp == C::KH - 1) tc_commit(accfull_bar(b));
         }
         __syncwarp();
@@ -637,37 +677,34 @@ __global__ void __launch_bounds__(kTThreads, 1)
     for (uint32_t j = h > (uint32_t)C::RS ? h - C::RS : 0; j < h; ++j)
       mbar_wait_warp(raw_full(j % C::RS), (j / C::RS) & 1, &never, kErrDrainWait);
   } else if (warp >= kTEpiWarps) {
-    // ---- converters: raw slot -> split BF16 -> operand stage -------------------
+    // ---- converters: raw slot -> split BF16 -> A stage in tensor memory --------
     const int ct = threadIdx.x - kTEpiWarps * 32;
     const int gg = ct % kTileGroups, half = ct / kTileGroups;
+    const uint32_t lanes = (uint32_t)(gg & ~31) << 16;  // this warp's TMEM sub-partition
     for (uint32_t h = 0;; ++h) {
       const uint64_t tile = blockIdx.x + (uint64_t)(h / C::KH) * gridDim.x;
       if (tile >= n_tiles) break;
       const uint32_t r = h % C::RS, ur = h / C::RS, q = h % C::S, uq = h / C::S;
       if (!mbar_wait_warp(raw_full(r), ur & 1, abort_flag, kErrConvertWait)) break;
-      if (!mbar_wait_warp(op_empty(q), (uq & 1) ^ 1, abort_flag, kErrConvertWait)) break;
+      if (!mbar_wait_warp(a_empty(q), (uq & 1) ^ 1, abort_flag, kErrConvertWait)) break;
+      tc_fence_after();
       const unsigned char *raw = sm + C::OFF_RAW + r * C::RAW + gg * 8;
-      unsigned char *xh = sm + C::OFF_OP + q * C::STAGE, *xl = xh + C::XBYTES;
+      uint32_t hb[16], lb[16];
 #pragma unroll
-      for (int jj = 0; jj < 4; ++jj) {
-        const int chunk = 4 * half + jj;
-        uint32_t hb4[4], lb4[4];
-#pragma unroll
-        for (int m = 0; m < 4; ++m) {
-          const float2 v = *reinterpret_cast<const float2 *>(raw + (4 * chunk + m) * (kTileGroups * 8));
-          const __nv_bfloat162 hv = __floats2bfloat162_rn(v.x, v.y);
-          const uint32_t hb = bf162_bits(hv);
-          const __nv_bfloat162 lv = __floats2bfloat162_rn(v.x - __uint_as_float(hb << 16),
-                                                          v.y - __uint_as_float(hb & 0xFFFF0000u));
-          hb4[m] = hb;
-          lb4[m] = bf162_bits(lv);
-        }
-        const uint32_t off = (uint32_t)gg * 128 + ((uint32_t)(chunk ^ (gg & 7)) << 4);
-        *reinterpret_cast<uint4 *>(xh + off) = make_uint4(hb4[0], hb4[1], hb4[2], hb4[3]);
-        *reinterpret_cast<uint4 *>(xl + off) = make_uint4(lb4[0], lb4[1], lb4[2], lb4[3]);
+      for (int i = 0; i < 16; ++i) {
+        const float2 v =
+            *reinterpret_cast<const float2 *>(raw + (16 * half + i) * (kTileGroups * 8));
+        const __nv_bfloat162 hv = __floats2bfloat162_rn(v.x, v.y);
+        hb[i] = bf162_bits(hv);
+        lb[i] = bf162_bits(__floats2bfloat162_rn(v.x - __uint_as_float(hb[i] << 16),
+                                                  v.y - __uint_as_float(hb[i] & 0xFFFF0000u)));
       }
-      fence_async_smem();
-      mbar_arrive(op_full(q));
+      const uint32_t col = tmem + lanes + C::COL_A + q * C::ACOLS + 16 * half;
+      tc_st16(col, hb);
+      tc_st16(col + kStageMembers, lb);
+      asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+      tc_fence_before();
+      mbar_arrive(a_full(q));
       mbar_arrive(raw_empty(r));
     }
   } else {
@@ -756,16 +793,16 @@ bool launch_um_k(const uint32_t *qubits, const void *d_tc, void *sv, uint32_t n,
 }
 
 template <int K, typename Off>
-bool launch_ut_k(const uint32_t *qubits, const void *d_tc, void *sv, uint32_t n, cudaStream_t s,
+bool launch_ux_k(const uint32_t *qubits, const void *d_tc, void *sv, uint32_t n, cudaStream_t s,
                  std::string &err) {
-  using C = UtCfg<K>;
+  using C = UxCfg<K>;
   static std::once_flag once;
   static cudaError_t attr_rc = cudaSuccess;
   std::call_once(once, [] {
-    attr_rc = cudaFuncSetAttribute(k_gate_umma_tma<K, Off>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    attr_rc = cudaFuncSetAttribute(k_gate_umma_tx<K, Off>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)C::SMEM);
   });
-  if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(tensor gate kernel, TMA)", err)) return false;
+  if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(tensor gate kernel, TMA, A in TMEM)", err)) return false;
   TcTargets t;
   for (uint32_t b = 0; b < kMaxGateQubits; ++b) {
     const uint32_t q = b < (uint32_t)K ? qubits[b] : 0;
@@ -775,9 +812,9 @@ bool launch_ut_k(const uint32_t *qubits, const void *d_tc, void *sv, uint32_t n,
   const uint64_t n_tiles = (1ull << (n - K)) / kTileGroups;
   const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(n_tiles, (uint64_t)sm_count()));
   const int run_log2 = (int)std::min<uint32_t>(qubits[0], 7);
-  k_gate_umma_tma<K, Off><<<grid, kTThreads, C::SMEM, s>>>(
+  k_gate_umma_tx<K, Off><<<grid, kTThreads, C::SMEM, s>>>(
       static_cast<float2 *>(sv), 1ull << (n - K), t, static_cast<const uint4 *>(d_tc), run_log2);
-  return cuda_ok(cudaGetLastError(), "tensor gate kernel launch (TMA)", err);
+  return cuda_ok(cudaGetLastError(), "tensor gate kernel launch (TMA, A in TMEM)", err);
 }
 
 }  // namespace
@@ -875,12 +912,13 @@ bool launch_gate_tensor(const GateData &g, void *sv, uint32_t n, cudaStream_t s,
   const void *op = g.d_tc;
   // member offsets are below 2^n amplitudes: 32-bit while n <= 32
   const bool narrow = n <= 32, stage = q[0] == 0;
-  // lowest target >= 7 and whole tiles: every member's 128 groups are one 1 KB
-  // run, fetched with one TMA bulk copy (shorter runs measured slower with TMA
-  // than with register loads: 256-byte copies ran at 2.0 TB/s for k = 6)
+  // TMA bulk-copy feed on request only (loader mode 2), for a lowest target >= 7
+  // and whole tiles, where every member's 128 groups are one 1 KB run: with the
+  // data operand in tensor memory the register loaders measured faster (one
+  // 30-qubit 6-qubit gate, high targets: 2.82 ms against 3.04 ms)
   if (g.tc_k == 6 && q[0] >= 7 && n >= 6 + 7 && tma_enabled())
-    return narrow ? launch_ut_k<6, uint32_t>(q, op, sv, n, s, err)
-                  : launch_ut_k<6, uint64_t>(q, op, sv, n, s, err);
+    return narrow ? launch_ux_k<6, uint32_t>(q, op, sv, n, s, err)
+                  : launch_ux_k<6, uint64_t>(q, op, sv, n, s, err);
   if (g.tc_k == 5) {
     if (narrow) return stage ? launch_um_k<5, uint32_t, true>(q, op, sv, n, s, err)
                              : launch_um_k<5, uint32_t, false>(q, op, sv, n, s, err);

@@ -110,10 +110,11 @@ int cast_b200_program_set_split_precision(void *program, int enable, char *err_b
  * that expired (the affected tiles were left unwritten).  Synchronizes the
  * device first, so every launch issued before the call is covered. */
 int cast_b200_tensor_status(uint32_t *out_bits, char *err_buf, size_t err_buf_len);
-/* Selects how the tensor-core kernel loads amplitudes: 0 = automatic (TMA bulk
- * copies for 6-qubit gates whose lowest target qubit is >= 7 when the statevector has
- * whole 128-group tiles, register loads otherwise), 1 = register loads always.
- * Both give the same results; returns the previous mode. */
+/* Selects how the tensor-core kernel loads amplitudes: 0 or 1 = register loads
+ * (the default, measured fastest), 2 = TMA bulk copies for 6-qubit gates whose
+ * lowest target qubit is >= 7 when the statevector has whole 128-group tiles,
+ * register loads otherwise.  Both give the same results; returns the previous
+ * mode. */
 int cast_b200_set_tensor_loader(int mode);
 uint32_t cast_b200_program_num_gates(const void *program);
 int cast_b200_program_run(void *program, uint64_t sv_dptr, void *stream, int use_graph,

@@ -47,11 +47,12 @@ def _cases(rng, k):
     return out
 
 
-@pytest.mark.parametrize("loader", [0, 1])
+@pytest.mark.parametrize("loader", [0, 2])
 @pytest.mark.parametrize("k", [5, 6])
 def test_single_gate_within_bound(mods, oracle, k, loader):
-    """loader 0: TMA bulk copies where eligible (lowest target >= 7, whole
-    tiles), register loads otherwise; loader 1: register loads everywhere."""
+    """loader 0: register loads everywhere (the default); loader 2: TMA bulk
+    copies where eligible (lowest target >= 7, whole tiles), register loads
+    otherwise."""
     cu, F, S, T = mods
     from cast_simulator_b200 import _lib as L
 
