@@ -565,9 +565,11 @@ def serving_leg(n_req: int, rates=(20.0, 80.0, 320.0)):
     depth 5..40, half complex64 / half complex128, 20% noisy (depolarizing 1e-3,
     256 trajectories; noisy circuits have at most 20 qubits, the trajectory
     kernel's range).  At each swept rate: p50/p99 latency and circuits/s of
-      * the engine: continuous batching, small pure requests (<= 16 qubits) run
-        together in the circuit-batch kernel, the rest on worker streams, complex64
-        requests of 20+ qubits as split-precision programs on the tensor cores;
+      * the engine: continuous batching, small pure requests (<= 16 qubits) on
+        the batcher thread (together in the circuit-batch kernel when 32 or more
+        wait, else one after another on the plain kernels), the rest on worker
+        streams, complex64 requests of 20+ qubits as split-precision programs on
+        the tensor cores;
       * the same engine with the circuit-batch kernel off;
       * sequential execution on the plain path: the same engine one request at a
         time (max_slots = 1, no batching, no tensor cores), on the same arrivals.
@@ -591,7 +593,7 @@ def serving_leg(n_req: int, rates=(20.0, 80.0, 320.0)):
             eng.run_stream(stream(max(rates)))
             for i, rate in enumerate(rates):
                 eng.max_concurrent = 0
-                b0, r0 = eng.batches_run, eng.batched_requests
+                b0, r0, p0 = eng.batches_run, eng.batched_requests, eng.small_plain_requests
                 t0 = time.perf_counter()
                 res = eng.run_stream(stream(rate))
                 wall = time.perf_counter() - t0
@@ -604,9 +606,10 @@ def serving_leg(n_req: int, rates=(20.0, 80.0, 320.0)):
                 entry["by_class"] = {c: {"p50_ms": float(np.percentile(v, 50) * 1e3),
                                          "p99_ms": float(np.percentile(v, 99) * 1e3), "n": len(v)}
                                      for c, v in classes.items() if v}
-                if eng.batches_run > b0:
+                if eng.batches_run > b0 or eng.small_plain_requests > p0:
                     entry["batch_launches"] = eng.batches_run - b0
                     entry["batched_requests"] = eng.batched_requests - r0
+                    entry["small_requests_on_plain_path"] = eng.small_plain_requests - p0
                 if label == "engine":
                     out["rates"][i].update(entry)
                 else:

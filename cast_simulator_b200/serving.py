@@ -13,7 +13,11 @@ this engine keeps many requests in flight:
   * a small pure request (at most ``batch_max_qubits`` qubits) goes to the
     batcher: every small request admitted while the previous batch ran is fused
     by the native planner and executed with the others in ONE persistent launch
-    of the circuit-batch kernel (one CTA a circuit, <Z_q> reduced on the device);
+    of the circuit-batch kernel (one CTA a circuit, <Z_q> reduced on the device)
+    when there are at least ``batch_min`` of them; a smaller batch runs its
+    requests one after another on the plain kernels, which take every SM for a
+    fraction of a millisecond instead of holding a few SMs for milliseconds in
+    the way of the persistent kernels of the large requests;
   * any other admitted request runs on its own CUDA stream in a worker thread:
     its gates are fused by the native planner and uploaded as a gate program
     that is launched on that stream (noisy requests run the persistent
@@ -110,6 +114,7 @@ class ServingEngine:
     def __init__(self, max_slots: int = 8, mem_budget_bytes: int | None = None, fusion_k: int = 4,
                  traj_fusion_k: int | None = None, use_graph: bool = False,
                  batch_max_qubits: int = 16, batch_fusion_k: int = 3, max_batch: int = 1024,
+                 batch_min: int = 32,
                  split_min_qubits: int = 20, heavy_slots: int = 1, heavy_pure_qubits: int = 22,
                  heavy_noisy_qubits: int = 17, heavy_priority: bool = False):
         """max_slots: requests running at once on the worker streams.
@@ -132,7 +137,10 @@ class ServingEngine:
         batch_max_qubits: pure requests of at most this many qubits run batched
         in the circuit-batch kernel (0 turns batching off); batch_fusion_k: their
         fusion width (<= 4); max_batch: circuits a batch launch takes at most
-        (batched requests do not use worker slots)."""
+        (batched requests do not use worker slots); batch_min: the fewest
+        circuits the batch kernel is launched for (fewer run on the plain
+        kernels in the batcher thread: a batch of one circuit would hold one SM
+        for its whole run)."""
         if mem_budget_bytes is None:
             free, _ = cuda_free_memory_bytes()
             mem_budget_bytes = int(free * 0.8)
@@ -146,6 +154,8 @@ class ServingEngine:
         self.batch_max_qubits = batch_max_qubits
         self.batch_fusion_k = batch_fusion_k
         self.max_batch = max_batch
+        self.batch_min = max(1, batch_min)
+        self.small_plain_requests = 0
         self.split_min_qubits = split_min_qubits
         self.heavy_slots = heavy_slots
         self.heavy_pure_qubits = heavy_pure_qubits
@@ -306,6 +316,9 @@ class ServingEngine:
                 if self._stop and not self._bwork:
                     return
                 items = [self._bwork.popleft() for _ in range(min(len(self._bwork), self.max_batch))]
+            if len(items) < self.batch_min:
+                self._run_small_plain(items, stream)
+                continue
             batch.clear()
             svs = []
             try:
@@ -338,6 +351,23 @@ class ServingEngine:
                     for *_, need, _ in items:
                         self._in_use -= need
                     self._batched_active -= len(items)
+                    self._cv.notify_all()
+
+    def _run_small_plain(self, items, stream: Stream) -> None:
+        """A batch below batch_min: its requests run one after another on the
+        plain kernels, on the batcher's stream."""
+        for req, fut, t_arr, need, t_adm in items:
+            try:
+                z = self._execute(req, stream)
+                fut.set_result(Result(req.rid, z, t_arr, t_adm, self.now(), req.circuit.n_qubits(),
+                                      req.precision, 0))
+                self.small_plain_requests += 1
+            except Exception as e:  # the request fails, the engine keeps serving
+                fut.set_exception(e)
+            finally:
+                with self._cv:
+                    self._in_use -= need
+                    self._batched_active -= 1
                     self._cv.notify_all()
 
     def _execute(self, req: Request, stream: Stream) -> np.ndarray:

@@ -34,7 +34,7 @@ def test_results_same_alone_and_in_mix(mods, oracle):
     tolerance) the request run alone on the worker path with batching off."""
     cu, S, T = mods
     reqs = _mix(S, T, cu)
-    eng = S.ServingEngine(max_slots=6)
+    eng = S.ServingEngine(max_slots=6, batch_min=1)
     try:
         mixed = eng.run_stream(reqs)
         assert eng.max_concurrent > 1
@@ -42,7 +42,7 @@ def test_results_same_alone_and_in_mix(mods, oracle):
         assert eng.batches_run < eng.batched_requests  # grouped into fewer launches
     finally:
         eng.shutdown()
-    solo_eng = S.ServingEngine(max_slots=1)
+    solo_eng = S.ServingEngine(max_slots=1, batch_min=1)
     try:
         alone = [solo_eng.submit(r).result() for r in reqs]
     finally:

@@ -181,6 +181,33 @@ class _FakeSv:
         return (16 if self.prec == CudaPrecision.F64 else 8) << self.n
 
 
+def test_small_batches_run_on_the_plain_path(fake_engine, monkeypatch):
+    """Below batch_min the batcher runs its requests one after another on the
+    plain path (never the batch kernel); a failing request fails alone and the
+    memory returns to the budget."""
+
+    class NoBatch:
+        def clear(self):
+            raise AssertionError("the batch kernel must not run for small batches")
+
+        run = add = clear
+
+    make, state = fake_engine
+    monkeypatch.setattr(S, "CircuitBatch", NoBatch)
+    eng = make(max_slots=2, mem_budget_bytes=1 << 40, batch_max_qubits=12, batch_min=1 << 20)
+    futs = [eng.submit(r) for r in _reqs(10, 12, seeds={4: -1})]
+    for i, f in enumerate(futs):
+        if i == 4:
+            with pytest.raises(RuntimeError, match="request 4 failed"):
+                f.result(timeout=30)
+        else:
+            r = f.result(timeout=30)
+            assert r.rid == i and np.all(r.z == float(i))
+    assert eng.small_plain_requests == 11 and eng.batches_run == 0
+    assert state["peak"] == 1  # one after another on the batcher thread
+    assert eng._in_use == 0 and eng._batched_active == 0
+
+
 def test_small_requests_run_batched(monkeypatch):
     """Small pure requests go to the batcher, which runs every request admitted
     while its previous launch ran in one batch; a failing batch fails only its
@@ -216,7 +243,7 @@ def test_small_requests_run_batched(monkeypatch):
     monkeypatch.setattr(S, "Stream", _FakeStream)
     monkeypatch.setattr(S, "CircuitBatch", FakeBatch)
     monkeypatch.setattr(S._SvPool, "get", pool_get)
-    eng = S.ServingEngine(max_slots=2, mem_budget_bytes=1 << 40, batch_max_qubits=12)
+    eng = S.ServingEngine(max_slots=2, mem_budget_bytes=1 << 40, batch_max_qubits=12, batch_min=1)
     try:
         futs = [eng.submit(r) for r in _reqs(10, 40)]
         res = [f.result(timeout=30) for f in futs]
