@@ -366,8 +366,8 @@ def largest_leg(threads: int, depth: int = 10, n64: int = 34, n128: int = 33, n_
     from cast_simulator_b200.types import QuantumCircuit
 
     peak = measured_peak_hbm()[0]
-    out = {"runs": [], "no_k7_tensor_form": "a 7-qubit gate's split operand (256 KB) does not fit in "
-           "shared memory beside the tiles; k = 7 runs on the CUDA cores only"}
+    out = {"runs": [], "no_k7_tensor_form": "a 7-qubit gate's split operand (256 KB) is the MMA's "
+           "shared-memory operand and does not fit there; k = 7 runs on the CUDA cores only"}
     for n, prec, label in ((n64, cu.CudaPrecision.F32, "c64"), (n128, cu.CudaPrecision.F64, "c128")):
         amp = 8 if label == "c64" else 16
         for name, circ in (("brickwork", QuantumCircuit.brickwork(n, depth, 2024)),
