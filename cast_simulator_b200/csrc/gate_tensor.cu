@@ -30,16 +30,17 @@
 //               Loader warp w writes lanes 32 (w % 4) .. +31, the groups it loads;
 //   warp 16     allocates tensor memory and issues the MMAs (one thread).
 // A tile takes 2^k / 32 consecutive stages.  The loader warps form 3 groups of
-// 128 threads, group j owning stage j, so three stages of loads (96 KB) are in
-// flight per SM.  Shared memory holds only the split gate (the MMA's B operand,
-// 64 KB for k = 6) and bookkeeping: it is carved from the same array as the L1
-// that holds the loads in flight, and with the data operand in tensor memory
-// instead of in shared stages a 6-qubit pass at 30 qubits went from 3.47 to
-// 2.82 ms.  Tensor memory (512 columns): two accumulators, so the epilogue of
-// one tile overlaps the MMAs of the next, and the three A stages.  Every wait on
-// an mbarrier is bounded: on expiry the CTA records an error code (read back by
-// tensor_error_status), drains its outstanding MMAs, frees its tensor memory and
-// exits.
+// 128 threads that fill 4 A stages in rotation (group j takes stages j, j + 3,
+// ...), each group issuing its next stage's loads before it waits for a free
+// stage, so three stages of loads (96 KB) are in flight per SM.  Shared memory
+// holds only the split gate (the MMA's B operand, 64 KB for k = 6) and
+// bookkeeping: it is carved from the same array as the L1 that holds the loads
+// in flight, and with the data operand in tensor memory instead of in shared
+// stages a 6-qubit pass at 30 qubits went from 3.47 to 2.82 ms.  Tensor memory
+// (512 columns): two accumulators, so the epilogue of one tile overlaps the MMAs
+// of the next, and the four A stages.  Every wait on an mbarrier is bounded: on
+// expiry the CTA records an error code (read back by tensor_error_status),
+// drains its outstanding MMAs, frees its tensor memory and exits.
 #include "internal.hpp"
 
 #include <cuda_bf16.h>
@@ -58,7 +59,8 @@ constexpr int kLoadWarps = 12;                     // warps 4-15
 constexpr int kMmaWarp = kEpiWarps + kLoadWarps;   // warp 16
 constexpr int kUmThreads = (kMmaWarp + 1) * 32;    // 544
 constexpr int kLoadThreads = kLoadWarps * 32;
-constexpr int kStages = 3;                          // A stages in TMEM = loader groups
+constexpr int kLoadGroups = 3;                      // loader groups of 128 threads
+constexpr int kStages = 4;                          // A stages in TMEM, filled in rotation
 constexpr int kStageMembers = 32;                   // members per stage: one 64-real K atom
 constexpr int kLoadItems = kStageMembers / 4;       // 4-member chunks per loader thread per stage
 constexpr uint32_t kSuspendNs = 20000;             // hardware suspend hint per try_wait poll
@@ -78,7 +80,7 @@ template <int K, bool kStage> struct UmCfg {
   static constexpr int D = 1 << K;
   static constexpr int R = 2 * D;                          // reals per group: MMA N and K extent
   static constexpr int KH = D / kStageMembers;             // stages (K atoms) per tile
-  static constexpr int LG = kStages;                       // loader groups: one per stage
+  static constexpr int LG = kLoadGroups;                   // loader groups
   static constexpr int GS = kLoadThreads / LG;             // threads per loader group: one per group row
   static constexpr uint32_t ATOM_G = R * 128;              // one 64-wide K block of Mr
   static constexpr uint32_t GBYTES = R * R * 2;            // one BF16 gate (hi or lo)
@@ -370,11 +372,15 @@ __global__ void __launch_bounds__(kUmThreads, 1)
     const int lt = threadIdx.x - kEpiWarps * 32;
     const int lg = lt / C::GS, gg = lt % C::GS;  // group row gg of every tile
     const uint64_t gb = tc_base<K>((uint64_t)gg, t);
-    // stage lg's columns in this warp's TMEM sub-partition (lanes of groups gg & ~31)
-    const uint32_t acol = tmem + ((uint32_t)(gg & ~31) << 16) + C::COL_A + lg * C::ACOLS;
-    // stage h holds K atom h % KH of tile h / KH; group lg fills stages h = lg, lg + S, ...
-    for (uint32_t h = lg;; h += C::S) {
-      const uint32_t ti = h / C::KH, kp = h % C::KH, u = h / C::S;
+    // the A stages' columns in this warp's TMEM sub-partition (lanes of groups gg & ~31)
+    const uint32_t acol0 = tmem + ((uint32_t)(gg & ~31) << 16) + C::COL_A;
+    // stage h holds K atom h % KH of tile h / KH in slot h % S; group lg fills
+    // stages h = lg, lg + LG, ...  Before it waits for slot h % S to be free
+    // (stage h - S consumed), it has seen stage h - LG - S consumed, so the wait
+    // is never more than one phase ahead of the slot's barrier.
+    for (uint32_t h = lg;; h += C::LG) {
+      const uint32_t ti = h / C::KH, kp = h % C::KH, u = h / C::S, sl = h % C::S;
+      const uint32_t acol = acol0 + sl * C::ACOLS;
       const uint64_t tile = blockIdx.x + (uint64_t)ti * gridDim.x;
       if (tile >= n_tiles) break;
       const bool live = tile * kTileGroups + gg < n_groups;
@@ -400,7 +406,7 @@ __global__ void __launch_bounds__(kUmThreads, 1)
           for (int q = 0; q < 4; ++q) v[j][q] = make_float2(0.f, 0.f);
         }
       }
-      if (!mbar_wait_warp(empty_bar(lg), (u & 1) ^ 1, abort_flag, kErrLoaderWait)) break;
+      if (!mbar_wait_warp(empty_bar(sl), (u & 1) ^ 1, abort_flag, kErrLoaderWait)) break;
       tc_fence_after();
       // member 4 j + q of the stage is column 4 j + q of the hi and of the lo block
       uint32_t hb[kStageMembers], lb[kStageMembers];
@@ -419,7 +425,7 @@ __global__ void __launch_bounds__(kUmThreads, 1)
       tc_st32(acol + kStageMembers, lb);
       asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
       tc_fence_before();
-      mbar_arrive(full_bar(lg));
+      mbar_arrive(full_bar(sl));
     }
   } else {
     // ---- epilogue: TMEM -> registers -> HBM -----------------------------------
