@@ -427,6 +427,23 @@ __global__ void __launch_bounds__(kStagedThreads, 2) k_gate_staged(
 // bookkeeping is broadcast shared loads.  The CTA barrier between the reads and
 // the in-place writes keeps every group's inputs intact until all its rows are
 // computed.
+// STAGED (gates with a row of more than one nonzero, e.g. the 4-nonzero blocks
+// of a fused QFT): thread (chunk, lane) loads members r0 .. r0 + RPT - 1 of its
+// group - every load in flight at once - into a [member][group] array in shared
+// memory; after one barrier each row reads its inputs there (consecutive lanes,
+// consecutive groups: no bank conflicts) instead of issuing a chain of
+// dependent global loads per row.  64 KB a CTA in every shape.
+// Shared memory of the sparse kernel: values, member offsets, row starts, columns.
+__host__ __device__ inline size_t sparse_smem_bytes(uint32_t k, size_t v_bytes, uint32_t nnz) {
+  return ((nnz * v_bytes + 15) & ~size_t(15)) + sizeof(uint64_t) * (1u << k) +
+         sizeof(uint32_t) * ((1u << k) + 1 + nnz);
+}
+
+// Staging array of the STAGED sparse kernel: after the table, 16-byte aligned.
+__host__ __device__ inline size_t sparse_stage_offset(uint32_t k, size_t v_bytes, uint32_t nnz) {
+  return (sparse_smem_bytes(k, v_bytes, nnz) + 15) & ~size_t(15);
+}
+
 template <typename T, int K> struct SparseShape {
   static constexpr int THREADS = 512;
   static constexpr int D = 1 << K;
@@ -437,7 +454,7 @@ template <typename T, int K> struct SparseShape {
   static constexpr int G = 32 * S;             // groups a CTA
 };
 
-template <typename T, int K>
+template <typename T, int K, bool STAGED>
 __global__ void __launch_bounds__(SparseShape<T, K>::THREADS, 2) k_gate_sparse(
     T *__restrict__ sv, uint64_t n_groups, Targets t, const typename Vec2<T>::type *__restrict__ g_vals,
     const uint32_t *__restrict__ g_rows, const uint32_t *__restrict__ g_cols, uint32_t nnz) {
@@ -465,6 +482,39 @@ __global__ void __launch_bounds__(SparseShape<T, K>::THREADS, 2) k_gate_sparse(
   const uint64_t g = (uint64_t)blockIdx.x * G + (uint64_t)(w / W) * 32 + lane;
   const bool live = g < n_groups;
   const uint64_t base = group_base<K>(live ? g : 0, t);
+  if constexpr (STAGED) {
+    V *xs = reinterpret_cast<V *>(smem_raw + sparse_stage_offset(K, sizeof(V), nnz));  // [D][G]
+    const int gl = (w / W) * 32 + lane;  // the group's column in the staging array
+    V xin[RPT];
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) xin[i] = live ? psi[base + offs[r0 + i]] : V{T(0), T(0)};
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) xs[(r0 + i) * G + gl] = xin[i];
+    __syncthreads();
+    if (!live) return;
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+      const uint32_t a = row_start[r0 + i], e = row_start[r0 + i + 1];
+      T re = T(0), im = T(0);
+      if (a < e) {
+        V m = vals[a];
+        V x = xs[cols[a] * G + gl];
+        re = fma(m.x, x.x, -m.y * x.y);
+        im = fma(m.x, x.y, m.y * x.x);
+        for (uint32_t j = a + 1; j < e; ++j) {
+          m = vals[j];
+          x = xs[cols[j] * G + gl];
+          re = fma(m.x, x.x, fma(-m.y, x.y, re));
+          im = fma(m.x, x.y, fma(m.y, x.x, im));
+        }
+      }
+      V o;
+      o.x = re;
+      o.y = im;
+      psi[base + offs[r0 + i]] = o;
+    }
+    return;
+  }
   uint32_t js[RPT], je[RPT];
   V x0[RPT];
 #pragma unroll
@@ -593,10 +643,16 @@ SparseLayout sparse_layout(uint32_t k, uint8_t precision, size_t nnz) {
   return l;
 }
 
-// Shared memory of the sparse kernel: values, member offsets, row starts, columns.
-size_t sparse_smem_bytes(uint32_t k, size_t v_bytes, uint32_t nnz) {
-  return ((nnz * v_bytes + 15) & ~size_t(15)) + sizeof(uint64_t) * (1u << k) +
-         sizeof(uint32_t) * ((1u << k) + 1 + nnz);
+// Largest number of nonzeros in one row of the gate.
+size_t gate_row_nnz_max(const GateData &g) {
+  const size_t d = size_t(1) << g.k;
+  size_t best = 0;
+  for (size_t r = 0; r < d; ++r) {
+    size_t c = 0;
+    for (size_t e = r * d; e < (r + 1) * d; ++e) c += g.m64[2 * e] != 0.0 || g.m64[2 * e + 1] != 0.0;
+    best = std::max(best, c);
+  }
+  return best;
 }
 
 size_t gate_nnz(const GateData &g) {
@@ -679,18 +735,29 @@ bool launch_sparse(const GateData &g, void *sv, uint32_t n, const Targets &t, cu
     return false;
   }
   const uint32_t nnz = (uint32_t)gate_nnz(g);
-  const size_t smem = sparse_smem_bytes(K, sizeof(V), nnz);
+  constexpr size_t kStage = sizeof(V) * SparseShape<T, K>::G * (1u << K);
   static std::once_flag once;
   static cudaError_t attr_rc = cudaSuccess;
   std::call_once(once, [] {  // the largest table: 2^(2k) / 4 entries
-    attr_rc = cudaFuncSetAttribute(k_gate_sparse<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)sparse_smem_bytes(K, sizeof(V), 1u << (2 * K - 2)));
+    const uint32_t most = 1u << (2 * K - 2);
+    attr_rc = cudaFuncSetAttribute(k_gate_sparse<T, K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)sparse_smem_bytes(K, sizeof(V), most));
+    if (attr_rc == cudaSuccess)
+      attr_rc = cudaFuncSetAttribute(k_gate_sparse<T, K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(sparse_stage_offset(K, sizeof(V), most) + kStage));
   });
   if (!cuda_ok(attr_rc, "cudaFuncSetAttribute(sparse gate kernel)", err)) return false;
-  k_gate_sparse<T, K><<<(unsigned)blocks, SparseShape<T, K>::THREADS, smem, s>>>(
-      static_cast<T *>(sv), n_groups, t, reinterpret_cast<const V *>(base),
-      reinterpret_cast<const uint32_t *>(base + l.row_off),
-      reinterpret_cast<const uint32_t *>(base + l.col_off), nnz);
+  const V *vals = reinterpret_cast<const V *>(base);
+  const uint32_t *rows = reinterpret_cast<const uint32_t *>(base + l.row_off);
+  const uint32_t *cols = reinterpret_cast<const uint32_t *>(base + l.col_off);
+  if (gate_row_nnz_max(g) > 1)
+    k_gate_sparse<T, K, true><<<(unsigned)blocks, SparseShape<T, K>::THREADS,
+                                sparse_stage_offset(K, sizeof(V), nnz) + kStage, s>>>(
+        static_cast<T *>(sv), n_groups, t, vals, rows, cols, nnz);
+  else
+    k_gate_sparse<T, K, false><<<(unsigned)blocks, SparseShape<T, K>::THREADS,
+                                 sparse_smem_bytes(K, sizeof(V), nnz), s>>>(
+        static_cast<T *>(sv), n_groups, t, vals, rows, cols, nnz);
   return cuda_ok(cudaGetLastError(), "sparse gate kernel launch", err);
 }
 
