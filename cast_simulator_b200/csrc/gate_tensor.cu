@@ -187,14 +187,6 @@ __device__ __forceinline__ void tc_commit(uint32_t mbar) {
                    mbar)
                : "memory");
 }
-__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
-                                       uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
-      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
 // 32 lanes x 32 consecutive FP32 columns; the wait is in the same asm block so
 // no use of the registers can be scheduled before the data has landed.
 __device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
