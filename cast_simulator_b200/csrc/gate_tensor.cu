@@ -442,9 +442,24 @@ __global__ void __launch_bounds__(kUmThreads, 1)
           mbar_arrive(accempty_bar(b));
         }
         if constexpr (!kStage) {
-          if (live) {
+          // qubit 0 is not a target: groups gg and gg ^ 1 are adjacent amplitudes, so
+          // lane pairs swap one member and each writes a 16-byte (even, odd group)
+          // pair: half the store instructions, and whole sectors when the warp's
+          // groups are not one contiguous run (targets 1..6: 4.96 -> 3.69 ms at 30
+          // qubits).  Both groups of a pair are live or neither (n_groups is even).
+          const bool odd = lane & 1;
+          float2 *pe = odd ? p - 1 : p;  // the even group's address
 #pragma unroll
-            for (int j = 0; j < 16; ++j) p[moff[cc * 16 + j]] = make_float2(r[2 * j], r[2 * j + 1]);
+          for (int j = 0; j < 16; j += 2) {
+            const float2 mine0 = make_float2(r[2 * j], r[2 * j + 1]);
+            const float2 mine1 = make_float2(r[2 * j + 2], r[2 * j + 3]);
+            const float2 give = odd ? mine0 : mine1;
+            float2 got;
+            got.x = __shfl_xor_sync(0xffffffffu, give.x, 1);
+            got.y = __shfl_xor_sync(0xffffffffu, give.y, 1);
+            const float4 v = odd ? make_float4(got.x, got.y, mine1.x, mine1.y)
+                                 : make_float4(mine0.x, mine0.y, got.x, got.y);
+            if (live) *reinterpret_cast<float4 *>(pe + moff[cc * 16 + j + (odd ? 1 : 0)]) = v;
           }
         } else {
           // a group's 16 members of this chunk go to its staging row; then the
