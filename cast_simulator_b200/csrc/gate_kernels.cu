@@ -579,9 +579,16 @@ __global__ void __launch_bounds__(kSparseTileThreads) k_gate_sparse_tile(
   uint64_t tile_base = (uint64_t)blockIdx.x << a.tb;
   for (uint32_t j = 0; j < a.k_hi; ++j)
     tile_base = ((tile_base & ~a.hi_lo_mask[j]) << 1) | (tile_base & a.hi_lo_mask[j]);
-  for (uint32_t i = threadIdx.x; i < TILE; i += kSparseTileThreads)
-    __pipeline_memcpy_async(&tile[i], &psi[tile_base + a.chunk_off[i >> a.tb] + (i & low_mask)],
-                            sizeof(V));
+  if constexpr (sizeof(V) == 8) {
+    // FP32: amplitude pairs (a chunk is a contiguous run of >= 32 amplitudes
+    // starting at an even index) as 16-byte copies
+    for (uint32_t i = 2 * threadIdx.x; i < TILE; i += 2 * kSparseTileThreads)
+      __pipeline_memcpy_async(&tile[i], &psi[tile_base + a.chunk_off[i >> a.tb] + (i & low_mask)], 16);
+  } else {
+    for (uint32_t i = threadIdx.x; i < TILE; i += kSparseTileThreads)
+      __pipeline_memcpy_async(&tile[i], &psi[tile_base + a.chunk_off[i >> a.tb] + (i & low_mask)],
+                              sizeof(V));
+  }
   __pipeline_commit();
   uint32_t tmask = 0;  // tile-local target bits
 #pragma unroll
@@ -624,8 +631,14 @@ __global__ void __launch_bounds__(kSparseTileThreads) k_gate_sparse_tile(
 #pragma unroll
   for (int u = 0; u < OPT; ++u) tile[threadIdx.x + u * kSparseTileThreads] = out[u];
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < TILE; i += kSparseTileThreads)
-    psi[tile_base + a.chunk_off[i >> a.tb] + (i & low_mask)] = tile[i];
+  if constexpr (sizeof(V) == 8) {
+    for (uint32_t i = 2 * threadIdx.x; i < TILE; i += 2 * kSparseTileThreads)
+      *reinterpret_cast<float4 *>(&psi[tile_base + a.chunk_off[i >> a.tb] + (i & low_mask)]) =
+          *reinterpret_cast<const float4 *>(&tile[i]);
+  } else {
+    for (uint32_t i = threadIdx.x; i < TILE; i += kSparseTileThreads)
+      psi[tile_base + a.chunk_off[i >> a.tb] + (i & low_mask)] = tile[i];
+  }
 }
 
 // Device CSR table of a sparse gate: values (interleaved, the gate's
