@@ -301,3 +301,37 @@ def test_misaligned_pointers_rejected_without_touching_the_device(cblib):
         eb.value = b""
         assert call() == 1, i
         assert b"16-byte aligned" in eb.value, (i, eb.value)
+
+
+def test_default_kernel_table_is_well_formed():
+    """The built-in routing table in gate_kernels.cu has one 32-entry row per
+    precision and k, 'r' / 'a' / 'b' exactly on the masks a k-qubit gate can
+    have, and round-trips through the autotuner's emitter."""
+    import os
+    import re
+
+    from cast_simulator_b200.autotune import cxx_table
+
+    src = open(os.path.join(os.path.dirname(__file__), "..", "cast_simulator_b200", "csrc",
+                            "gate_kernels.cu")).read()
+    body = src[src.index("kDefaultChoice[2][5][33] = {"):]
+    body = body[:body.index("};")]
+    rows = re.findall(r'\{""((?:, "[^"]*")*)\}', body)
+    assert len(rows) == 2
+    table = {}
+    recs = []
+    for p, row in zip(("f32", "f64"), rows):
+        cells = re.findall(r'"([^"]*)"', row)
+        assert len(cells) == 4
+        for k, cell in zip(range(1, 5), cells):
+            assert len(cell) == 32
+            for m, ch in enumerate(cell):
+                possible = m > 0 and bin(m).count("1") <= k
+                assert (ch in "rab") == possible and (ch == "-") == (not possible), (p, k, m, ch)
+                if possible:
+                    eng, tb = {"r": ("register", 0), "a": ("tile", 11), "b": ("tile", 12)}[ch]
+                    recs.append({"precision": p, "k": k, "low_mask": m, "engine": eng, "tile_bits": tb})
+            table[(p, k)] = cell
+    emitted = cxx_table(recs).splitlines()
+    for line, p in zip(emitted, ("f32", "f64")):
+        assert line.strip() == "{" + '""' + "".join(f', "{table[(p, k)]}"' for k in range(1, 5)) + "},"
