@@ -150,6 +150,36 @@ def test_caller_output_buffer(mods, oracle):
         S.sample(sv, 30000, seed=5, out=np.zeros(100, dtype=np.uint64))
 
 
+def test_concurrent_callers_get_their_own_scratch(mods, oracle):
+    """Threads sampling at the same time on their own streams each take a
+    scratch buffer of their own from the cache: every result equals the same
+    draw made alone, and repeated rounds reuse the buffers."""
+    import threading
+
+    cu, S = mods
+    svs = [_upload(cu, oracle.random_state(15, 20 + i), i % 2)[0] for i in range(4)]
+    alone = [S.sample(sv, 20000 + 1000 * i, seed=7 + i) for i, sv in enumerate(svs)]
+    for _ in range(3):
+        got = [None] * 4
+        errors = []
+
+        def run(i):
+            try:
+                st = S.Stream()
+                got[i] = S.sample(svs[i], 20000 + 1000 * i, seed=7 + i, stream=st)
+            except Exception as e:  # reported below
+                errors.append(e)
+
+        threads = [threading.Thread(target=run, args=(i,)) for i in range(4)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        assert not errors
+        for a, g in zip(alone, got):
+            assert np.array_equal(a, g)
+
+
 def test_quantum_state_sample_histogram(mods, oracle):
     """QuantumState.sample on a simulated circuit: H on qubit 0 and CX(0, 3) give
     outcomes 0b0000 and 0b1001 only, in roughly equal counts."""
