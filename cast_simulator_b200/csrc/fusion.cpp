@@ -8,7 +8,7 @@
 //     (src/fusion.rs:14-345);
 //   * SizeOnlyCostModel and HardwareAdaptiveCostModel (src/cost_model.rs:20-44,
 //     238-275), the latter with a per-gate-size crossover so that gates that run
-//     on the tensor-core path are judged against the tensor pipe's ceiling.
+//     on the tensor-core path are measured against the tensor pipe's ceiling.
 // Unitary gates only (the state-vector path); noisy circuits are fused on the
 // host-side Python mirror, which keeps the Kraus branches.
 #include "../../include/cast_b200.h"
