@@ -883,39 +883,44 @@ def sharded_line(args, ws: int, rank: int, local: int, pg) -> dict:
         sv.set_zero()
         sv.apply_circuit(gates)
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    ex0, amps0 = sv.n_exchanges, sv.exchanged_amps
-    st = torch.cuda.current_stream()
-    e0, e1 = Event(), Event()
-    if pg:
-        pg.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        e0.record(st.cuda_stream)
+    # every launch of the run (torch ops, gate kernels, NCCL ordering) goes to one
+    # non-default stream, the one the events are recorded on: the legacy default
+    # stream has no handle an event can be recorded on through the C ABI
+    st = torch.cuda.Stream(device=f"cuda:{local}")
+    with torch.cuda.stream(st):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        ex0, amps0 = sv.n_exchanges, sv.exchanged_amps
+        e0, e1 = Event(), Event()
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            e0.record(st.cuda_stream)
+            for _ in range(args.steps):
+                step()
+            e1.record(st.cuda_stream)
+            e1.sync()
+        t = max(e1.elapsed_s(e0), 1e-12)
+        ex_step = (sv.n_exchanges - ex0) / max(1, args.steps)
+        amps_step = (sv.exchanged_amps - amps0) / max(1, args.steps)
+        if pg:
+            tt = torch.tensor([t], device=f"cuda:{local}", dtype=torch.float64)
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+            t = float(tt.item())
+        amp = 16 if f64 else 8
+        bytes_per_pass = 2 * (1 << n_tot) * amp
+        value = args.steps * len(gates) * bytes_per_pass / t / 1e9
+        # e2e: <Z> back to the host every step
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
         for _ in range(args.steps):
             step()
-        e1.record(st.cuda_stream)
-        e1.sync()
-    t = max(e1.elapsed_s(e0), 1e-12)
-    ex_step = (sv.n_exchanges - ex0) / max(1, args.steps)
-    amps_step = (sv.exchanged_amps - amps0) / max(1, args.steps)
-    if pg:
-        tt = torch.tensor([t], device=f"cuda:{local}", dtype=torch.float64)
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        t = float(tt.item())
-    amp = 16 if f64 else 8
-    bytes_per_pass = 2 * (1 << n_tot) * amp
-    value = args.steps * len(gates) * bytes_per_pass / t / 1e9
-    # e2e: <Z> back to the host every step
-    if pg:
-        pg.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        step()
-        z = sv.expectation_z()
-    e2e_t = time.perf_counter() - t0
+            z = sv.expectation_z()
+        e2e_t = time.perf_counter() - t0
+        torch.cuda.synchronize()
     if pg:
         et = torch.tensor([e2e_t], device=f"cuda:{local}", dtype=torch.float64)
         pg.all_reduce(et, op=pg.ReduceOp.MAX)
