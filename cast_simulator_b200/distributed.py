@@ -220,12 +220,32 @@ class ShardedStatevector:
         """<Z_q> for every logical qubit, every rank (FP64 all-reduce)."""
         import torch
 
-        p = torch.view_as_real(self.shard).to(torch.float64).square().sum(-1)  # |psi|^2 in FP64
-        ones = torch.zeros(self.n + 1, dtype=torch.float64, device=p.device)
-        idx = torch.arange(1 << self.n_local, device=p.device)
-        for pos in range(self.n_local):
-            ones[pos] = p[((idx >> pos) & 1) == 1].sum()
-        tot = p.sum()
+        if self.shard.is_cuda:
+            # one FP64 device pass over the shard for every local qubit
+            # (cast_b200_qubit_populations), on torch's current stream
+            import ctypes as C
+
+            from . import _lib as L
+
+            pop = np.zeros(max(1, self.n_local), dtype=np.float64)
+            nrm = C.c_double()
+            eb = L.errbuf()
+            stream = torch.cuda.current_stream(self.shard.device).cuda_stream
+            prec = 1 if self.shard.dtype == torch.complex128 else 0
+            L.check(L.lib().cast_b200_qubit_populations(
+                self.shard.data_ptr(), self.n_local, prec, pop.ctypes.data_as(L.c_dp), C.byref(nrm),
+                C.c_void_p(stream) if stream else None, eb, L.ERR_LEN), eb, "qubit_populations")
+            host = np.zeros(self.n + 1, dtype=np.float64)
+            host[:self.n_local] = pop[:self.n_local]
+            tot = nrm.value
+            ones = torch.tensor(host, dtype=torch.float64, device=self.shard.device)
+        else:
+            p = torch.view_as_real(self.shard).to(torch.float64).square().sum(-1)  # |psi|^2 in FP64
+            ones = torch.zeros(self.n + 1, dtype=torch.float64, device=p.device)
+            idx = torch.arange(1 << self.n_local, device=p.device)
+            for pos in range(self.n_local):
+                ones[pos] = p[((idx >> pos) & 1) == 1].sum()
+            tot = p.sum()
         for b in range(self.g):
             ones[self.n_local + b] = tot if (self.rank >> b) & 1 else 0.0
         ones[self.n] = tot
